@@ -1,0 +1,401 @@
+// C entry points of the CPU oracle -- TEST INFRASTRUCTURE ONLY (tests/,
+// smoke() and the CPU-baseline leg of bench.py load this through ctypes).
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "smmp_oracle.hpp"
+
+using oracle::Smmp;
+
+namespace {
+thread_local std::string g_err;
+template <class F>
+int guard(F&& f) {
+  try {
+    f();
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return 1;
+  }
+}
+Smmp* S(void* h) { return static_cast<Smmp*>(h); }
+int ntlvr(Smmp* s) { return s->ivrml1[s->ntlml] + s->nvrml[s->ntlml] - 1; }
+}  // namespace
+
+extern "C" {
+
+const char* orc_last_error() { return g_err.c_str(); }
+
+void* orc_create(const char* libdir, int sh2, int epsd, int itysol) {
+  auto s = std::make_unique<Smmp>();
+  s->sh2 = sh2 != 0;
+  s->epsd = epsd != 0;
+  s->itysol = itysol;
+  if (guard([&] { s->init_energy(libdir); })) return nullptr;
+  return s.release();
+}
+
+void* orc_clone(void* h) { return new Smmp(*S(h)); }
+void orc_destroy(void* h) { delete S(h); }
+
+int orc_init_molecule(void* h, const char* seq, const char* var, const char* grpn,
+                      const char* grpc) {
+  return guard([&] { S(h)->init_molecule(seq, var ? var : " ", grpn, grpc); });
+}
+
+// Sizes: [natoms, ntlvr (all variables), nvr (free variables), nres,
+//         nvw (vdW domains), n14 (1-4 partners), nms (moving sets)].
+void orc_sizes(void* h, int* out) {
+  Smmp* s = S(h);
+  int n = s->ntlml;
+  out[0] = s->iatrs2[s->irsml2[n]];
+  out[1] = ntlvr(s);
+  out[2] = s->nvr;
+  out[3] = s->irsml2[n];
+  out[4] = s->ivwml1[n] + s->nvwml[n] - 1;
+  out[5] = s->i14ml1[n] + s->n14ml[n] - 1;
+  out[6] = s->imsml1[n] + s->nmsml[n] - 1;
+}
+
+// Energy of the current variables; terms = [eyel, eyvw, eyhb, eyvr, eysl, eysm].
+int orc_energy(void* h, double* e, double* terms) {
+  Smmp* s = S(h);
+  return guard([&] {
+    *e = s->energy();
+    if (terms) {
+      terms[0] = s->eyel;
+      terms[1] = s->eyvw;
+      terms[2] = s->eyhb;
+      terms[3] = s->eyvr;
+      terms[4] = s->eysl;
+      terms[5] = s->eysm;
+    }
+  });
+}
+
+void orc_get_vlvr(void* h, double* out) {
+  Smmp* s = S(h);
+  for (int i = 1; i <= ntlvr(s); ++i) out[i - 1] = s->vlvr[i];
+}
+void orc_set_vlvr(void* h, const double* in) {
+  Smmp* s = S(h);
+  for (int i = 1; i <= ntlvr(s); ++i) s->vlvr[i] = in[i - 1];
+}
+void orc_get_idvr(void* h, int* out) {
+  Smmp* s = S(h);
+  for (int i = 1; i <= s->nvr; ++i) out[i - 1] = s->idvr[i];
+}
+void orc_get_axvr(void* h, double* out) {
+  Smmp* s = S(h);
+  for (int i = 1; i <= ntlvr(s); ++i) out[i - 1] = s->axvr[i];
+}
+void orc_get_coords(void* h, double* xyz) {
+  Smmp* s = S(h);
+  int na = s->iatrs2[s->irsml2[s->ntlml]];
+  for (int i = 1; i <= na; ++i) {
+    xyz[3 * (i - 1) + 0] = s->xat(i);
+    xyz[3 * (i - 1) + 1] = s->yat(i);
+    xyz[3 * (i - 1) + 2] = s->zat(i);
+  }
+}
+// Internal state that the rebuild reads: toat (per atom).
+void orc_get_toat(void* h, double* out) {
+  Smmp* s = S(h);
+  int na = s->iatrs2[s->irsml2[s->ntlml]];
+  for (int i = 1; i <= na; ++i) out[i - 1] = s->toat[i];
+}
+
+// Topology and interaction lists, 1-based values as in the reference arrays.
+//   atom_i:  per atom [ityat, iowat, nbdat, ibdat1, ibdat2, ibdat3, ixmsat,
+//                      ivwat1, ivwat2, i14at1, i14at2]          (11 ints)
+//   atom_d:  per atom [cgat, blat, baat, toat]                 (4 doubles)
+//   var_i:   per variable [iatvr, ityvr, iclvr, iorvr, imsvr1, imsvr2,
+//                          iadvr1, iadvr2, fxvr]               (9 ints)
+//   ms:      per moving set [latms1, latms2]
+//   vw:      per vdW domain [lvwat1, lvwat2, ixatvw]
+//   l14:     per 1-4 entry  [l14at, ixat14]
+void orc_get_topology(void* h, int* atom_i, double* atom_d, int* var_i, int* ms, int* vw,
+                      int* l14) {
+  Smmp* s = S(h);
+  int sz[7];
+  orc_sizes(h, sz);
+  for (int i = 1; i <= sz[0]; ++i) {
+    int* a = atom_i + 11 * (i - 1);
+    a[0] = s->ityat[i];
+    a[1] = s->iowat[i];
+    a[2] = s->nbdat[i];
+    a[3] = s->IBD(1, i);
+    a[4] = s->IBD(2, i);
+    a[5] = s->IBD(3, i);
+    a[6] = s->ixmsat[i];
+    a[7] = s->ivwat1[i];
+    a[8] = s->ivwat2[i];
+    a[9] = s->i14at1[i];
+    a[10] = s->i14at2[i];
+    double* d = atom_d + 4 * (i - 1);
+    d[0] = s->cgat[i];
+    d[1] = s->blat[i];
+    d[2] = s->baat[i];
+    d[3] = s->toat[i];
+  }
+  for (int i = 1; i <= sz[1]; ++i) {
+    int* v = var_i + 9 * (i - 1);
+    v[0] = s->iatvr[i];
+    v[1] = s->ityvr[i];
+    v[2] = s->iclvr[i];
+    v[3] = s->iorvr[i];
+    v[4] = s->imsvr1[i];
+    v[5] = s->imsvr2[i];
+    v[6] = s->iadvr1[i];
+    v[7] = s->iadvr2[i];
+    v[8] = s->fxvr[i];
+  }
+  for (int i = 1; i <= sz[6]; ++i) {
+    ms[2 * (i - 1)] = s->latms1[i];
+    ms[2 * (i - 1) + 1] = s->latms2[i];
+  }
+  for (int i = 1; i <= sz[4]; ++i) {
+    vw[3 * (i - 1)] = s->lvwat1[i];
+    vw[3 * (i - 1) + 1] = s->lvwat2[i];
+    vw[3 * (i - 1) + 2] = s->ixatvw[i];
+  }
+  for (int i = 1; i <= sz[5]; ++i) {
+    l14[2 * (i - 1)] = s->l14at[i];
+    l14[2 * (i - 1) + 1] = s->ixat14[i];
+  }
+}
+
+// Atom names (4 chars each, no terminator) and variable names (3 chars each).
+void orc_get_names(void* h, char* atoms, char* vars) {
+  Smmp* s = S(h);
+  int sz[7];
+  orc_sizes(h, sz);
+  for (int i = 1; i <= sz[0]; ++i) std::memcpy(atoms + 4 * (i - 1), s->nmat[i].data(), 4);
+  for (int i = 1; i <= sz[1]; ++i) std::memcpy(vars + 3 * (i - 1), s->nmvr[i].data(), 3);
+}
+
+void orc_set_beta(void* h, double beta) { S(h)->beta = beta; }
+void orc_set_rndord(void* h, int r) { S(h)->rndord = r != 0; }
+void orc_sgrnd(void* h, int seed) { S(h)->sgrnd(seed); }
+double orc_grnd(void* h) { return S(h)->grnd(); }
+void orc_get_mt(void* h, unsigned* state, int* mti) {
+  std::memcpy(state, S(h)->mt, sizeof(S(h)->mt));
+  *mti = S(h)->mti;
+}
+
+// Canonical random start (canon.f:60-67): vlvr(idvr(i)) = addang(pi, axvr*(grnd()-0.5)).
+void orc_random_start(void* h) {
+  Smmp* s = S(h);
+  for (int i = 1; i <= s->nvr; ++i) {
+    int iv = s->idvr[i];
+    double dv = s->axvr[iv] * (s->grnd() - 0.5);
+    s->vlvr[iv] = oracle::addang(3.141592653589793, dv);
+  }
+}
+
+// nsweeps calls of metropolis with the canonical weight at s->beta.  If
+// accept_log is given, it receives one byte per proposal (1 = accepted).
+int orc_sweeps(void* h, int nsweeps, double* eol, double* acz, unsigned char* accept_log) {
+  Smmp* s = S(h);
+  return guard([&] {
+    Smmp::Weight w;
+    for (int k = 0; k < nsweeps; ++k) {
+      long long before = s->nacalls;
+      long long cbefore = s->ncalls;
+      if (accept_log) {
+        // replay the sweep proposal by proposal to record decisions
+        std::vector<double> vrol(s->vlvr);
+        double e = s->energy();
+        for (int nsw = 1; nsw <= s->nvr; ++nsw) {
+          int ivar = s->rndord ? 1 + int(s->nvr * s->grnd()) : nsw;
+          int jv = s->idvr[ivar];
+          vrol = s->vlvr;
+          double dv = s->axvr[jv] * (s->grnd() - 0.5);
+          s->vlvr[jv] = oracle::addang(vrol[jv], dv);
+          double enw = s->energy();
+          double delta = s->weight(w, enw) - s->weight(w, e);
+          int up = 0;
+          if (delta <= 0.0) {
+            e = enw;
+            up = 1;
+          } else {
+            double rd = s->grnd();
+            delta = std::min(delta, 100.0);
+            if (std::exp(-delta) >= rd) {
+              e = enw;
+              up = 1;
+            } else {
+              s->vlvr = vrol;
+            }
+          }
+          *acz += up;
+          ++s->ncalls;
+          s->nacalls += up;
+          accept_log[(size_t)k * s->nvr + (nsw - 1)] = (unsigned char)up;
+        }
+        double enw = s->energy();
+        if (std::fabs(e - enw) > 0.000001 && e < 100000)
+          throw std::runtime_error("metropolis: eol and enw difference unacceptable");
+        *eol = e;
+      } else {
+        s->metropolis(*eol, *acz, w);
+      }
+      (void)before;
+      (void)cbefore;
+    }
+  });
+}
+
+// Simulated annealing driver (anneal.f:13-152): random start, nequi sweeps at
+// 1/tmax, then nswp+1 sweeps with beta = bmin*db**nsw.  out = [start energy,
+// energy after equilibration, acceptance, last energy, lowest energy,
+// sweep of lowest energy].
+int orc_anneal(void* h, int nequi, int nswp, double tmax, double tmin, int lrand, double* out) {
+  Smmp* s = S(h);
+  return guard([&] {
+    Smmp::Weight w;
+    double bmin = 1.0 / (tmax * 1.98773e-3);
+    double bmax = 1.0 / (tmin * 1.98773e-3);
+    double db = std::exp(std::log(bmax / bmin) / nswp);
+    if (lrand) orc_random_start(h);
+    double eol = s->energy();
+    out[0] = eol;
+    s->beta = bmin;
+    double acz = 0.0;
+    for (int nsw = 1; nsw <= nequi; ++nsw) s->metropolis(eol, acz, w);
+    out[1] = eol;
+    acz = 0.0;
+    double ymin = eol;
+    int nemin = 0;
+    int nsw;
+    for (nsw = 0; nsw <= nswp; ++nsw) {
+      s->beta = bmin * std::pow(db, nsw);
+      s->metropolis(eol, acz, w);
+      if (eol < ymin) {
+        ymin = eol;
+        nemin = nsw;
+      }
+    }
+    out[2] = acz / double(nsw * s->nvr);
+    out[3] = eol;
+    out[4] = ymin;
+    out[5] = nemin;
+  });
+}
+
+// Serial parallel tempering (partem_s.f:13-258, newsta=.true., switch=1):
+// betas[num_rep] (index k = temperature label), one shared MT stream.
+// eol_out[num_rep] per replica, ipoi_out[num_rep] final temperature->replica
+// map, vl_out[num_rep*nvr] final free variables of each replica.
+int orc_partem(void* h, int num_rep, const double* betas, int nequi, int nswp, double* eol_out,
+               int* ipoi_out, double* vl_out) {
+  Smmp* s = S(h);
+  return guard([&] {
+    Smmp::Weight w;
+    int nvr = s->nvr;
+    const double pi = 3.141592653589793;
+    std::vector<double> coor((size_t)nvr * num_rep), eol(num_rep + 1), acc(num_rep + 1);
+    std::vector<int> ipoi(num_rep + 1);
+    for (int j = 1; j <= num_rep; ++j) ipoi[j] = j;
+    for (int i = 1; i <= num_rep; ++i)
+      for (int j = 1; j <= nvr; ++j) {
+        int iv = s->idvr[j];
+        double dv = s->axvr[iv] * (s->grnd() - 0.5);
+        coor[(size_t)(i - 1) * nvr + (j - 1)] = oracle::addang(pi, dv);
+      }
+    for (int k = 1; k <= num_rep; ++k) {
+      s->beta = betas[k - 1];
+      for (int i = 1; i <= nvr; ++i) s->vlvr[s->idvr[i]] = coor[(size_t)(k - 1) * nvr + i - 1];
+      double energ = s->energy();
+      double acz = 0.0;
+      for (int nsw = 1; nsw <= nequi; ++nsw) s->metropolis(energ, acz, w);
+      for (int i = 1; i <= nvr; ++i) coor[(size_t)(k - 1) * nvr + i - 1] = s->vlvr[s->idvr[i]];
+      eol[k] = energ;
+    }
+    int iswitch = 1;
+    for (int nsw = 1; nsw <= nswp; ++nsw) {
+      for (int k1 = 1; k1 <= num_rep; ++k1) {
+        int k = ipoi[k1];
+        s->beta = betas[k1 - 1];
+        double energ = eol[k];
+        double acz = acc[k];
+        for (int i = 1; i <= nvr; ++i) s->vlvr[s->idvr[i]] = coor[(size_t)(k - 1) * nvr + i - 1];
+        s->setvar(1, s->vlvr.data());
+        s->metropolis(energ, acz, w);
+        for (int i = 1; i <= nvr; ++i) coor[(size_t)(k - 1) * nvr + i - 1] = s->vlvr[s->idvr[i]];
+        eol[k] = energ;
+        acc[k] = acz;
+      }
+      if (!(num_rep > 1)) continue;
+      int num_rep1, nu;
+      if (iswitch == 1) {
+        num_rep1 = num_rep - 1;
+        nu = 1;
+        iswitch = 2;
+      } else {
+        num_rep1 = num_rep;
+        nu = 2;
+        iswitch = 1;
+      }
+      for (int i = nu; i <= num_rep1; i += 2) {
+        int j = i + 1;
+        if (i == num_rep) j = 1;
+        int in = ipoi[i], jn = ipoi[j];
+        double delta = -betas[i - 1] * eol[jn] - betas[j - 1] * eol[in] + betas[i - 1] * eol[in] +
+                       betas[j - 1] * eol[jn];
+        double ra = s->grnd();
+        if (ra <= std::exp(delta)) {
+          ipoi[i] = jn;
+          ipoi[j] = in;
+        }
+      }
+    }
+    for (int k = 1; k <= num_rep; ++k) {
+      eol_out[k - 1] = eol[k];
+      ipoi_out[k - 1] = ipoi[k];
+      for (int i = 0; i < nvr; ++i) vl_out[(size_t)(k - 1) * nvr + i] = coor[(size_t)(k - 1) * nvr + i];
+    }
+  });
+}
+
+// CPU baseline: nchains independent canonical chains (each a copy of h with
+// its own MT seed seeds[c] and beta betas[c]) run for nsweeps sweeps from
+// their current variables, spread over nthreads host threads.  Returns the
+// wall time in seconds; energies in eol_out[nchains].
+double orc_bench_chains(void* h, int nchains, const int* seeds, const double* betas, int nsweeps,
+                        int nthreads, double* eol_out) {
+  std::vector<std::unique_ptr<Smmp>> chains;
+  for (int c = 0; c < nchains; ++c) {
+    chains.emplace_back(new Smmp(*S(h)));
+    chains.back()->sgrnd(seeds[c]);
+    chains.back()->beta = betas[c];
+  }
+  auto t0 = std::chrono::steady_clock::now();
+  std::vector<std::thread> th;
+  if (nthreads < 1) nthreads = 1;
+  for (int t = 0; t < nthreads; ++t)
+    th.emplace_back([&, t] {
+      Smmp::Weight w;
+      for (int c = t; c < nchains; c += nthreads) {
+        Smmp* s = chains[c].get();
+        double eol = s->energy(), acz = 0.0;
+        try {
+          for (int k = 0; k < nsweeps; ++k) s->metropolis(eol, acz, w);
+        } catch (...) {
+          eol = NAN;
+        }
+        eol_out[c] = eol;
+      }
+    });
+  for (auto& t : th) t.join();
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+}  // extern "C"

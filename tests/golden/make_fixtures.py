@@ -1,0 +1,77 @@
+"""Generate the input fixtures and published golden values used by the tests.
+
+Run once in a container that has the SMMP reference mounted (the GPU box does
+not): it copies the ECEPP residue libraries, the SASA sphere points and the
+Met-enkephalin input decks into tests/golden/smmp_data/, and records the
+reference's published numbers (README and EXAMPLES/annealing.out) with their
+sources in tests/golden/golden.json.
+
+    python tests/golden/make_fixtures.py /root/reference/trunk
+"""
+import json
+import os
+import shutil
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+DATA = [
+    ("SMMP/lib.sh3", "lib.sh3"),        # ECEPP/3 residue library
+    ("SMMP/lib.sh2", "lib.sh2"),        # ECEPP/2 residue library
+    ("SMMP/tes.dat", "tes.dat"),        # 122 unit-sphere points (enysol)
+    ("EXAMPLES/enkefa.seq", "enkefa.seq"),
+    ("EXAMPLES/enkefa.var", "enkefa.var"),
+    ("EXAMPLES/enkefa.ann", "enkefa.ann"),
+    ("EXAMPLES/temperatures", "temperatures"),
+]
+
+
+def read_lines(path):
+    with open(path) as f:
+        return f.read().split("\n")
+
+
+def main(ref):
+    out = os.path.join(HERE, "smmp_data")
+    os.makedirs(out, exist_ok=True)
+    for src, dst in DATA:
+        shutil.copyfile(os.path.join(ref, src), os.path.join(out, dst))
+
+    readme = read_lines(os.path.join(ref, "README"))
+    ann = read_lines(os.path.join(ref, "EXAMPLES/annealing.out"))
+
+    def fnum(s):
+        return float(s.replace("D", "E"))
+
+    # README:391-393  "Total:  0.10354E+04" / "Coulomb: ... HB: ..." / "Variables: ..."
+    l391, l392, l393 = readme[390].split(), readme[391].split(), readme[392].split()
+    golden = {
+        "enkefa_ecepp3": {
+            "source": "README:389-393",
+            "setup": "enkefa.seq + enkefa.var, nh2/cooh, ECEPP/3, epsd=.false., itysol=0",
+            "total": fnum(l391[1]),
+            "coulomb": fnum(l392[1]),
+            "lennard_jones": fnum(l392[3]),
+            "hbond": fnum(l392[5]),
+            "torsion": fnum(l393[1]),
+            "digits": 4,
+        },
+        "anneal_ecepp2": {
+            "source": "EXAMPLES/annealing.out:14-45; EXAMPLES/annealing.f:37-72",
+            "setup": "enkefa.seq + enkefa.ann, nh2/cooh, ECEPP/2, seed 81236, "
+                     "nequi=100, nswp=100000, tmax=1000, tmin=100, lrand",
+            "start": fnum(ann[13].split(":")[1]),
+            "after_equilibration": fnum(ann[15].split(":")[1]),
+            "acceptance": fnum(ann[16].split(":")[1]),
+            "last": fnum(ann[18].split()[-1]),
+            "lowest": fnum(ann[44].split()[-1]),
+            "lowest_sweep": int(ann[44].split()[-2]),
+        },
+    }
+    with open(os.path.join(HERE, "golden.json"), "w") as f:
+        json.dump(golden, f, indent=1)
+    print(json.dumps(golden, indent=1))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/trunk")
