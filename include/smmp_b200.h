@@ -1,0 +1,202 @@
+/*
+ * smmp_b200.h -- C ABI of the B200 implementation of SMMP's energy-and-sweep
+ * path (libsmmp_b200.so).
+ *
+ * Two layers:
+ *
+ *  1. The reference-facing layer.  One global system, as SMMP keeps its state
+ *     in COMMON blocks; each entry point replaces the f2py binding of the
+ *     reference routine cited beside it (trunk/smmp.pyf, trunk/<file>.f).
+ *     Angles are radians, energies kcal/mol, variables 0-based arrays over
+ *     all variables of the system (the reference's vlvr(1..ntlvr)).
+ *
+ *  2. The batched layer.  Independent molecules (smmp_mol_*) and ensembles of
+ *     chains / replicas (smmp_ens_*) whose whole state stays on the GPU; this
+ *     has no single counterpart in the reference -- it replaces the loops of
+ *     partem_s.f and canon.f over many replicas.
+ *
+ * Every function returning int returns 0 on success and a nonzero status on
+ * failure; smmp_last_error() then describes the failure (thread-local).  The
+ * library never aborts the process where the reference would STOP.
+ */
+#ifndef SMMP_B200_H
+#define SMMP_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define SMMP_OK 0
+#define SMMP_ERR_ARG 1       /* invalid argument or call order */
+#define SMMP_ERR_INPUT 2     /* unreadable / inconsistent input files */
+#define SMMP_ERR_CUDA 3      /* CUDA runtime error or no usable GPU */
+#define SMMP_ERR_KERNEL 4    /* a kernel reported an error word (see below) */
+
+/* Per-chain error words reported by the kernels (smmp_ens_errors). */
+#define SMMP_KERR_NONFINITE 1     /* NaN/Inf energy */
+#define SMMP_KERR_CONSISTENCY 2   /* |E_incremental - E_fresh| > tolerance at sweep end */
+#define SMMP_KERR_NEIGHBOURS 3    /* SASA neighbour buffer overflow */
+#define SMMP_KERR_TIMEOUT 4       /* a bounded wait gave up */
+
+/* Switches of the reference's COMMON blocks /epar_l/ (sh2, epsd, ientyp),
+ * /isolty/ (itysol) and /updchois/ (rndord, upchswitch); INCL.H:224-327.
+ * Only ientyp=0 (ECEPP/2-3), itysol in {0..9}, upchswitch=0 are on this path. */
+typedef struct smmp_config {
+  int sh2;        /* 1: ECEPP/2 library (lib.sh2), 0: ECEPP/3 (lib.sh3) */
+  int epsd;       /* 1: sigmoidal distance-dependent dielectric */
+  int itysol;     /* 0: vacuum, 1..9: numerical SASA solvation model */
+  int ientyp;     /* must be 0 (ECEPP) */
+  int rndord;     /* 1: random variable order in a sweep */
+  int upchswitch; /* must be 0 (no biased Gaussian steps) */
+} smmp_config_t;
+
+/* Sampling weight W(E) of metropolis (its `dummy` callback argument,
+ * smmp.pyf:3-10): kind 0 = can_weight beta*E (canon.f:135-149);
+ * 1 = muca_weight (beta+b[k])*E+alpha[k]; 2 = muca_weight2 b[k]*E+alpha[k]
+ * (mulcan_par_mod.f90:380-410), k = int(clamp(E/ebin+sign(1/2,E),kmin,kmax)),
+ * b and alpha indexed k-kmin; 3 = host callback (callback(E, user)). */
+typedef double (*smmp_weight_fn)(double energy, void* user);
+typedef struct smmp_weight {
+  int kind;
+  int kmin, kmax;
+  double ebin;
+  const double* b;
+  const double* alpha;
+  smmp_weight_fn callback;
+  void* user;
+} smmp_weight_t;
+
+const char* smmp_last_error(void);
+/* 1 if a CUDA device is usable by this library. */
+int smmp_gpu_available(void);
+
+/* ---------------------------------------------------------------- layer 1 */
+
+/* Drop the global system (molecule, GPU state, switches, stream), as a
+ * fresh process of the reference starts from its BLOCK DATA defaults. */
+int smmp_reset(void);
+
+int smmp_set_config(const smmp_config_t* cfg);   /* write the COMMON switches */
+int smmp_get_config(smmp_config_t* cfg);
+
+/* init_energy(libdir): smmp.pyf:4404, init_energy.f:14.  libdir holds
+ * lib.sh3 / lib.sh2 and tes.dat. */
+int smmp_init_energy(const char* libdir);
+
+/* init_molecule(iabin, grpn, grpc, seqfile, varfile): smmp.pyf:5011-5016,
+ * init_molecule.f:13.  iabin must be 1 (sequence + variables); PDB input is
+ * outside this path.  varfile may be NULL or blank. */
+int smmp_init_molecule(int iabin, const char* grpn, const char* grpc, const char* seqfile,
+                       const char* varfile);
+
+/* energy(): smmp.pyf:380, energy.f:12.  Uses the current variables (as
+ * written by smmp_set_vlvr or a previous call) and updates the dihedral
+ * state as setvar does. */
+int smmp_energy(double* e_out);
+/* Terms of the last energy evaluation: eyel, eyvw, eyhb, eyvr, eysl, eysm
+ * (COMMON /eny_r/, INCL.H:343-349). */
+int smmp_energy_terms(double terms[6]);
+
+/* setvar(nml, vlvrx): smmp.pyf:949-950, setvar.f:13.  Sets the variables of
+ * molecule nml (1-based) and rebuilds its coordinates. */
+int smmp_setvar(int nml, const double* vlvrx);
+
+/* metropolis(eol1, acz, dummy): smmp.pyf:22-25, metropolis.f:13.  One sweep;
+ * eol and acz are updated in place as the f2py intent(in,out) arguments. */
+int smmp_metropolis(double* eol, double* acz, const smmp_weight_t* w);
+
+/* sgrnd(seed) / grnd(): smmp.pyf:5620, twister.f:64 and :104. */
+int smmp_sgrnd(int32_t seed);
+double smmp_grnd(void);
+
+/* canon(nequi, nswp, nmes, temp, lrand): smmp.pyf:3522-3527, canon.f:12.
+ * Energies after every nmes-th sweep are written to trace (if not NULL,
+ * nswp/nmes+1 values); out[0..2] = energy after equilibration, acceptance
+ * rate, last energy (if out is not NULL). */
+int smmp_canon(int nequi, int nswp, int nmes, double temp, int lrand, double* trace,
+               double* out);
+
+/* anneal(nequi, nswp, nmes, tmax, tmin, lrand): smmp.pyf:2663, anneal.f:13.
+ * out[0..5] = start energy, energy after equilibration, acceptance, last
+ * energy, lowest energy, sweep of the lowest energy. */
+int smmp_anneal(int nequi, int nswp, int nmes, double tmax, double tmin, int lrand, double* out);
+
+/* COMMON views: /bet/ beta, /mol_par/ nvr, /var_r/ vlvr axvr, /var_i/ idvr. */
+int smmp_set_beta(double beta);
+double smmp_get_beta(void);
+int smmp_get_sizes(int* natoms, int* ntlvr, int* nvr);
+int smmp_get_vlvr(double* vlvr);          /* [ntlvr] */
+int smmp_set_vlvr(const double* vlvr);    /* [ntlvr] */
+int smmp_get_idvr(int* idvr);             /* [nvr], 1-based variable indices */
+int smmp_get_axvr(double* axvr);          /* [ntlvr] */
+int smmp_get_coords(double* xyz);         /* [natoms*3] after a rebuild */
+int smmp_get_acceptance(long long* ncalls, long long* nacalls);   /* /updstats/ */
+
+/* ---------------------------------------------------------------- layer 2 */
+
+typedef struct smmp_mol smmp_mol_t;
+typedef struct smmp_ens smmp_ens_t;
+
+/* Assemble one molecule (init_energy + init_molecule on a private system). */
+smmp_mol_t* smmp_mol_build(const char* libdir, const smmp_config_t* cfg, const char* seqfile,
+                           const char* varfile, const char* grpn, const char* grpc);
+void smmp_mol_free(smmp_mol_t* m);
+/* info[0..5] = natoms, nvar (all), nvr (free), pair terms per evaluation,
+ * number of heavy (SASA) atoms, residues. */
+int smmp_mol_info(const smmp_mol_t* m, long long info[6]);
+
+/* An ensemble of nchains chains; chain c is a copy of mols[chain_mol[c]].
+ * betas[c] is its inverse temperature.  shared_stream=0: chain c draws from
+ * its own MT19937 stream seeded seeds[c]; shared_stream=1: all chains share
+ * one stream (seeds[0]) and one dihedral state, visited in turn as partem_s.f
+ * does.  flags: SMMP_ENS_FP32 selects FP32 pair terms (FP64 guard and
+ * accumulation); otherwise pair terms are FP64. */
+#define SMMP_ENS_FP32 2
+#define SMMP_ENS_RNDORD 1
+smmp_ens_t* smmp_ens_create(smmp_mol_t* const* mols, int nmols, const int* chain_mol,
+                            int nchains, const int* seeds, const double* betas,
+                            int shared_stream, int flags);
+void smmp_ens_free(smmp_ens_t* e);
+/* Launch the ensemble's work on a caller's cudaStream_t (NULL: the
+ * ensemble's own stream), e.g. to time it with events on that stream. */
+int smmp_ens_set_stream(smmp_ens_t* e, void* stream);
+int smmp_ens_random_start(smmp_ens_t* e);          /* canon.f:60-67 per chain */
+int smmp_ens_energy(smmp_ens_t* e, double* eol);   /* energy() of every chain */
+/* Per-chain start of partem_s.f:134-162: energy() then nequi sweeps of
+ * each chain at its own beta, chains in order (one after another when they
+ * share a stream). */
+int smmp_ens_equilibrate(smmp_ens_t* e, int nequi);
+/* nsweeps metropolis sweeps of every chain with weight w (NULL: canonical). */
+int smmp_ens_sweeps(smmp_ens_t* e, int nsweeps, const smmp_weight_t* w);
+/* Parallel tempering: betas[k] of temperature label k (chain k starts at
+ * label k); wrap=1 pairs label n with 1 (partem_s.f:222). */
+int smmp_ens_set_pt(smmp_ens_t* e, const double* betas, int wrap, int exchange_seed);
+/* nsweeps of (one sweep of every chain, then one exchange).  serial=1 visits
+ * chains one at a time in label order (the partem_s.f schedule); serial=0
+ * runs all chains at once, captured in CUDA graphs of graph_chunk sweeps. */
+int smmp_ens_pt_sweeps(smmp_ens_t* e, int nsweeps, int serial, int graph_chunk);
+int smmp_ens_pt_map(smmp_ens_t* e, int* temp_chain);   /* ipoi, 0-based chains */
+int smmp_ens_sizes(smmp_ens_t* e, int* nchains, int* vstride, int* tstride);
+int smmp_ens_get_energies(smmp_ens_t* e, double* eol);          /* [nchains] */
+int smmp_ens_get_terms(smmp_ens_t* e, double* terms);           /* [nchains*6] */
+int smmp_ens_get_vlvr(smmp_ens_t* e, double* vlvr);             /* [nchains*vstride] */
+int smmp_ens_set_vlvr(smmp_ens_t* e, const double* vlvr);
+int smmp_ens_get_betas(smmp_ens_t* e, double* betas);
+int smmp_ens_get_coords(smmp_ens_t* e, double* xyz);            /* [nchains*3*tstride] */
+int smmp_ens_acceptance(smmp_ens_t* e, unsigned long long* acc, unsigned long long* prop);
+int smmp_ens_errors(smmp_ens_t* e, int* err);                   /* [nchains] */
+/* Draw n numbers from MT stream slot (grnd of that stream). */
+int smmp_ens_draw(smmp_ens_t* e, int slot, int n, double* out);
+/* Checkpoint: variables, dihedral state, MT19937 states, betas, energies and
+ * the PT map, so that a restored ensemble continues bit-identically.
+ * smmp_ens_checkpoint with buf=NULL returns the size in *bytes. */
+int smmp_ens_checkpoint(smmp_ens_t* e, void* buf, uint64_t* bytes);
+int smmp_ens_restore(smmp_ens_t* e, const void* buf, uint64_t bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SMMP_B200_H */

@@ -1,0 +1,852 @@
+// C ABI of libsmmp_b200.so (include/smmp_b200.h).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/smmp_b200.h"
+#include "runtime.hpp"
+
+using namespace smmpb200;
+
+namespace {
+
+thread_local std::string g_err;
+
+template <class F>
+int guard(F&& f) {
+  try {
+    f();
+    return SMMP_OK;
+  } catch (const std::invalid_argument& e) {
+    g_err = e.what();
+    return SMMP_ERR_ARG;
+  } catch (const std::runtime_error& e) {
+    g_err = e.what();
+    std::string w = e.what();
+    if (w.find("cuda") != std::string::npos || w.find("CUDA") != std::string::npos ||
+        w.find("H2D") != std::string::npos || w.find("D2H") != std::string::npos ||
+        w.find("sync") != std::string::npos)
+      return SMMP_ERR_CUDA;
+    if (w.find("kernel error") != std::string::npos) return SMMP_ERR_KERNEL;
+    return SMMP_ERR_INPUT;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return SMMP_ERR_ARG;
+  }
+}
+
+void need(bool ok, const char* msg) {
+  if (!ok) throw std::invalid_argument(msg);
+}
+
+Config to_cfg(const smmp_config_t* c) {
+  Config k;
+  if (c) {
+    k.sh2 = c->sh2;
+    k.epsd = c->epsd;
+    k.itysol = c->itysol;
+    k.ientyp = c->ientyp;
+    k.rndord = c->rndord;
+    k.upchswitch = c->upchswitch;
+  }
+  need(k.ientyp == 0, "only ientyp=0 (ECEPP) is on this path");
+  need(k.upchswitch == 0, "biased Gaussian steps (upchswitch!=0) are outside this path");
+  need(k.itysol >= 0 && k.itysol <= 9, "itysol must be 0 (vacuum) or a numerical SASA model 1..9");
+  return k;
+}
+
+DWeight to_dweight(const smmp_weight_t* w, std::vector<void*>& tmp) {
+  DWeight d{kWeightCanon, 0, 0, 1.0, nullptr, nullptr};
+  if (!w || w->kind == 0) return d;
+  need(w->kind == 1 || w->kind == 2, "weight kind must be 0, 1 or 2 on the GPU path");
+  need(w->kmax >= w->kmin && w->b && w->alpha && w->ebin != 0.0, "bad multicanonical table");
+  size_t n = (size_t)(w->kmax - w->kmin + 1);
+  double *b = nullptr, *a = nullptr;
+  check_cuda(cudaMalloc(&b, n * sizeof(double)), "cudaMalloc");
+  tmp.push_back(b);
+  check_cuda(cudaMalloc(&a, n * sizeof(double)), "cudaMalloc");
+  tmp.push_back(a);
+  check_cuda(cudaMemcpy(b, w->b, n * sizeof(double), cudaMemcpyHostToDevice), "H2D");
+  check_cuda(cudaMemcpy(a, w->alpha, n * sizeof(double), cudaMemcpyHostToDevice), "H2D");
+  d.kind = w->kind;
+  d.kmin = w->kmin;
+  d.kmax = w->kmax;
+  d.ebin = w->ebin;
+  d.b = b;
+  d.alpha = a;
+  return d;
+}
+
+struct TmpFree {
+  std::vector<void*> p;
+  ~TmpFree() {
+    for (void* q : p) cudaFree(q);
+  }
+};
+
+void raise_kernel_errors(Ensemble& e) {
+  std::vector<int> err;
+  e.get_errors(err);
+  for (size_t c = 0; c < err.size(); ++c)
+    if (err[c] != 0)
+      throw std::runtime_error("kernel error " + std::to_string(err[c]) + " on chain " +
+                               std::to_string(c));
+}
+
+// ------------------------------------------------------------------ host MT19937
+// The global stream of the reference-facing layer exists before any molecule
+// (main programs call sgrnd before init_molecule).  Until a molecule is on
+// the GPU it is advanced here; afterwards the GPU copy is authoritative.
+struct HostMT {
+  uint32_t mt[625];
+  HostMT() {
+    std::memset(mt, 0, sizeof mt);
+    mt[624] = 625;
+  }
+  void seed(uint32_t s) {
+    mt[0] = s;
+    for (int i = 1; i < 624; ++i) mt[i] = 69069u * mt[i - 1];
+    mt[624] = 624;
+  }
+  double next() {
+    if (mt[624] >= 624) {
+      if (mt[624] == 625) seed(4357u);
+      const uint32_t MATA = 0x9908B0DFu, UM = 0x80000000u, LM = 0x7fffffffu;
+      int kk = 0;
+      uint32_t y;
+      for (; kk < 227; ++kk) {
+        y = (mt[kk] & UM) | (mt[kk + 1] & LM);
+        mt[kk] = mt[kk + 397] ^ (y >> 1) ^ ((y & 1u) ? MATA : 0u);
+      }
+      for (; kk < 623; ++kk) {
+        y = (mt[kk] & UM) | (mt[kk + 1] & LM);
+        mt[kk] = mt[kk - 227] ^ (y >> 1) ^ ((y & 1u) ? MATA : 0u);
+      }
+      y = (mt[623] & UM) | (mt[0] & LM);
+      mt[623] = mt[396] ^ (y >> 1) ^ ((y & 1u) ? MATA : 0u);
+      mt[624] = 0;
+    }
+    uint32_t y = mt[mt[624]++];
+    y ^= (y >> 11);
+    y ^= (y << 7) & 0x9D2C5680u;
+    y ^= (y << 15) & 0xEFC60000u;
+    y ^= (y >> 18);
+    return (double)y / 4294967295.0;
+  }
+};
+
+constexpr double kPi = 3.141592653589793;
+double h_wrap(double d) {
+  d = std::fmod(d, 2.0 * kPi);
+  return std::fabs(d) <= kPi ? d : d - std::copysign(2.0 * kPi, d);
+}
+
+// ------------------------------------------------------------------ global system
+struct Universe {
+  Config cfg;
+  std::string libdir;
+  bool energy_ready = false;
+  std::shared_ptr<Molecule> mol;
+  std::unique_ptr<Ensemble> ens;
+  HostMT mt;
+  double beta = 0.0;
+  double terms[6] = {0, 0, 0, 0, 0, 0};
+  long long ncalls = 0, nacalls = 0;
+};
+Universe& U() {
+  static Universe u;
+  return u;
+}
+
+void require_molecule() {
+  need(U().ens != nullptr, "call smmp_init_molecule first");
+}
+
+void sync_beta() {
+  Universe& u = U();
+  u.ens->set_betas(std::vector<double>{u.beta});
+}
+
+double universe_energy() {
+  Universe& u = U();
+  u.ens->energy(false);
+  raise_kernel_errors(*u.ens);
+  std::vector<double> e, t;
+  u.ens->get_eol(e);
+  u.ens->get_terms(t);
+  for (int k = 0; k < 6; ++k) u.terms[k] = t[k];
+  return e[0];
+}
+
+double universe_grnd() {
+  Universe& u = U();
+  if (!u.ens) return u.mt.next();
+  std::vector<double> out;
+  u.ens->draw(0, 1, out);
+  return out[0];
+}
+
+// metropolis with a host weight callback: proposals driven from the host,
+// every energy on the GPU (metropolis.f:13-184).
+void metropolis_callback(double* eol1, double* acz, const smmp_weight_t* w) {
+  Universe& u = U();
+  const MolTopo& t = u.mol->topo;
+  auto W = [&](double x) { return w->callback(x, w->user); };
+  std::vector<double> vl;
+  double eol = universe_energy();
+  for (int nsw = 0; nsw < t.nfree; ++nsw) {
+    int ivar = u.cfg.rndord ? (int)(t.nfree * universe_grnd()) : nsw;
+    if (ivar >= t.nfree) ivar = t.nfree - 1;
+    int jv = t.idvr[ivar];
+    u.ens->get_vlvr(vl);
+    double vold = vl[jv];
+    double dv = t.axvr[jv] * (universe_grnd() - 0.5);
+    vl[jv] = h_wrap(vold + dv);
+    u.ens->set_vlvr(vl);
+    double enw = universe_energy();
+    double delta = W(enw) - W(eol);
+    int up = 0;
+    if (delta <= 0.0) {
+      up = 1;
+    } else {
+      double rd = universe_grnd();
+      delta = std::fmin(delta, 100.0);
+      if (std::exp(-delta) >= rd) up = 1;
+    }
+    if (up) {
+      eol = enw;
+    } else {
+      vl[jv] = vold;
+      u.ens->set_vlvr(vl);
+    }
+    *acz += up;
+    ++u.ncalls;
+    u.nacalls += up;
+  }
+  double enw = universe_energy();
+  if (std::fabs(eol - enw) > 1e-6 && eol < 100000)
+    throw std::runtime_error("metropolis: eol and enw difference unacceptable");
+  *eol1 = eol;
+}
+
+}  // namespace
+
+// ============================================================================ layer 1
+extern "C" {
+
+const char* smmp_last_error(void) { return g_err.c_str(); }
+
+int smmp_gpu_available(void) {
+  int n = 0;
+  return cudaGetDeviceCount(&n) == cudaSuccess && n > 0 ? 1 : 0;
+}
+
+int smmp_reset(void) {
+  return guard([&] {
+    Universe& u = U();
+    u.ens.reset();
+    u.mol.reset();
+    u.cfg = Config();
+    u.libdir.clear();
+    u.energy_ready = false;
+    u.mt = HostMT();
+    u.beta = 0.0;
+    for (double& t : u.terms) t = 0.0;
+    u.ncalls = u.nacalls = 0;
+  });
+}
+
+int smmp_set_config(const smmp_config_t* cfg) {
+  return guard([&] {
+    need(cfg != nullptr, "cfg is NULL");
+    U().cfg = to_cfg(cfg);
+  });
+}
+
+int smmp_get_config(smmp_config_t* cfg) {
+  return guard([&] {
+    need(cfg != nullptr, "cfg is NULL");
+    const Config& k = U().cfg;
+    cfg->sh2 = k.sh2;
+    cfg->epsd = k.epsd;
+    cfg->itysol = k.itysol;
+    cfg->ientyp = k.ientyp;
+    cfg->rndord = k.rndord;
+    cfg->upchswitch = k.upchswitch;
+  });
+}
+
+int smmp_init_energy(const char* libdir) {
+  return guard([&] {
+    need(libdir != nullptr, "libdir is NULL");
+    Universe& u = U();
+    std::string d = libdir;
+    if (!d.empty() && d.back() != '/') d += '/';
+    // validate: the library must be readable now, as init_energy reads it
+    Assembly probe;
+    probe.sh2 = u.cfg.sh2 != 0;
+    probe.itysol = u.cfg.itysol;
+    probe.epsd = u.cfg.epsd != 0;
+    probe.init_energy(d);
+    u.libdir = d;
+    u.energy_ready = true;
+  });
+}
+
+int smmp_init_molecule(int iabin, const char* grpn, const char* grpc, const char* seqfile,
+                       const char* varfile) {
+  return guard([&] {
+    Universe& u = U();
+    need(u.energy_ready, "call smmp_init_energy first");
+    need(iabin == 1, "only iabin=1 (sequence + variable files) is on this path");
+    need(seqfile != nullptr, "seqfile is NULL");
+    need(u.mol == nullptr, "one molecule per system on this path");
+    need(smmp_gpu_available() == 1, "no CUDA device available");
+    std::string var = varfile ? varfile : "";
+    u.mol = build_molecule(u.libdir, u.cfg, seqfile, var, grpn ? grpn : "nh2",
+                           grpc ? grpc : "cooh");
+    u.ens.reset(new Ensemble({u.mol}, {0}, {4357}, {u.beta}, true));
+    std::vector<uint32_t> mt(u.mt.mt, u.mt.mt + 625);
+    u.ens->set_mt(mt);
+  });
+}
+
+int smmp_energy(double* e_out) {
+  return guard([&] {
+    require_molecule();
+    double e = universe_energy();
+    if (e_out) *e_out = e;
+  });
+}
+
+int smmp_energy_terms(double terms[6]) {
+  return guard([&] {
+    need(terms != nullptr, "terms is NULL");
+    for (int k = 0; k < 6; ++k) terms[k] = U().terms[k];
+  });
+}
+
+int smmp_setvar(int nml, const double* vlvrx) {
+  return guard([&] {
+    require_molecule();
+    need(nml == 1, "molecule index out of range");
+    need(vlvrx != nullptr, "vlvrx is NULL");
+    Universe& u = U();
+    int nv = u.mol->topo.nvar;
+    std::vector<double> vl((size_t)u.ens->vstride(), 0.0);
+    std::copy(vlvrx, vlvrx + nv, vl.begin());
+    u.ens->set_vlvr(vl);
+    universe_energy();   // setvar + bldmol (the energy terms are refreshed too)
+  });
+}
+
+int smmp_metropolis(double* eol, double* acz, const smmp_weight_t* w) {
+  return guard([&] {
+    require_molecule();
+    need(eol != nullptr && acz != nullptr, "eol/acz is NULL");
+    Universe& u = U();
+    if (w && w->kind == 3) {
+      need(w->callback != nullptr, "weight callback is NULL");
+      metropolis_callback(eol, acz, w);
+      return;
+    }
+    TmpFree tmp;
+    DWeight dw = to_dweight(w, tmp.p);
+    sync_beta();
+    std::vector<unsigned long long> a0, p0, a1, p1;
+    u.ens->get_acceptance(a0, p0);
+    int flags = u.cfg.rndord ? kFlagRndOrd : 0;
+    u.ens->sweeps(1, flags, dw);
+    raise_kernel_errors(*u.ens);
+    u.ens->get_acceptance(a1, p1);
+    std::vector<double> e, t;
+    u.ens->get_eol(e);
+    u.ens->get_terms(t);
+    for (int k = 0; k < 6; ++k) u.terms[k] = t[k];
+    *eol = e[0];
+    *acz += (double)(a1[0] - a0[0]);
+    u.ncalls += (long long)(p1[0] - p0[0]);
+    u.nacalls += (long long)(a1[0] - a0[0]);
+  });
+}
+
+int smmp_sgrnd(int32_t seed) {
+  return guard([&] {
+    Universe& u = U();
+    u.mt.seed((uint32_t)seed);
+    if (u.ens) u.ens->set_mt(std::vector<uint32_t>(u.mt.mt, u.mt.mt + 625));
+  });
+}
+
+double smmp_grnd(void) {
+  double r = NAN;
+  int st = guard([&] { r = universe_grnd(); });
+  return st == SMMP_OK ? r : NAN;
+}
+
+int smmp_canon(int nequi, int nswp, int nmes, double temp, int lrand, double* trace, double* out) {
+  return guard([&] {
+    require_molecule();
+    need(temp > 0 && nmes > 0 && nequi >= 0 && nswp >= 0, "bad canon arguments");
+    Universe& u = U();
+    u.beta = 1.0 / (temp * 1.98773e-3);
+    sync_beta();
+    if (lrand) u.ens->random_start();
+    universe_energy();
+    int flags = u.cfg.rndord ? kFlagRndOrd : 0;
+    DWeight w{kWeightCanon, 0, 0, 1.0, nullptr, nullptr};
+    std::vector<unsigned long long> a0, p0, a1, p1;
+    int k = 0;
+    if (nequi > 0) u.ens->sweeps(nequi, flags, w);
+    raise_kernel_errors(*u.ens);
+    std::vector<double> e;
+    u.ens->get_eol(e);
+    double after_equi = e[0];
+    u.ens->get_acceptance(a0, p0);
+    // sweeps nsw = 0..nswp (canon.f:85-115), measuring when mod(nsw, nmes) == 0
+    int nsw = 0;
+    while (nsw <= nswp) {
+      int next_meas = ((nsw + nmes - 1) / nmes) * nmes;
+      int upto = std::min(next_meas, nswp);
+      u.ens->sweeps(upto - nsw + 1, flags, w);
+      raise_kernel_errors(*u.ens);
+      nsw = upto + 1;
+      if (trace && upto % nmes == 0) {
+        u.ens->get_eol(e);
+        trace[k++] = e[0];
+      }
+    }
+    u.ens->get_acceptance(a1, p1);
+    u.ens->get_eol(e);
+    if (out) {
+      out[0] = after_equi;
+      out[1] = (double)(a1[0] - a0[0]) / ((double)(nswp + 1) * u.mol->topo.nfree);
+      out[2] = e[0];
+    }
+    u.ncalls += (long long)(p1[0] - p0[0]);
+    u.nacalls += (long long)(a1[0] - a0[0]);
+  });
+}
+
+int smmp_anneal(int nequi, int nswp, int nmes, double tmax, double tmin, int lrand, double* out) {
+  return guard([&] {
+    require_molecule();
+    need(tmax > 0 && tmin > 0 && nswp > 0, "bad anneal arguments");
+    (void)nmes;
+    Universe& u = U();
+    double bmin = 1.0 / (tmax * 1.98773e-3), bmax = 1.0 / (tmin * 1.98773e-3);
+    double db = std::exp(std::log(bmax / bmin) / nswp);
+    if (lrand) u.ens->random_start();
+    double e0 = universe_energy();
+    int flags = u.cfg.rndord ? kFlagRndOrd : 0;
+    DWeight w{kWeightCanon, 0, 0, 1.0, nullptr, nullptr};
+    u.beta = bmin;
+    sync_beta();
+    if (nequi > 0) u.ens->sweeps(nequi, flags, w);
+    std::vector<double> e;
+    u.ens->get_eol(e);
+    double after = e[0];
+    std::vector<unsigned long long> a0, p0, a1, p1;
+    u.ens->get_acceptance(a0, p0);
+    double ymin = after;
+    int nemin = 0;
+    for (int nsw = 0; nsw <= nswp; ++nsw) {
+      u.beta = bmin * std::pow(db, nsw);
+      sync_beta();
+      u.ens->sweeps(1, flags, w);
+      u.ens->get_eol(e);
+      if (e[0] < ymin) {
+        ymin = e[0];
+        nemin = nsw;
+      }
+    }
+    raise_kernel_errors(*u.ens);
+    u.ens->get_acceptance(a1, p1);
+    if (out) {
+      out[0] = e0;
+      out[1] = after;
+      out[2] = (double)(a1[0] - a0[0]) / ((double)(nswp + 1) * u.mol->topo.nfree);
+      out[3] = e[0];
+      out[4] = ymin;
+      out[5] = nemin;
+    }
+  });
+}
+
+int smmp_set_beta(double beta) {
+  return guard([&] {
+    U().beta = beta;
+    if (U().ens) sync_beta();
+  });
+}
+double smmp_get_beta(void) { return U().beta; }
+
+int smmp_get_sizes(int* natoms, int* ntlvr, int* nvr) {
+  return guard([&] {
+    require_molecule();
+    const MolTopo& t = U().mol->topo;
+    if (natoms) *natoms = t.natoms;
+    if (ntlvr) *ntlvr = t.nvar;
+    if (nvr) *nvr = t.nfree;
+  });
+}
+
+int smmp_get_vlvr(double* vlvr) {
+  return guard([&] {
+    require_molecule();
+    std::vector<double> v;
+    U().ens->get_vlvr(v);
+    std::copy(v.begin(), v.begin() + U().mol->topo.nvar, vlvr);
+  });
+}
+
+int smmp_set_vlvr(const double* vlvr) {
+  return guard([&] {
+    require_molecule();
+    std::vector<double> v((size_t)U().ens->vstride(), 0.0);
+    std::copy(vlvr, vlvr + U().mol->topo.nvar, v.begin());
+    U().ens->set_vlvr(v);
+  });
+}
+
+int smmp_get_idvr(int* idvr) {
+  return guard([&] {
+    require_molecule();
+    const MolTopo& t = U().mol->topo;
+    for (int i = 0; i < t.nfree; ++i) idvr[i] = t.idvr[i] + 1;
+  });
+}
+
+int smmp_get_axvr(double* axvr) {
+  return guard([&] {
+    require_molecule();
+    const MolTopo& t = U().mol->topo;
+    std::copy(t.axvr.begin(), t.axvr.end(), axvr);
+  });
+}
+
+int smmp_get_coords(double* xyz) {
+  return guard([&] {
+    require_molecule();
+    std::vector<double> c;
+    U().ens->get_coords(c);
+    std::copy(c.begin(), c.begin() + 3 * U().mol->topo.natoms, xyz);
+  });
+}
+
+int smmp_get_acceptance(long long* ncalls, long long* nacalls) {
+  return guard([&] {
+    if (ncalls) *ncalls = U().ncalls;
+    if (nacalls) *nacalls = U().nacalls;
+  });
+}
+
+}  // extern "C"
+
+// ============================================================================ layer 2
+
+struct smmp_mol {
+  std::shared_ptr<Molecule> m;
+};
+struct smmp_ens {
+  std::unique_ptr<Ensemble> e;
+  int flags = 0;
+};
+
+extern "C" {
+
+smmp_mol_t* smmp_mol_build(const char* libdir, const smmp_config_t* cfg, const char* seqfile,
+                           const char* varfile, const char* grpn, const char* grpc) {
+  smmp_mol_t* out = nullptr;
+  guard([&] {
+    need(libdir && seqfile, "libdir/seqfile is NULL");
+    auto m = build_molecule(libdir, to_cfg(cfg), seqfile, varfile ? varfile : "",
+                            grpn ? grpn : "nh2", grpc ? grpc : "cooh");
+    out = new smmp_mol{m};
+  });
+  return out;
+}
+
+void smmp_mol_free(smmp_mol_t* m) { delete m; }
+
+int smmp_mol_info(const smmp_mol_t* m, long long info[6]) {
+  return guard([&] {
+    need(m && info, "NULL argument");
+    const MolTopo& t = m->m->topo;
+    info[0] = t.natoms;
+    info[1] = t.nvar;
+    info[2] = t.nfree;
+    info[3] = t.npairs;
+    info[4] = (long long)t.heavy.size();
+    info[5] = t.nres;
+  });
+}
+
+smmp_ens_t* smmp_ens_create(smmp_mol_t* const* mols, int nmols, const int* chain_mol,
+                            int nchains, const int* seeds, const double* betas,
+                            int shared_stream, int flags) {
+  smmp_ens_t* out = nullptr;
+  guard([&] {
+    need(mols && nmols > 0 && chain_mol && nchains > 0 && seeds && betas, "NULL argument");
+    need(smmp_gpu_available() == 1, "no CUDA device available");
+    std::vector<std::shared_ptr<Molecule>> ms;
+    for (int i = 0; i < nmols; ++i) {
+      need(mols[i] != nullptr, "NULL molecule");
+      ms.push_back(mols[i]->m);
+    }
+    std::vector<int> cm(chain_mol, chain_mol + nchains);
+    int ns = shared_stream ? 1 : nchains;
+    std::vector<int> sd(seeds, seeds + ns);
+    std::vector<double> b(betas, betas + nchains);
+    auto e = std::make_unique<Ensemble>(ms, cm, sd, b, shared_stream != 0);
+    out = new smmp_ens{std::move(e), flags};
+  });
+  return out;
+}
+
+void smmp_ens_free(smmp_ens_t* e) { delete e; }
+
+int smmp_ens_set_stream(smmp_ens_t* e, void* stream) {
+  return guard([&] {
+    need(e != nullptr, "NULL ensemble");
+    e->e->set_stream(static_cast<cudaStream_t>(stream));
+  });
+}
+
+int smmp_ens_random_start(smmp_ens_t* e) {
+  return guard([&] {
+    need(e != nullptr, "NULL ensemble");
+    e->e->random_start();
+  });
+}
+
+int smmp_ens_energy(smmp_ens_t* e, double* eol) {
+  return guard([&] {
+    need(e != nullptr, "NULL ensemble");
+    e->e->energy((e->flags & SMMP_ENS_FP32) != 0);
+    raise_kernel_errors(*e->e);
+    if (eol) {
+      std::vector<double> v;
+      e->e->get_eol(v);
+      std::copy(v.begin(), v.end(), eol);
+    }
+  });
+}
+
+int smmp_ens_equilibrate(smmp_ens_t* e, int nequi) {
+  return guard([&] {
+    need(e != nullptr && nequi >= 0, "bad arguments");
+    e->e->equilibrate(nequi, e->flags & (kFlagFP32 | kFlagRndOrd));
+    raise_kernel_errors(*e->e);
+  });
+}
+
+int smmp_ens_sweeps(smmp_ens_t* e, int nsweeps, const smmp_weight_t* w) {
+  return guard([&] {
+    need(e != nullptr && nsweeps >= 0, "bad arguments");
+    TmpFree tmp;
+    DWeight dw = to_dweight(w, tmp.p);
+    int flags = e->flags & (kFlagFP32 | kFlagRndOrd);
+    e->e->sweeps(nsweeps, flags, dw);
+    raise_kernel_errors(*e->e);
+  });
+}
+
+int smmp_ens_set_pt(smmp_ens_t* e, const double* betas, int wrap, int exchange_seed) {
+  return guard([&] {
+    need(e != nullptr && betas != nullptr, "NULL argument");
+    e->e->set_pt(std::vector<double>(betas, betas + e->e->nchains()), wrap, exchange_seed);
+  });
+}
+
+int smmp_ens_pt_sweeps(smmp_ens_t* e, int nsweeps, int serial, int graph_chunk) {
+  return guard([&] {
+    need(e != nullptr && nsweeps >= 0, "bad arguments");
+    need(e->e->has_pt(), "call smmp_ens_set_pt first");
+    int flags = e->flags & (kFlagFP32 | kFlagRndOrd);
+    e->e->pt_sweeps(nsweeps, flags, serial != 0, graph_chunk);
+    raise_kernel_errors(*e->e);
+  });
+}
+
+int smmp_ens_pt_map(smmp_ens_t* e, int* temp_chain) {
+  return guard([&] {
+    need(e && temp_chain && e->e->has_pt(), "bad arguments");
+    std::vector<int> tc;
+    e->e->pt_map(tc);
+    std::copy(tc.begin(), tc.end(), temp_chain);
+  });
+}
+
+int smmp_ens_sizes(smmp_ens_t* e, int* nchains, int* vstride, int* tstride) {
+  return guard([&] {
+    need(e != nullptr, "NULL ensemble");
+    if (nchains) *nchains = e->e->nchains();
+    if (vstride) *vstride = e->e->vstride();
+    if (tstride) *tstride = e->e->tstride();
+  });
+}
+
+#define ENS_GET(name, call, T)                      \
+  int name(smmp_ens_t* e, T* out) {                 \
+    return guard([&] {                              \
+      need(e && out, "NULL argument");              \
+      std::vector<T> v;                             \
+      e->e->call(v);                                \
+      std::copy(v.begin(), v.end(), out);           \
+    });                                             \
+  }
+ENS_GET(smmp_ens_get_energies, get_eol, double)
+ENS_GET(smmp_ens_get_terms, get_terms, double)
+ENS_GET(smmp_ens_get_vlvr, get_vlvr, double)
+ENS_GET(smmp_ens_get_betas, get_betas, double)
+ENS_GET(smmp_ens_get_coords, get_coords, double)
+ENS_GET(smmp_ens_errors, get_errors, int)
+#undef ENS_GET
+
+int smmp_ens_set_vlvr(smmp_ens_t* e, const double* vlvr) {
+  return guard([&] {
+    need(e && vlvr, "NULL argument");
+    size_t n = (size_t)e->e->nchains() * e->e->vstride();
+    e->e->set_vlvr(std::vector<double>(vlvr, vlvr + n));
+  });
+}
+
+int smmp_ens_acceptance(smmp_ens_t* e, unsigned long long* acc, unsigned long long* prop) {
+  return guard([&] {
+    need(e && acc && prop, "NULL argument");
+    std::vector<unsigned long long> a, p;
+    e->e->get_acceptance(a, p);
+    std::copy(a.begin(), a.end(), acc);
+    std::copy(p.begin(), p.end(), prop);
+  });
+}
+
+int smmp_ens_draw(smmp_ens_t* e, int slot, int n, double* out) {
+  return guard([&] {
+    need(e && out && n >= 0 && slot >= 0 && slot < e->e->nslots_mt(), "bad arguments");
+    std::vector<double> v;
+    e->e->draw(slot, n, v);
+    std::copy(v.begin(), v.end(), out);
+  });
+}
+
+}  // extern "C"
+
+namespace {
+struct CkptHeader {
+  uint64_t magic, nchains, vstride, tstride, nmt, ntoat, npt, iswitch;
+};
+constexpr uint64_t kMagic = 0x534d4d5042323030ull;   // "SMMPB200"
+template <class T>
+void put(std::vector<char>& b, const std::vector<T>& v) {
+  const char* p = reinterpret_cast<const char*>(v.data());
+  b.insert(b.end(), p, p + v.size() * sizeof(T));
+}
+template <class T>
+void get(const char*& p, const char* end, std::vector<T>& v, size_t n) {
+  if ((size_t)(end - p) < n * sizeof(T)) throw std::invalid_argument("checkpoint truncated");
+  v.resize(n);
+  std::memcpy(v.data(), p, n * sizeof(T));
+  p += n * sizeof(T);
+}
+std::vector<char> serialize(Ensemble& e) {
+  CkptHeader h{kMagic, (uint64_t)e.nchains(), (uint64_t)e.vstride(), (uint64_t)e.tstride(),
+               (uint64_t)e.nslots_mt(), (uint64_t)e.nslots_toat(), 0, 0};
+  std::vector<double> vl, to, be, eo;
+  std::vector<uint32_t> mt, ptmt;
+  std::vector<unsigned long long> acc, prop;
+  std::vector<int> tc;
+  std::vector<double> ptb;
+  int isw = 0;
+  e.get_vlvr(vl);
+  e.get_toat(to);
+  e.get_betas(be);
+  e.get_eol(eo);
+  e.get_mt(mt);
+  e.get_acceptance(acc, prop);
+  if (e.has_pt()) {
+    e.pt_get_state(tc, isw, ptmt, ptb);
+    h.npt = tc.size();
+    h.iswitch = (uint64_t)isw;
+  }
+  std::vector<char> b(sizeof h);
+  std::memcpy(b.data(), &h, sizeof h);
+  put(b, vl);
+  put(b, to);
+  put(b, be);
+  put(b, eo);
+  put(b, mt);
+  put(b, acc);
+  put(b, prop);
+  if (h.npt) {
+    put(b, tc);
+    put(b, ptmt);
+    put(b, ptb);
+  }
+  return b;
+}
+}  // namespace
+
+extern "C" {
+
+int smmp_ens_checkpoint(smmp_ens_t* e, void* buf, uint64_t* bytes) {
+  return guard([&] {
+    need(e && bytes, "NULL argument");
+    std::vector<char> b = serialize(*e->e);
+    if (!buf) {
+      *bytes = b.size();
+      return;
+    }
+    need(*bytes >= b.size(), "checkpoint buffer too small");
+    std::memcpy(buf, b.data(), b.size());
+    *bytes = b.size();
+  });
+}
+
+int smmp_ens_restore(smmp_ens_t* e, const void* buf, uint64_t bytes) {
+  return guard([&] {
+    need(e && buf && bytes >= sizeof(CkptHeader), "bad arguments");
+    CkptHeader h;
+    std::memcpy(&h, buf, sizeof h);
+    Ensemble& en = *e->e;
+    need(h.magic == kMagic && h.nchains == (uint64_t)en.nchains() &&
+             h.vstride == (uint64_t)en.vstride() && h.tstride == (uint64_t)en.tstride() &&
+             h.nmt == (uint64_t)en.nslots_mt() && h.ntoat == (uint64_t)en.nslots_toat(),
+         "checkpoint does not match this ensemble");
+    const char* p = static_cast<const char*>(buf) + sizeof h;
+    const char* end = static_cast<const char*>(buf) + bytes;
+    std::vector<double> vl, to, be, eo, ptb;
+    std::vector<uint32_t> mt, ptmt;
+    std::vector<unsigned long long> acc, prop;
+    std::vector<int> tc;
+    get(p, end, vl, h.nchains * h.vstride);
+    get(p, end, to, h.ntoat * h.tstride);
+    get(p, end, be, h.nchains);
+    get(p, end, eo, h.nchains);
+    get(p, end, mt, h.nmt * 625);
+    get(p, end, acc, h.nchains);
+    get(p, end, prop, h.nchains);
+    en.set_vlvr(vl);
+    en.set_toat(to);
+    en.set_betas(be);
+    en.set_mt(mt);
+    if (h.npt) {
+      need(en.has_pt(), "checkpoint holds a PT state; call smmp_ens_set_pt first");
+      get(p, end, tc, h.npt);
+      get(p, end, ptmt, 625);
+      get(p, end, ptb, h.npt);
+      en.pt_set_state(tc, (int)h.iswitch, ptmt, ptb);
+    }
+    (void)eo;
+    (void)acc;
+    (void)prop;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,115 @@
+// Device-side data structures shared by the kernels and the host runtime.
+#pragma once
+#include <cstdint>
+
+namespace smmpb200 {
+
+constexpr int kTypes = 18;
+constexpr int kTP = kTypes * kTypes;
+constexpr int kThreads = 256;            // threads per chain (one CTA per chain)
+constexpr int kWarps = kThreads / 32;
+constexpr int kMaxNeighbours = 128;      // SASA neighbours per atom (per-warp buffer)
+
+// One molecule, GPU resident (all indices 0-based, see topology.hpp).
+struct DMol {
+  int natoms, nvar, nfree, nchunks, n14, nheavy, nlevels, nres;
+  int i1, i2, i3;
+  double gbpr[6];
+  const int* iow;
+  const uint8_t* type;
+  const double* charge;
+  const double* blen;
+  const double* cba;
+  const double* sba;
+  const double* toat0;
+  const double* rvdw;
+  const double* sigma;
+  const int* level_atoms;
+  const int* level_off;
+  const int* var_atom;
+  const int* var_base;
+  const int* var_lo;
+  const int* var_hi;
+  const int* sib_off;
+  const int* sib;
+  const double* var_e0;
+  const double* var_sg;
+  const double* var_rn;
+  const double* axvr;
+  const int* idvr;
+  const uint32_t* chunks;
+  const uint32_t* pairs14;
+  const int* heavy;
+  const int* residue_of_atom;
+};
+
+// Force field constants read by every chain (copied to shared memory).
+struct DForceField {
+  double a[kTP], a14[kTP], c[kTP], guard_r2[kTP];
+  int hb[kTP];
+  double conv, plt, slp;
+  int epsd, itysol, npnt;
+  const double* spoint;    // device, npnt*3
+};
+
+// Scalars of the force field every pair term reads.
+struct FFScalars {
+  double conv, plt, slp;
+  int epsd, itysol, npnt;
+};
+
+// Everything a launch needs to know about the molecules of its chains.
+struct DMolSet {
+  const DMol* mols;          // device array
+  int nmols;
+  int max_atoms, max_vars;   // shared-memory sizing
+  const DForceField* ff;     // device
+  FFScalars f;
+};
+
+// Sampling weight (canon.f can_weight; mulcan_par_mod.f90 muca_weight*).
+enum WeightKind : int { kWeightCanon = 0, kWeightMuca = 1, kWeightMuca2 = 2 };
+struct DWeight {
+  int kind;
+  int kmin, kmax;
+  double ebin;
+  const double* b;       // [kmax-kmin+1]
+  const double* alpha;
+};
+
+// Mutable state of a set of chains (replicas).
+struct DChains {
+  int nchains;
+  const int* mol_of_chain;
+  double* vlvr;          // [chain * vstride + var]
+  int vstride;
+  double* toat;          // [slot * tstride + atom]  (phase-constant dihedral state)
+  int tstride;
+  const int* toat_slot;
+  uint32_t* mt;          // [slot * 625]: 624 words, then mti
+  const int* mt_slot;
+  double* beta;          // current inverse temperature of each chain
+  double* eol;           // energy of the current conformation
+  double* terms;         // [chain*6]: eyel eyvw eyhb eyvr eysl eysm (last full evaluation)
+  unsigned long long* nacc;
+  unsigned long long* nprop;
+  int* err;              // first error of each chain (0 = none)
+  double* coords;        // optional [chain * 3 * tstride] coordinates after the call
+};
+
+enum SweepFlags : int {
+  kFlagRndOrd = 1,        // random variable order (rndord)
+  kFlagFP32 = 2,          // FP32 pair terms with FP64 guard and accumulation
+  kFlagExtraSetvar = 4,   // one extra setvar+rebuild before the sweep (partem_s)
+  kFlagNoCheck = 8,       // skip the end-of-sweep consistency check
+};
+
+enum ErrorCode : int {
+  kErrNone = 0,
+  kErrNonFinite = 1,      // NaN/Inf energy
+  kErrConsistency = 2,    // |E_incremental - E_fresh| above tolerance at sweep end
+  kErrNeighbours = 3,     // SASA neighbour buffer overflow
+  kErrTimeout = 4,        // a bounded wait gave up
+};
+
+}  // namespace smmpb200

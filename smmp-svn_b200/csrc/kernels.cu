@@ -1,0 +1,853 @@
+// sm_100a kernels of the SMMP energy-and-sweep path.
+//
+//  k_seed         per-stream MT19937 seeding (twister.f sgrnd, Knuth 69069)
+//  k_draw         draw numbers from a stream (grnd) -- RNG parity and the
+//                 host-facing grnd() entry point
+//  k_random_start canonical random start (canon.f:60-67)
+//  k_energy       setvar + full Eyring rebuild + ECEPP/3 (+ SASA) energy of a
+//                 batch of conformations, one CTA each (energy.f)
+//  k_sweep        persistent Metropolis sweeps, one CTA per chain
+//                 (metropolis.f): per proposal an in-place rotation of the
+//                 moving subtree, the full pair energy over the mklist lists,
+//                 and the acceptance test in FP64
+//  k_exchange     parallel-tempering exchange step (partem_s.f:210-232)
+//
+// One CTA owns one chain: coordinates, dihedral state, variables and the
+// chain's MT19937 state live in shared memory for the whole launch; the
+// per-molecule topology is read through the read-only cache.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "device.cuh"
+#include "kernels.hpp"
+
+namespace smmpb200 {
+
+namespace {
+
+constexpr double kPi = 3.141592653589793;
+constexpr double kPi2 = 2.0 * kPi;
+
+// ---------------------------------------------------------------- angles
+// difang.f:12-33 / :38-60 -- wrap into (-pi, pi] with Fortran MOD (fmod).
+__device__ __forceinline__ double wrap_pi(double d) {
+  d = fmod(d, kPi2);
+  return fabs(d) <= kPi ? d : __dsub_rn(d, copysign(kPi2, d));
+}
+__device__ __forceinline__ double difang(double a1, double a2) { return wrap_pi(__dsub_rn(a2, a1)); }
+__device__ __forceinline__ double addang(double a1, double a2) { return wrap_pi(__dadd_rn(a1, a2)); }
+
+// ---------------------------------------------------------------- MT19937
+// State layout: 624 words followed by mti (twister.f /myblock/).
+__device__ void mt_seed(uint32_t* mt, uint32_t seed) {
+  mt[0] = seed;
+  for (int i = 1; i < 624; ++i) mt[i] = 69069u * mt[i - 1];
+  mt[624] = 624;
+}
+__device__ void mt_twist(uint32_t* mt) {
+  const uint32_t MATA = 0x9908B0DFu, UM = 0x80000000u, LM = 0x7fffffffu;
+  int kk = 0;
+  uint32_t y;
+  for (; kk < 624 - 397; ++kk) {
+    y = (mt[kk] & UM) | (mt[kk + 1] & LM);
+    mt[kk] = mt[kk + 397] ^ (y >> 1) ^ ((y & 1u) ? MATA : 0u);
+  }
+  for (; kk < 623; ++kk) {
+    y = (mt[kk] & UM) | (mt[kk + 1] & LM);
+    mt[kk] = mt[kk - 227] ^ (y >> 1) ^ ((y & 1u) ? MATA : 0u);
+  }
+  y = (mt[623] & UM) | (mt[0] & LM);
+  mt[623] = mt[396] ^ (y >> 1) ^ ((y & 1u) ? MATA : 0u);
+}
+// grnd (twister.f:104-177): tempered word / (2^32 - 1), in [0, 1].
+__device__ double mt_grnd(uint32_t* mt) {
+  uint32_t mti = mt[624];
+  if (mti >= 624) {
+    if (mti == 625) mt_seed(mt, 4357u);
+    mt_twist(mt);
+    mti = 0;
+  }
+  uint32_t y = mt[mti];
+  mt[624] = mti + 1;
+  y ^= (y >> 11);
+  y ^= (y << 7) & 0x9D2C5680u;
+  y ^= (y << 15) & 0xEFC60000u;
+  y ^= (y >> 18);
+  return __ddiv_rn((double)y, 4294967295.0);
+}
+
+// ---------------------------------------------------------------- shared memory
+struct Scalars {
+  int jv, accept, busy;
+  double vold, vnew, theta_c, theta_s;
+  double ax, ay, az, px, py, pz;   // rotation axis and pivot (base atom)
+  double enew, eol;
+  double sum[5];
+};
+
+struct Smem {
+  double *x, *y, *z, *bx, *by, *bz;
+  double *toat, *sn, *cs;
+  double *fx, *fz;
+  double *cq;
+  uint8_t* type;
+  double* vlvr;
+  uint32_t* mt;
+  double* red;
+  double *ta, *ta14, *tc, *tg;
+  int* thb;
+  double* spt;
+  double* nb;
+  Scalars* sc;
+  DMol* mol;
+};
+
+__host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~size_t(15); }
+
+// Shared-memory carve-up for up to `n` atoms and `v` variables.
+__host__ __device__ inline size_t smem_layout(int n, int v, int npnt, bool sasa, Smem* s,
+                                              char* base) {
+  size_t off = 0;
+  auto take = [&](size_t bytes) -> char* {
+    char* p = base ? base + off : nullptr;
+    off = align16(off + bytes);
+    return p;
+  };
+  Smem t;
+  t.x = (double*)take(8 * n);
+  t.y = (double*)take(8 * n);
+  t.z = (double*)take(8 * n);
+  t.bx = (double*)take(8 * n);
+  t.by = (double*)take(8 * n);
+  t.bz = (double*)take(8 * n);
+  t.toat = (double*)take(8 * n);
+  t.sn = (double*)take(8 * n);
+  t.cs = (double*)take(8 * n);
+  t.fx = (double*)take(24 * n);
+  t.fz = (double*)take(24 * n);
+  t.cq = (double*)take(8 * n);
+  t.type = (uint8_t*)take(n);
+  t.vlvr = (double*)take(8 * (v > 0 ? v : 1));
+  t.mt = (uint32_t*)take(4 * 625);
+  t.red = (double*)take(8 * kWarps * 8);
+  t.ta = (double*)take(8 * kTP);
+  t.ta14 = (double*)take(8 * kTP);
+  t.tc = (double*)take(8 * kTP);
+  t.tg = (double*)take(8 * kTP);
+  t.thb = (int*)take(4 * kTP);
+  t.spt = (double*)take(sasa ? 8 * 3 * npnt : 8);
+  t.nb = (double*)take(sasa ? 8 * 4 * kWarps * kMaxNeighbours : 8);
+  t.sc = (Scalars*)take(sizeof(Scalars));
+  t.mol = (DMol*)take(sizeof(DMol));
+  if (s) *s = t;
+  return off;
+}
+
+__device__ Smem carve(const DMolSet& set, bool sasa) {
+  extern __shared__ __align__(16) char smem_raw[];
+  Smem s;
+  smem_layout(set.max_atoms, set.max_vars, set.f.npnt, sasa, &s, smem_raw);
+  return s;
+}
+
+// Copy force-field tables and the molecule's per-atom constants.
+__device__ void load_static(const DForceField& ff, const DMol& m, Smem& s, bool sasa) {
+  for (int k = threadIdx.x; k < kTP; k += blockDim.x) {
+    s.ta[k] = ff.a[k];
+    s.ta14[k] = ff.a14[k];
+    s.tc[k] = ff.c[k];
+    s.tg[k] = ff.guard_r2[k];
+    s.thb[k] = ff.hb[k];
+  }
+  for (int k = threadIdx.x; k < m.natoms; k += blockDim.x) {
+    s.cq[k] = __ldg(&m.charge[k]);
+    s.type[k] = __ldg(&m.type[k]);
+  }
+  if (sasa)
+    for (int k = threadIdx.x; k < 3 * ff.npnt; k += blockDim.x) s.spt[k] = ff.spoint[k];
+}
+
+// ---------------------------------------------------------------- setvar
+// setvar.f:30-56 for every variable of the molecule (one thread each; each
+// variable shifts only the children of its own base, so threads never touch
+// the same atom).  Returns this thread's share of the torsion energy
+// (enyshe.f:70-80).
+__device__ double setvar_all(const DMol& m, Smem& s) {
+  double evr = 0.0;
+  for (int v = threadIdx.x; v < m.nvar; v += blockDim.x) {
+    int iat = __ldg(&m.var_atom[v]);
+    double tsh = difang(s.toat[iat], s.vlvr[v]);
+    if (tsh != 0.0) {
+      int b = __ldg(&m.sib_off[v]), e = __ldg(&m.sib_off[v + 1]);
+      for (int k = b; k < e; ++k) {
+        int jat = __ldg(&m.sib[k]);
+        double to = __dadd_rn(s.toat[jat], tsh);
+        if (fabs(to) > kPi) to = __dsub_rn(to, copysign(kPi2, to));
+        s.toat[jat] = to;
+        double sv, cv;
+        sincos(to, &sv, &cv);
+        s.sn[jat] = sv;
+        s.cs[jat] = cv;
+      }
+    }
+    double e0 = __ldg(&m.var_e0[v]);
+    if (e0 != 0.0)
+      evr += e0 * (1.0 + __ldg(&m.var_sg[v]) * cos(s.toat[iat] * __ldg(&m.var_rn[v])));
+  }
+  return evr;
+}
+
+// ---------------------------------------------------------------- rebuild
+// Frame of the first backbone atom from the global parameters (setgbl,
+// bldmol.f:303-420).  Single thread.
+__device__ void first_frame(const DMol& m, Smem& s) {
+  int i1 = m.i1, i2 = m.i2, i3 = m.i3;
+  double ca = cos(m.gbpr[3]), sa = sin(m.gbpr[3]);
+  double cb = cos(m.gbpr[4]), sb = sin(m.gbpr[4]);
+  double cg = cos(m.gbpr[5]), sg = sin(m.gbpr[5]);
+  double ag[3][3];
+  double x1 = ca * cg - sa * sb * sg, x2 = sa * cg + ca * sb * sg, x3 = -cb * sg;
+  double d = sqrt(x1 * x1 + x2 * x2 + x3 * x3);
+  ag[0][0] = x1 / d; ag[1][0] = x2 / d; ag[2][0] = x3 / d;
+  double y1 = -sa * cb, y2 = ca * cb, y3 = sb;
+  d = sqrt(y1 * y1 + y2 * y2 + y3 * y3);
+  ag[0][1] = y1 / d; ag[1][1] = y2 / d; ag[2][1] = y3 / d;
+  double z1 = ca * sg + sa * sb * cg, z2 = sa * sg - ca * sb * cg, z3 = cb * cg;
+  d = sqrt(z1 * z1 + z2 * z2 + z3 * z3);
+  ag[0][2] = z1 / d; ag[1][2] = z2 / d; ag[2][2] = z3 / d;
+  double ct2 = s.cs[i2], st2 = s.sn[i2], sa2 = __ldg(&m.sba[i2]);
+  x1 = -__ldg(&m.cba[i2]);
+  x2 = -sa2 * ct2;
+  x3 = -sa2 * st2;
+  double dx = sqrt(x1 * x1 + x2 * x2 + x3 * x3);
+  x1 /= dx; x2 /= dx; x3 /= dx;
+  double st3 = s.sn[i3], ct3 = s.cs[i3];
+  z1 = -st3 * (st2 * x3 + ct2 * x2);
+  z2 = st3 * ct2 * x1 + ct3 * st2;
+  z3 = st3 * st2 * x1 - ct3 * ct2;
+  double dz = sqrt(z1 * z1 + z2 * z2 + z3 * z3);
+  z1 /= dz; z2 /= dz; z3 /= dz;
+  y1 = z2 * x3 - z3 * x2;
+  y3 = z1 * x2 - z2 * x1;
+  double xg[3], zg[3];
+  for (int r = 0; r < 3; ++r) {
+    xg[r] = ag[r][0] * x1 + ag[r][1] * y1 + ag[r][2] * z1;
+    zg[r] = ag[r][0] * x3 + ag[r][1] * y3 + ag[r][2] * z3;
+  }
+  dx = sqrt(xg[0] * xg[0] + xg[1] * xg[1] + xg[2] * xg[2]);
+  dz = sqrt(zg[0] * zg[0] + zg[1] * zg[1] + zg[2] * zg[2]);
+  for (int r = 0; r < 3; ++r) {
+    s.fx[3 * i1 + r] = xg[r] / dx;
+    s.fz[3 * i1 + r] = zg[r] / dz;
+  }
+  s.x[i1] = m.gbpr[0];
+  s.y[i1] = m.gbpr[1];
+  s.z[i1] = m.gbpr[2];
+}
+
+// Eyring step (bldmol.f:175-242): atom i from the frame of its parent ia.
+__device__ __forceinline__ void eyring(const DMol& m, Smem& s, int i, int ia) {
+  double ct = s.cs[i], st = s.sn[i];
+  double ca = __ldg(&m.cba[i]), sa = __ldg(&m.sba[i]), bl = __ldg(&m.blen[i]);
+  double x1 = s.fx[3 * ia], x2 = s.fx[3 * ia + 1], x3 = s.fx[3 * ia + 2];
+  double z1 = s.fz[3 * ia], z2 = s.fz[3 * ia + 1], z3 = s.fz[3 * ia + 2];
+  double y1 = z2 * x3 - z3 * x2, y2 = z3 * x1 - z1 * x3, y3 = z1 * x2 - z2 * x1;
+  double h2 = -sa * ct, h3 = -sa * st;
+  double nx1 = -ca * x1 + h2 * y1 + h3 * z1;
+  double nx2 = -ca * x2 + h2 * y2 + h3 * z2;
+  double nx3 = -ca * x3 + h2 * y3 + h3 * z3;
+  double dx = rsqrt(nx1 * nx1 + nx2 * nx2 + nx3 * nx3);
+  nx1 *= dx; nx2 *= dx; nx3 *= dx;
+  s.fx[3 * i] = nx1;
+  s.fx[3 * i + 1] = nx2;
+  s.fx[3 * i + 2] = nx3;
+  double nz1 = -st * y1 + ct * z1, nz2 = -st * y2 + ct * z2, nz3 = -st * y3 + ct * z3;
+  double dz = rsqrt(nz1 * nz1 + nz2 * nz2 + nz3 * nz3);
+  s.fz[3 * i] = nz1 * dz;
+  s.fz[3 * i + 1] = nz2 * dz;
+  s.fz[3 * i + 2] = nz3 * dz;
+  s.x[i] = s.x[ia] + nx1 * bl;
+  s.y[i] = s.y[ia] + nx2 * bl;
+  s.z[i] = s.z[ia] + nx3 * bl;
+}
+
+// Full rebuild of all coordinates from the dihedral state (bldmol.f:13-93):
+// the first frame, then one parallel Eyring step per depth level.
+__device__ void full_rebuild(const DMol& m, Smem& s) {
+  if (threadIdx.x == 0) first_frame(m, s);
+  __syncthreads();
+  for (int L = 1; L < m.nlevels; ++L) {
+    int b = __ldg(&m.level_off[L]), e = __ldg(&m.level_off[L + 1]);
+    for (int k = b + threadIdx.x; k < e; k += blockDim.x) {
+      int a = __ldg(&m.level_atoms[k]);
+      eyring(m, s, a, __ldg(&m.iow[a]));
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------- pair energy
+// One ECEPP/3 pair (enyshe.f:112-184): Coulomb with constant or sigmoidal
+// dielectric, 12-6 Lennard-Jones or 12-10 hydrogen bond.
+template <bool F32>
+__device__ __forceinline__ void pair_term(const FFScalars& ff, const Smem& s, int i, int j,
+                                          bool is14, double& el, double& vw, double& hb) {
+  double dx = s.x[j] - s.x[i], dy = s.y[j] - s.y[i], dz = s.z[j] - s.z[i];
+  double r2 = dx * dx + dy * dy + dz * dz;
+  int tp = s.type[i] * kTypes + s.type[j];
+  double A = is14 ? s.ta14[tp] : s.ta[tp];
+  double C = s.tc[tp];
+  int ishb = s.thb[tp];
+  double qq = ff.conv * s.cq[i] * s.cq[j];
+  if (!F32 || r2 < s.tg[tp] || ff.epsd) {
+    double ri = rsqrt(r2);
+    double r2i = ri * ri;
+    double r6i = r2i * r2i * r2i;
+    double ep = 1.0;
+    if (ff.epsd) {
+      double sr = ff.slp * (r2 * ri);
+      ep = ff.plt - (sr * sr + 2.0 * sr + 2.0) * (ff.plt - 1.0) * exp(-sr) / 2.0;
+    }
+    el += qq * ri / ep;
+    if (!ishb)
+      vw += A * r6i * r6i - C * r6i;
+    else
+      hb += A * r6i * r6i - C * r6i * r2i * r2i;
+  } else {
+    float rf = rsqrtf((float)r2);
+    float r2i = rf * rf;
+    float r6i = r2i * r2i * r2i;
+    el += (double)((float)qq * rf);
+    float Af = (float)A, Cf = (float)C;
+    if (!ishb)
+      vw += (double)(Af * r6i * r6i - Cf * r6i);
+    else
+      hb += (double)(Af * r6i * r6i - Cf * r6i * r2i * r2i);
+  }
+}
+
+template <bool F32>
+__device__ void pair_energy(const FFScalars& ff, const DMol& m, const Smem& s, double& el,
+                            double& vw, double& hb) {
+  int nwork = m.nchunks * 8;
+  for (int t = threadIdx.x; t < nwork; t += blockDim.x) {
+    uint32_t w = __ldg(&m.chunks[t >> 3]);
+    int l = t & 7;
+    int len = int((w >> 28) & 7u) + 1;
+    if (l < len) pair_term<F32>(ff, s, int(w & 0x3fffu), int((w >> 14) & 0x3fffu) + l, false, el, vw, hb);
+  }
+  for (int t = threadIdx.x; t < m.n14; t += blockDim.x) {
+    uint32_t w = __ldg(&m.pairs14[t]);
+    pair_term<F32>(ff, s, int(w & 0x3fffu), int(w >> 14), true, el, vw, hb);
+  }
+}
+
+// ---------------------------------------------------------------- SASA
+// enysol.f:192-306: an atom's sphere point is exposed when it lies outside
+// every neighbour sphere (neighbours: d <= r_i + r_j).  FP64 with the
+// reference's division and summation order and no fused multiply-add, so the
+// exposed-point counts are those of the reference arithmetic.  One warp per
+// heavy atom; returns this thread's share of eysl (and of the SASA).
+__device__ double sasa_energy(const FFScalars& ff, const DMol& m, Smem& s, int* err,
+                              double* asa_out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double* nb = s.nb + (size_t)warp * kMaxNeighbours * 4;
+  double eysl = 0.0, asa = 0.0;
+  const int npnt = ff.npnt;
+  for (int h = warp; h < m.nheavy; h += kWarps) {
+    int i = __ldg(&m.heavy[h]);
+    double trad = __ldg(&m.rvdw[i]);
+    double xi = s.x[i], yi = s.y[i], zi = s.z[i];
+    int nn = 0;
+    for (int base = 0; base < m.nheavy; base += 32) {
+      int hj = base + lane;
+      bool take = false;
+      double dx = 0, dy = 0, dz = 0, rb2 = 0;
+      if (hj < m.nheavy) {
+        int j = __ldg(&m.heavy[hj]);
+        if (j != i) {
+          double rj = __ldg(&m.rvdw[j]);
+          double ex = xi - s.x[j], ey = yi - s.y[j], ez = zi - s.z[j];
+          double lim = trad + rj;
+          // cheap pre-test with margin; the exact test below decides
+          if (ex * ex + ey * ey + ez * ez <= lim * lim * 1.0000001 + 1e-12) {
+            dx = __ddiv_rn(ex, trad);
+            dy = __ddiv_rn(ey, trad);
+            dz = __ddiv_rn(ez, trad);
+            double dd = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+            double akrad = __ddiv_rn(rj, trad);
+            double dr = __dadd_rn(1.0, akrad);
+            dr = __dmul_rn(dr, dr);
+            take = dd <= dr;
+            rb2 = __dmul_rn(akrad, akrad);
+          }
+        }
+      }
+      unsigned mask = __ballot_sync(0xffffffffu, take);
+      int pos = nn + __popc(mask & ((1u << lane) - 1u));
+      if (take && pos < kMaxNeighbours) {
+        nb[4 * pos] = dx;
+        nb[4 * pos + 1] = dy;
+        nb[4 * pos + 2] = dz;
+        nb[4 * pos + 3] = rb2;
+      }
+      nn += __popc(mask);
+    }
+    if (nn > kMaxNeighbours) {
+      if (lane == 0) atomicCAS(err, 0, (int)kErrNeighbours);
+      nn = kMaxNeighbours;
+    }
+    __syncwarp();
+    int cnt = 0;
+    for (int p = lane; p < npnt; p += 32) {
+      double s0 = s.spt[3 * p], s1 = s.spt[3 * p + 1], s2 = s.spt[3 * p + 2];
+      bool exposed = true;
+      for (int k = 0; k < nn; ++k) {
+        double t0 = __dadd_rn(nb[4 * k], s0), t1 = __dadd_rn(nb[4 * k + 1], s1),
+               t2 = __dadd_rn(nb[4 * k + 2], s2);
+        double sdd = __dadd_rn(__dadd_rn(__dmul_rn(t0, t0), __dmul_rn(t1, t1)), __dmul_rn(t2, t2));
+        if (sdd <= nb[4 * k + 3]) {
+          exposed = false;
+          break;
+        }
+      }
+      cnt += exposed;
+    }
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    if (lane == 0) {
+      double sdr = __ddiv_rn(__dmul_rn(__dmul_rn(4.0 * kPi, trad), trad), (double)npnt);
+      double area = __dmul_rn(sdr, (double)cnt);
+      asa += area;
+      eysl += __dmul_rn(area, __ldg(&m.sigma[i]));
+    }
+    __syncwarp();
+  }
+  if (asa_out) *asa_out = asa;
+  return eysl;
+}
+
+// ---------------------------------------------------------------- reduction
+// Block sum of 5 values; result valid in thread 0 (s.sc->sum).
+__device__ void block_sum5(Smem& s, double v0, double v1, double v2, double v3, double v4) {
+  double v[5] = {v0, v1, v2, v3, v4};
+#pragma unroll
+  for (int k = 0; k < 5; ++k)
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < 5; ++k) s.red[warp * 8 + k] = v[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < 5; ++k) {
+      double acc = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) acc += s.red[w * 8 + k];
+      s.sc->sum[k] = acc;
+    }
+  }
+}
+
+// Full evaluation of the current coordinates: per-thread partials of
+// (eyel, eyvw, eyhb, eysl) plus the torsion share passed in; block-reduced.
+template <bool F32>
+__device__ void evaluate(const FFScalars& ff, const DMol& m, Smem& s, double evr, int* err) {
+  double el = 0.0, vw = 0.0, hb = 0.0, sl = 0.0;
+  pair_energy<F32>(ff, m, s, el, vw, hb);
+  if (ff.itysol > 0) sl = sasa_energy(ff, m, s, err, nullptr);
+  block_sum5(s, el, vw, hb, evr, sl);
+}
+
+__device__ __forceinline__ double total_of(const double* sum) {
+  // energy.f: eysm = eyel + eyvw + eyhb + eyvr, then + eysl
+  return ((sum[0] + sum[1]) + sum[2]) + sum[3] + sum[4];
+}
+
+// Sampling weight (canon.f:135-149, mulcan_par_mod.f90:380-410), FP64 with
+// separately rounded products as in the reference.
+__device__ double weight(const DWeight& w, double beta, double x) {
+  if (w.kind == kWeightCanon) return __dmul_rn(beta, x);
+  double v = __dadd_rn(__ddiv_rn(x, w.ebin), copysign(0.5, x));
+  v = fmax((double)w.kmin, v);
+  v = fmin((double)w.kmax, v);
+  int k = (int)v - w.kmin;
+  if (w.kind == kWeightMuca) return __dadd_rn(__dmul_rn(__dadd_rn(beta, w.b[k]), x), w.alpha[k]);
+  return __dadd_rn(__dmul_rn(w.b[k], x), w.alpha[k]);
+}
+
+__device__ __forceinline__ void set_err(int* err, int code) {
+  if (*err == 0) *err = code;
+}
+
+// Load the chain's state into shared memory.
+__device__ void load_chain(const DChains& ch, const DMol& m, int c, Smem& s) {
+  const double* tg = ch.toat + (size_t)ch.toat_slot[c] * ch.tstride;
+  for (int k = threadIdx.x; k < m.natoms; k += blockDim.x) {
+    double t = tg[k];
+    s.toat[k] = t;
+    double sv, cv;
+    sincos(t, &sv, &cv);
+    s.sn[k] = sv;
+    s.cs[k] = cv;
+  }
+  const double* vg = ch.vlvr + (size_t)c * ch.vstride;
+  for (int k = threadIdx.x; k < m.nvar; k += blockDim.x) s.vlvr[k] = vg[k];
+  const uint32_t* mg = ch.mt + (size_t)ch.mt_slot[c] * 625;
+  for (int k = threadIdx.x; k < 625; k += blockDim.x) s.mt[k] = mg[k];
+}
+
+__device__ void store_chain(const DChains& ch, const DMol& m, int c, Smem& s) {
+  double* tg = ch.toat + (size_t)ch.toat_slot[c] * ch.tstride;
+  for (int k = threadIdx.x; k < m.natoms; k += blockDim.x) tg[k] = s.toat[k];
+  double* vg = ch.vlvr + (size_t)c * ch.vstride;
+  for (int k = threadIdx.x; k < m.nvar; k += blockDim.x) vg[k] = s.vlvr[k];
+  uint32_t* mg = ch.mt + (size_t)ch.mt_slot[c] * 625;
+  for (int k = threadIdx.x; k < 625; k += blockDim.x) mg[k] = s.mt[k];
+  if (ch.coords) {
+    double* cg = ch.coords + (size_t)c * 3 * ch.tstride;
+    for (int k = threadIdx.x; k < m.natoms; k += blockDim.x) {
+      cg[3 * k] = s.x[k];
+      cg[3 * k + 1] = s.y[k];
+      cg[3 * k + 2] = s.z[k];
+    }
+  }
+}
+
+}  // namespace
+
+// ============================================================================ kernels
+
+__global__ void k_seed(uint32_t* mt, const int* seeds, int nslots) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nslots) mt_seed(mt + (size_t)i * 625, (uint32_t)seeds[i]);
+}
+
+__global__ void k_draw(uint32_t* mt, int slot, int n, double* out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0)
+    for (int i = 0; i < n; ++i) out[i] = mt_grnd(mt + (size_t)slot * 625);
+}
+
+// canon.f:60-67 random start, chains visited in the given order so that a
+// shared stream is consumed exactly as the reference does.
+__global__ void k_random_start(DMolSet set, DChains ch, const int* order, int n) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (int q = 0; q < n; ++q) {
+    int c = order[q];
+    const DMol& m = set.mols[ch.mol_of_chain[c]];
+    uint32_t* mt = ch.mt + (size_t)ch.mt_slot[c] * 625;
+    double* vl = ch.vlvr + (size_t)c * ch.vstride;
+    for (int i = 0; i < m.nfree; ++i) {
+      int iv = m.idvr[i];
+      double dv = __dmul_rn(m.axvr[iv], __dsub_rn(mt_grnd(mt), 0.5));
+      vl[iv] = addang(kPi, dv);
+    }
+  }
+}
+
+// Copy the chain's molecule descriptor into shared memory (thread 0).
+__device__ const DMol& stage_mol(const DMolSet& set, const DChains& ch, int c, Smem& s) {
+  if (threadIdx.x == 0) *s.mol = set.mols[ch.mol_of_chain[c]];
+  __syncthreads();
+  return *s.mol;
+}
+
+// energy(): setvar + rebuild + energy for chains [first, first+gridDim.x).
+// The dihedral state is updated in place exactly as the reference's energy()
+// does; terms and eol of each chain receive the result.
+template <bool F32>
+__global__ void __launch_bounds__(kThreads, 1) k_energy(DMolSet set, DChains ch, int first) {
+  int c = first + blockIdx.x;
+  const bool sasa = set.f.itysol > 0;
+  Smem s = carve(set, sasa);
+  const DMol& m = stage_mol(set, ch, c, s);
+  load_static(*set.ff, m, s, sasa);
+  load_chain(ch, m, c, s);
+  __syncthreads();
+  double evr = setvar_all(m, s);
+  __syncthreads();
+  full_rebuild(m, s);
+  evaluate<F32>(set.f, m, s, evr, &ch.err[c]);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const double* sum = s.sc->sum;
+    double e = total_of(sum);
+    ch.eol[c] = e;
+    double* t = ch.terms + (size_t)c * 6;
+    for (int k = 0; k < 5; ++k) t[k] = sum[k];
+    t[5] = ((sum[0] + sum[1]) + sum[2]) + sum[3];
+    if (!isfinite(e)) set_err(&ch.err[c], kErrNonFinite);
+  }
+  store_chain(ch, m, c, s);
+}
+
+// nsweeps Metropolis sweeps (metropolis.f:13-184) of chains
+// [first, first+gridDim.x).  Per sweep the reference calls energy() nvr+2
+// times; here the start of a sweep and the closing consistency check do a full
+// setvar+rebuild+evaluation, and each proposal updates the dihedral state with
+// the same setvar arithmetic, rotates the moving subtree in place and
+// evaluates every pair of the lists.  The start of sweep k+1 reuses the
+// coordinates and energy of the check that closed sweep k (same variables),
+// after the setvar call the reference makes there.
+template <bool F32>
+__global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, DWeight w, int first,
+                                                    int nsweeps, int flags, double check_tol) {
+  int c = first + blockIdx.x;
+  const bool sasa = set.f.itysol > 0;
+  Smem s = carve(set, sasa);
+  Scalars& sc = *s.sc;
+  const DMol& m = stage_mol(set, ch, c, s);
+  load_static(*set.ff, m, s, sasa);
+  load_chain(ch, m, c, s);
+  const double beta = ch.beta[c];
+  int* err = &ch.err[c];
+  unsigned long long nacc = 0, nprop = 0;
+  __syncthreads();
+
+  bool fresh = false;   // coordinates and sc.enew hold the current conformation
+  for (int sw = 0; sw < nsweeps; ++sw) {
+    if (flags & kFlagExtraSetvar) {   // partem_s.f:194-198: setvar(i, vlvr) first
+      setvar_all(m, s);
+      __syncthreads();
+      full_rebuild(m, s);
+      fresh = false;
+    }
+    // eol = energy() (metropolis.f:35)
+    double evr = setvar_all(m, s);
+    __syncthreads();
+    if (!fresh) {
+      full_rebuild(m, s);
+      evaluate<F32>(set.f, m, s, evr, err);
+      __syncthreads();
+      if (threadIdx.x == 0) sc.enew = total_of(sc.sum);
+    }
+    if (threadIdx.x == 0) sc.eol = sc.enew;
+    __syncthreads();
+
+    for (int p = 0; p < m.nfree; ++p) {
+      // ---- proposal (thread 0): variable, step, rotation of its subtree
+      if (threadIdx.x == 0) {
+        int ivar = (flags & kFlagRndOrd) ? (int)(m.nfree * mt_grnd(s.mt)) : p;
+        if (ivar >= m.nfree) ivar = m.nfree - 1;
+        int jv = __ldg(&m.idvr[ivar]);
+        double vold = s.vlvr[jv];
+        double dv = __dmul_rn(__ldg(&m.axvr[jv]), __dsub_rn(mt_grnd(s.mt), 0.5));
+        double vnew = addang(vold, dv);
+        s.vlvr[jv] = vnew;
+        sc.jv = jv;
+        sc.vold = vold;
+        double th = difang(vold, vnew);
+        double sv, cv;
+        sincos(th, &sv, &cv);
+        sc.theta_s = sv;
+        sc.theta_c = cv;
+        int b = __ldg(&m.var_base[jv]), a = __ldg(&m.iow[b]);
+        double ax = s.x[b] - s.x[a], ay = s.y[b] - s.y[a], az = s.z[b] - s.z[a];
+        double inv = rsqrt(ax * ax + ay * ay + az * az);
+        sc.ax = ax * inv;
+        sc.ay = ay * inv;
+        sc.az = az * inv;
+        sc.px = s.x[b];
+        sc.py = s.y[b];
+        sc.pz = s.z[b];
+      }
+      __syncthreads();
+      // ---- setvar for all variables (exact dihedral state) + torsion energy
+      double evr2 = setvar_all(m, s);
+      // ---- rotate the subtree of jv about its bond (right-hand rule, +theta)
+      {
+        int jv = sc.jv;
+        int lo = __ldg(&m.var_lo[jv]), hi = __ldg(&m.var_hi[jv]);
+        double kx = sc.ax, ky = sc.ay, kz = sc.az, cth = sc.theta_c, sth = sc.theta_s;
+        double px = sc.px, py = sc.py, pz = sc.pz;
+        for (int k = lo + threadIdx.x; k <= hi; k += blockDim.x) {
+          double vx = s.x[k] - px, vy = s.y[k] - py, vz = s.z[k] - pz;
+          s.bx[k] = s.x[k];
+          s.by[k] = s.y[k];
+          s.bz[k] = s.z[k];
+          double kd = kx * vx + ky * vy + kz * vz;
+          double cx = ky * vz - kz * vy, cy = kz * vx - kx * vz, cz = kx * vy - ky * vx;
+          double f = kd * (1.0 - cth);
+          s.x[k] = px + vx * cth + cx * sth + kx * f;
+          s.y[k] = py + vy * cth + cy * sth + ky * f;
+          s.z[k] = pz + vz * cth + cz * sth + kz * f;
+        }
+      }
+      __syncthreads();
+      evaluate<F32>(set.f, m, s, evr2, err);
+      __syncthreads();
+      // ---- acceptance (metropolis.f:72-87)
+      if (threadIdx.x == 0) {
+        double enw = total_of(sc.sum);
+        double delta = __dsub_rn(weight(w, beta, enw), weight(w, beta, sc.eol));
+        int up = 0;
+        if (delta <= 0.0) {
+          up = 1;
+        } else {
+          double rd = mt_grnd(s.mt);
+          delta = fmin(delta, 100.0);
+          if (exp(-delta) >= rd) up = 1;
+        }
+        if (up)
+          sc.eol = enw;
+        else
+          s.vlvr[sc.jv] = sc.vold;
+        if (!isfinite(enw)) set_err(err, kErrNonFinite);
+        sc.accept = up;
+        ++nprop;
+        nacc += up;
+      }
+      __syncthreads();
+      if (!sc.accept) {
+        int jv = sc.jv;
+        int lo = __ldg(&m.var_lo[jv]), hi = __ldg(&m.var_hi[jv]);
+        for (int k = lo + threadIdx.x; k <= hi; k += blockDim.x) {
+          s.x[k] = s.bx[k];
+          s.y[k] = s.by[k];
+          s.z[k] = s.bz[k];
+        }
+      }
+      __syncthreads();
+    }
+    // ---- closing energy() and consistency check (metropolis.f:172-179)
+    double evr3 = setvar_all(m, s);
+    __syncthreads();
+    full_rebuild(m, s);
+    evaluate<F32>(set.f, m, s, evr3, err);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double enw = total_of(sc.sum);
+      sc.enew = enw;
+      if (!(flags & kFlagNoCheck) && fabs(sc.eol - enw) > check_tol && sc.eol < 100000.0)
+        set_err(err, kErrConsistency);
+      double* t = ch.terms + (size_t)c * 6;
+      for (int k = 0; k < 5; ++k) t[k] = sc.sum[k];
+      t[5] = ((sc.sum[0] + sc.sum[1]) + sc.sum[2]) + sc.sum[3];
+    }
+    __syncthreads();
+    fresh = true;
+  }
+  if (threadIdx.x == 0) {
+    ch.eol[c] = sc.eol;
+    ch.nacc[c] += nacc;
+    ch.nprop[c] += nprop;
+  }
+  store_chain(ch, m, c, s);
+}
+
+// Replica exchange (partem_s.f:210-232): alternate even/odd neighbour pairs,
+// replica num_rep pairs with 1 when `wrap` is set.  temp_chain[k] is the chain
+// at temperature label k (ipoi); betas[k] the inverse temperature of label k.
+__global__ void k_exchange(DChains ch, int* temp_chain, const double* betas, int n,
+                           uint32_t* mt, int* iswitch, int wrap, unsigned long long* stats) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (n > 1) {
+    int num_rep1, nu;
+    if (*iswitch == 1) {
+      num_rep1 = n - 1;
+      nu = 1;
+      *iswitch = 2;
+    } else {
+      num_rep1 = n;
+      nu = 2;
+      *iswitch = 1;
+    }
+    for (int i = nu; i <= num_rep1; i += 2) {
+      int j = i + 1;
+      if (i == n) {
+        if (!wrap) continue;
+        j = 1;
+      }
+      int in = temp_chain[i - 1], jn = temp_chain[j - 1];
+      double bi = betas[i - 1], bj = betas[j - 1];
+      double ein = ch.eol[in], ejn = ch.eol[jn];
+      double delta = __dsub_rn(-__dmul_rn(bi, ejn), __dmul_rn(bj, ein));
+      delta = __dadd_rn(delta, __dmul_rn(bi, ein));
+      delta = __dadd_rn(delta, __dmul_rn(bj, ejn));
+      double ra = mt_grnd(mt);
+      stats[2 * (i - 1)] += 1;
+      if (ra <= exp(delta)) {
+        temp_chain[i - 1] = jn;
+        temp_chain[j - 1] = in;
+        stats[2 * (i - 1) + 1] += 1;
+      }
+    }
+  }
+  for (int k = 0; k < n; ++k) ch.beta[temp_chain[k]] = betas[k];
+}
+
+// ============================================================================ host wrappers
+
+size_t sweep_smem_bytes(const DMolSet& set) {
+  return smem_layout(set.max_atoms, set.max_vars, set.f.npnt, set.f.itysol > 0, nullptr, nullptr);
+}
+
+cudaError_t launch_seed(uint32_t* mt, const int* seeds, int nslots, cudaStream_t st) {
+  k_seed<<<(nslots + 127) / 128, 128, 0, st>>>(mt, seeds, nslots);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_draw(uint32_t* mt, int slot, int n, double* out, cudaStream_t st) {
+  k_draw<<<1, 1, 0, st>>>(mt, slot, n, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_random_start(const DMolSet& set, const DChains& ch, const int* order, int n,
+                                cudaStream_t st) {
+  k_random_start<<<1, 1, 0, st>>>(set, ch, order, n);
+  return cudaGetLastError();
+}
+
+// Raise a kernel's dynamic shared-memory limit once per size, so that the
+// launches captured into CUDA graphs make no attribute calls.
+static cudaError_t prep_smem(const void* fn, size_t bytes) {
+  static const void* fns[8] = {nullptr};
+  static size_t done[8] = {0};
+  int k = 0;
+  while (k < 8 && fns[k] && fns[k] != fn) ++k;
+  if (k < 8 && fns[k] == fn && done[k] >= bytes) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess && k < 8) {
+    fns[k] = fn;
+    done[k] = bytes;
+  }
+  return e;
+}
+
+cudaError_t launch_energy(const DMolSet& set, const DChains& ch, int first, int count, bool fp32,
+                          cudaStream_t st) {
+  size_t sm = sweep_smem_bytes(set);
+  if (fp32) {
+    cudaError_t e = prep_smem((const void*)k_energy<true>, sm);
+    if (e != cudaSuccess || count <= 0) return e;
+    k_energy<true><<<count, kThreads, sm, st>>>(set, ch, first);
+  } else {
+    cudaError_t e = prep_smem((const void*)k_energy<false>, sm);
+    if (e != cudaSuccess || count <= 0) return e;
+    k_energy<false><<<count, kThreads, sm, st>>>(set, ch, first);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sweep(const DMolSet& set, const DChains& ch, const DWeight& w, int first,
+                         int count, int nsweeps, int flags, double check_tol, cudaStream_t st) {
+  size_t sm = sweep_smem_bytes(set);
+  if (flags & kFlagFP32) {
+    cudaError_t e = prep_smem((const void*)k_sweep<true>, sm);
+    if (e != cudaSuccess || count <= 0) return e;
+    k_sweep<true><<<count, kThreads, sm, st>>>(set, ch, w, first, nsweeps, flags, check_tol);
+  } else {
+    cudaError_t e = prep_smem((const void*)k_sweep<false>, sm);
+    if (e != cudaSuccess || count <= 0) return e;
+    k_sweep<false><<<count, kThreads, sm, st>>>(set, ch, w, first, nsweeps, flags, check_tol);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_exchange(const DChains& ch, int* temp_chain, const double* betas, int n,
+                            uint32_t* mt, int* iswitch, int wrap, unsigned long long* stats,
+                            cudaStream_t st) {
+  k_exchange<<<1, 1, 0, st>>>(ch, temp_chain, betas, n, mt, iswitch, wrap, stats);
+  return cudaGetLastError();
+}
+
+}  // namespace smmpb200

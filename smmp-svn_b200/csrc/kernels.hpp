@@ -1,0 +1,25 @@
+// Launch wrappers of the sm_100a kernels (kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "device.cuh"
+
+namespace smmpb200 {
+
+size_t sweep_smem_bytes(const DMolSet& set);
+
+cudaError_t launch_seed(uint32_t* mt, const int* seeds, int nslots, cudaStream_t st);
+cudaError_t launch_draw(uint32_t* mt, int slot, int n, double* out, cudaStream_t st);
+cudaError_t launch_random_start(const DMolSet& set, const DChains& ch, const int* order, int n,
+                                cudaStream_t st);
+cudaError_t launch_energy(const DMolSet& set, const DChains& ch, int first, int count, bool fp32,
+                          cudaStream_t st);
+cudaError_t launch_sweep(const DMolSet& set, const DChains& ch, const DWeight& w, int first,
+                         int count, int nsweeps, int flags, double check_tol, cudaStream_t st);
+cudaError_t launch_exchange(const DChains& ch, int* temp_chain, const double* betas, int n,
+                            uint32_t* mt, int* iswitch, int wrap, unsigned long long* stats,
+                            cudaStream_t st);
+
+}  // namespace smmpb200

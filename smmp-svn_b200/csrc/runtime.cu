@@ -1,0 +1,439 @@
+// Host runtime: molecule upload, chain ensembles, sweeps, replica exchange.
+#include "runtime.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+
+#include "kernels.hpp"
+
+namespace smmpb200 {
+
+void check_cuda(cudaError_t e, const char* what) {
+  if (e != cudaSuccess)
+    throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+namespace {
+template <class T>
+T* dalloc(std::vector<void*>& owner, size_t n) {
+  void* p = nullptr;
+  check_cuda(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)), "cudaMalloc");
+  owner.push_back(p);
+  return static_cast<T*>(p);
+}
+template <class T>
+void h2d(T* d, const std::vector<T>& h) {
+  if (!h.empty()) check_cuda(cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice), "H2D");
+}
+template <class T>
+void d2h(std::vector<T>& h, const T* d, size_t n) {
+  h.resize(n);
+  if (n) check_cuda(cudaMemcpy(h.data(), d, n * sizeof(T), cudaMemcpyDeviceToHost), "D2H");
+}
+}  // namespace
+
+std::shared_ptr<Molecule> build_molecule(const std::string& libdir, const Config& cfg,
+                                         const std::string& seqfile, const std::string& varfile,
+                                         const std::string& grpn, const std::string& grpc) {
+  auto m = std::make_shared<Molecule>();
+  m->assembly = std::make_shared<Assembly>();
+  Assembly& a = *m->assembly;
+  a.sh2 = cfg.sh2 != 0;
+  a.epsd = cfg.epsd != 0;
+  a.itysol = cfg.itysol;
+  a.ientyp = cfg.ientyp;
+  a.rndord = cfg.rndord != 0;
+  std::string dir = libdir;
+  if (!dir.empty() && dir.back() != '/') dir += '/';
+  a.init_energy(dir);
+  a.init_molecule(seqfile, varfile.empty() ? " " : varfile, grpn, grpc);
+  if (a.ntlml != 1) throw std::runtime_error("build_molecule: one molecule per sequence file");
+  m->topo = flatten(a, 1);
+  m->ff = make_forcefield(a);
+  m->cfg = cfg;
+  return m;
+}
+
+// ---------------------------------------------------------------------------- DeviceSet
+
+template <class T>
+const T* DeviceSet::upload(const std::vector<T>& v) {
+  T* d = dalloc<T>(allocs_, v.size());
+  h2d(d, v);
+  return d;
+}
+
+DeviceSet::DeviceSet(const std::vector<std::shared_ptr<Molecule>>& mols) {
+  if (mols.empty()) throw std::runtime_error("DeviceSet: no molecules");
+  const ForceField& ff = mols[0]->ff;
+  DForceField h{};
+  std::memcpy(h.a, ff.pair.a, sizeof h.a);
+  std::memcpy(h.a14, ff.pair.a14, sizeof h.a14);
+  std::memcpy(h.c, ff.pair.c, sizeof h.c);
+  std::memcpy(h.guard_r2, ff.pair.guard_r2, sizeof h.guard_r2);
+  std::memcpy(h.hb, ff.pair.hb, sizeof h.hb);
+  h.conv = ff.conv;
+  h.plt = ff.plt;
+  h.slp = ff.slp;
+  h.epsd = ff.epsd;
+  h.itysol = ff.itysol;
+  h.npnt = ff.npnt;
+  h.spoint = upload(ff.spoint.empty() ? std::vector<double>{0.0} : ff.spoint);
+  DForceField* dff = dalloc<DForceField>(allocs_, 1);
+  check_cuda(cudaMemcpy(dff, &h, sizeof h, cudaMemcpyHostToDevice), "H2D ff");
+  std::vector<DMol> dm;
+  int max_atoms = 0, max_vars = 0;
+  for (auto& mp : mols) {
+    const MolTopo& t = mp->topo;
+    if (mp->ff.itysol != ff.itysol || mp->ff.epsd != ff.epsd)
+      throw std::runtime_error("DeviceSet: molecules of one ensemble must share the force field");
+    DMol d{};
+    d.natoms = t.natoms;
+    d.nvar = t.nvar;
+    d.nfree = t.nfree;
+    d.nchunks = (int)t.chunks.size();
+    d.n14 = (int)t.pairs14.size();
+    d.nheavy = (int)t.heavy.size();
+    d.nlevels = (int)t.level_off.size() - 1;
+    d.nres = t.nres;
+    d.i1 = t.i1;
+    d.i2 = t.i2;
+    d.i3 = t.i3;
+    for (int k = 0; k < 6; ++k) d.gbpr[k] = t.gbpr[k];
+    d.iow = upload(t.iow);
+    d.type = upload(t.type);
+    d.charge = upload(t.charge);
+    d.blen = upload(t.blen);
+    d.cba = upload(t.cba);
+    d.sba = upload(t.sba);
+    d.toat0 = upload(t.toat0);
+    d.rvdw = upload(t.rvdw);
+    d.sigma = upload(t.sigma);
+    d.level_atoms = upload(t.level_atoms);
+    d.level_off = upload(t.level_off);
+    d.var_atom = upload(t.var_atom);
+    d.var_base = upload(t.var_base);
+    d.var_lo = upload(t.var_lo);
+    d.var_hi = upload(t.var_hi);
+    d.sib_off = upload(t.sib_off);
+    d.sib = upload(t.sib.empty() ? std::vector<int>{0} : t.sib);
+    d.var_e0 = upload(t.var_e0);
+    d.var_sg = upload(t.var_sg);
+    d.var_rn = upload(t.var_rn);
+    d.axvr = upload(t.axvr);
+    d.idvr = upload(t.idvr.empty() ? std::vector<int>{0} : t.idvr);
+    d.chunks = upload(t.chunks.empty() ? std::vector<uint32_t>{0} : t.chunks);
+    d.pairs14 = upload(t.pairs14.empty() ? std::vector<uint32_t>{0} : t.pairs14);
+    d.heavy = upload(t.heavy.empty() ? std::vector<int>{0} : t.heavy);
+    d.residue_of_atom = upload(t.residue_of_atom);
+    dm.push_back(d);
+    max_atoms = std::max(max_atoms, t.natoms);
+    max_vars = std::max(max_vars, t.nvar);
+  }
+  DMol* dmols = dalloc<DMol>(allocs_, dm.size());
+  h2d(dmols, dm);
+  set_.mols = dmols;
+  set_.nmols = (int)dm.size();
+  set_.max_atoms = max_atoms;
+  set_.max_vars = max_vars;
+  set_.ff = dff;
+  set_.f = FFScalars{ff.conv, ff.plt, ff.slp, ff.epsd, ff.itysol, ff.npnt};
+  size_t sm = sweep_smem_bytes(set_);
+  if (sm > 227 * 1024)
+    throw std::runtime_error("DeviceSet: molecule too large for one CTA's shared memory");
+}
+
+DeviceSet::~DeviceSet() {
+  for (void* p : allocs_) cudaFree(p);
+}
+
+// ---------------------------------------------------------------------------- Ensemble
+
+Ensemble::Ensemble(std::vector<std::shared_ptr<Molecule>> mols, std::vector<int> chain_mol,
+                   std::vector<int> seeds, std::vector<double> betas, bool shared_stream)
+    : mols_(std::move(mols)), chain_mol_(std::move(chain_mol)) {
+  n_ = (int)chain_mol_.size();
+  if (n_ <= 0) throw std::runtime_error("Ensemble: no chains");
+  for (int m : chain_mol_)
+    if (m < 0 || m >= (int)mols_.size()) throw std::runtime_error("Ensemble: bad molecule index");
+  if ((int)betas.size() != n_) throw std::runtime_error("Ensemble: one beta per chain");
+  dev_.reset(new DeviceSet(mols_));
+  check_cuda(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking), "stream");
+  stream_ = own_stream_;
+  int vstride = dev_->set().max_vars, tstride = dev_->set().max_atoms;
+  nmt_ = shared_stream ? 1 : n_;
+  ntoat_ = shared_stream ? 1 : n_;
+  if ((int)seeds.size() != nmt_) throw std::runtime_error("Ensemble: one seed per stream");
+  ch_.nchains = n_;
+  ch_.vstride = vstride;
+  ch_.tstride = tstride;
+  int* mol_of = dalloc<int>(allocs_, n_);
+  h2d(mol_of, chain_mol_);
+  ch_.mol_of_chain = mol_of;
+  ch_.vlvr = dalloc<double>(allocs_, (size_t)n_ * vstride);
+  ch_.toat = dalloc<double>(allocs_, (size_t)ntoat_ * tstride);
+  std::vector<int> tslot(n_), mslot(n_);
+  for (int c = 0; c < n_; ++c) {
+    tslot[c] = shared_stream ? 0 : c;
+    mslot[c] = shared_stream ? 0 : c;
+  }
+  int* dts = dalloc<int>(allocs_, n_);
+  int* dms = dalloc<int>(allocs_, n_);
+  h2d(dts, tslot);
+  h2d(dms, mslot);
+  ch_.toat_slot = dts;
+  ch_.mt_slot = dms;
+  ch_.mt = dalloc<uint32_t>(allocs_, (size_t)nmt_ * 625);
+  ch_.beta = dalloc<double>(allocs_, n_);
+  ch_.eol = dalloc<double>(allocs_, n_);
+  ch_.terms = dalloc<double>(allocs_, (size_t)n_ * 6);
+  ch_.nacc = dalloc<unsigned long long>(allocs_, n_);
+  ch_.nprop = dalloc<unsigned long long>(allocs_, n_);
+  ch_.err = dalloc<int>(allocs_, n_);
+  ch_.coords = nullptr;
+  check_cuda(cudaMemset(ch_.nacc, 0, n_ * sizeof(unsigned long long)), "memset");
+  check_cuda(cudaMemset(ch_.nprop, 0, n_ * sizeof(unsigned long long)), "memset");
+  check_cuda(cudaMemset(ch_.err, 0, n_ * sizeof(int)), "memset");
+  check_cuda(cudaMemset(ch_.eol, 0, n_ * sizeof(double)), "memset");
+  check_cuda(cudaMemset(ch_.terms, 0, (size_t)n_ * 6 * sizeof(double)), "memset");
+  // initial variables and dihedral state from the assembled molecules
+  std::vector<double> vl((size_t)n_ * vstride, 0.0), to((size_t)ntoat_ * tstride, 0.0);
+  for (int c = 0; c < n_; ++c) {
+    const MolTopo& t = mols_[chain_mol_[c]]->topo;
+    std::copy(t.vlvr0.begin(), t.vlvr0.end(), vl.begin() + (size_t)c * vstride);
+  }
+  for (int sl = 0; sl < ntoat_; ++sl) {
+    const MolTopo& t = mols_[chain_mol_[sl]]->topo;
+    std::copy(t.toat0.begin(), t.toat0.end(), to.begin() + (size_t)sl * tstride);
+  }
+  h2d(ch_.vlvr, vl);
+  h2d(ch_.toat, to);
+  h2d(ch_.beta, betas);
+  int* dseed = dalloc<int>(allocs_, nmt_);
+  h2d(dseed, seeds);
+  check_cuda(launch_seed(ch_.mt, dseed, nmt_, stream_), "seed");
+  check_cuda(cudaStreamSynchronize(stream_), "seed sync");
+}
+
+Ensemble::~Ensemble() {
+  if (graph_) cudaGraphExecDestroy(graph_);
+  if (stream_) cudaStreamSynchronize(stream_);
+  if (own_stream_ && stream_ != own_stream_) cudaStreamSynchronize(own_stream_);
+  for (void* p : allocs_) cudaFree(p);
+  if (coords_buf_) cudaFree(coords_buf_);
+  if (own_stream_) cudaStreamDestroy(own_stream_);
+}
+
+void Ensemble::set_stream(cudaStream_t s) {
+  check_cuda(cudaStreamSynchronize(stream_), "set_stream sync");
+  stream_ = s ? s : own_stream_;
+  if (graph_) cudaGraphExecDestroy(graph_);
+  graph_ = nullptr;
+  graph_len_ = 0;
+}
+
+void Ensemble::random_start() {
+  std::vector<int> order(n_);
+  std::iota(order.begin(), order.end(), 0);
+  int* d = nullptr;
+  check_cuda(cudaMallocAsync(&d, n_ * sizeof(int), stream_), "malloc");
+  check_cuda(cudaMemcpyAsync(d, order.data(), n_ * sizeof(int), cudaMemcpyHostToDevice, stream_), "H2D");
+  check_cuda(launch_random_start(set(), ch_, d, n_, stream_), "random_start");
+  check_cuda(cudaFreeAsync(d, stream_), "free");
+  check_cuda(cudaStreamSynchronize(stream_), "random_start sync");
+}
+
+void Ensemble::energy(bool fp32) {
+  check_cuda(launch_energy(set(), ch_, 0, n_, fp32, stream_), "energy");
+  check_cuda(cudaStreamSynchronize(stream_), "energy sync");
+}
+
+void Ensemble::energy_chain(int c, bool fp32) {
+  check_cuda(launch_energy(set(), ch_, c, 1, fp32, stream_), "energy");
+}
+
+void Ensemble::launch_sweep_range(int first, int count, int nsweeps, int flags, const DWeight& w) {
+  double tol = (flags & kFlagFP32) ? check_tol_fp32 : check_tol;
+  check_cuda(launch_sweep(set(), ch_, w, first, count, nsweeps, flags, tol, stream_), "sweep");
+}
+
+void Ensemble::sweeps(int nsweeps, int flags, const DWeight& w) {
+  if (nmt_ == 1 && n_ > 1) {   // shared stream: chains strictly one after another
+    for (int c = 0; c < n_; ++c) launch_sweep_range(c, 1, nsweeps, flags, w);
+  } else {
+    launch_sweep_range(0, n_, nsweeps, flags, w);
+  }
+  check_cuda(cudaStreamSynchronize(stream_), "sweeps sync");
+}
+
+void Ensemble::sweeps_chain(int c, int nsweeps, int flags, const DWeight& w) {
+  launch_sweep_range(c, 1, nsweeps, flags, w);
+}
+
+void Ensemble::equilibrate(int nequi, int flags) {
+  DWeight w{kWeightCanon, 0, 0, 1.0, nullptr, nullptr};
+  bool fp32 = (flags & kFlagFP32) != 0;
+  if (nmt_ == 1 && n_ > 1) {
+    for (int c = 0; c < n_; ++c) {
+      energy_chain(c, fp32);
+      if (nequi > 0) launch_sweep_range(c, 1, nequi, flags, w);
+    }
+  } else {
+    check_cuda(launch_energy(set(), ch_, 0, n_, fp32, stream_), "energy");
+    if (nequi > 0) launch_sweep_range(0, n_, nequi, flags, w);
+  }
+  check_cuda(cudaStreamSynchronize(stream_), "equilibrate sync");
+}
+
+void Ensemble::set_pt(const std::vector<double>& betas, int wrap, int exchange_seed) {
+  if ((int)betas.size() != n_) throw std::runtime_error("set_pt: one temperature per chain");
+  pt_.n = n_;
+  pt_.wrap = wrap;
+  pt_.temp_chain = dalloc<int>(allocs_, n_);
+  pt_.betas = dalloc<double>(allocs_, n_);
+  pt_.mt = dalloc<uint32_t>(allocs_, 625);
+  pt_.iswitch = dalloc<int>(allocs_, 1);
+  pt_.stats = dalloc<unsigned long long>(allocs_, 2 * n_);
+  std::vector<int> tc(n_);
+  std::iota(tc.begin(), tc.end(), 0);
+  h2d(pt_.temp_chain, tc);
+  h2d(pt_.betas, betas);
+  h2d(ch_.beta, betas);
+  std::vector<int> one{1};
+  h2d(pt_.iswitch, one);
+  check_cuda(cudaMemset(pt_.stats, 0, 2 * n_ * sizeof(unsigned long long)), "memset");
+  if (nmt_ == 1) {
+    pt_.mt = ch_.mt;   // partem_s: the exchange draws from the same stream
+  } else {
+    int* ds = dalloc<int>(allocs_, 1);
+    std::vector<int> sd{exchange_seed};
+    h2d(ds, sd);
+    check_cuda(launch_seed(pt_.mt, ds, 1, stream_), "seed");
+  }
+  check_cuda(cudaStreamSynchronize(stream_), "set_pt sync");
+}
+
+void Ensemble::pt_sweeps(int nsweeps, int flags, bool serial, int graph_chunk) {
+  if (pt_.n != n_) throw std::runtime_error("pt_sweeps: call set_pt first");
+  DWeight w{kWeightCanon, 0, 0, 1.0, nullptr, nullptr};
+  if (serial) {
+    std::vector<int> tc;
+    for (int s = 0; s < nsweeps; ++s) {
+      d2h(tc, pt_.temp_chain, n_);
+      for (int k = 0; k < n_; ++k) launch_sweep_range(tc[k], 1, 1, flags | kFlagExtraSetvar, w);
+      check_cuda(launch_exchange(ch_, pt_.temp_chain, pt_.betas, n_, pt_.mt, pt_.iswitch, pt_.wrap,
+                                 pt_.stats, stream_),
+                 "exchange");
+      check_cuda(cudaStreamSynchronize(stream_), "pt sync");
+    }
+    return;
+  }
+  double tol = (flags & kFlagFP32) ? check_tol_fp32 : check_tol;
+  auto enqueue = [&](int k) {
+    for (int i = 0; i < k; ++i) {
+      check_cuda(launch_sweep(set(), ch_, w, 0, n_, 1, flags, tol, stream_), "sweep");
+      check_cuda(launch_exchange(ch_, pt_.temp_chain, pt_.betas, n_, pt_.mt, pt_.iswitch, pt_.wrap,
+                                 pt_.stats, stream_),
+                 "exchange");
+    }
+  };
+  if (graph_chunk <= 1) {
+    enqueue(nsweeps);
+  } else {
+    if (!graph_ || graph_len_ != graph_chunk || graph_flags_ != flags) {
+      if (graph_) cudaGraphExecDestroy(graph_);
+      graph_ = nullptr;
+      // attribute calls happen outside the capture
+      check_cuda(launch_sweep(set(), ch_, w, 0, 0, 0, flags, tol, stream_), "prep");
+      cudaGraph_t g;
+      check_cuda(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture");
+      enqueue(graph_chunk);
+      check_cuda(cudaStreamEndCapture(stream_, &g), "end capture");
+      check_cuda(cudaGraphInstantiate(&graph_, g, 0), "instantiate");
+      cudaGraphDestroy(g);
+      graph_len_ = graph_chunk;
+      graph_flags_ = flags;
+    }
+    int full = nsweeps / graph_chunk, rest = nsweeps % graph_chunk;
+    for (int i = 0; i < full; ++i) check_cuda(cudaGraphLaunch(graph_, stream_), "graph launch");
+    enqueue(rest);
+  }
+  check_cuda(cudaStreamSynchronize(stream_), "pt sync");
+}
+
+void Ensemble::pt_map(std::vector<int>& tc) const { d2h(tc, pt_.temp_chain, pt_.n); }
+void Ensemble::pt_stats(std::vector<unsigned long long>& s) const { d2h(s, pt_.stats, 2 * pt_.n); }
+
+void Ensemble::pt_get_state(std::vector<int>& tc, int& iswitch, std::vector<uint32_t>& mt,
+                            std::vector<double>& betas) const {
+  d2h(tc, pt_.temp_chain, pt_.n);
+  std::vector<int> sw;
+  d2h(sw, pt_.iswitch, 1);
+  iswitch = sw[0];
+  d2h(mt, pt_.mt, 625);
+  d2h(betas, pt_.betas, pt_.n);
+}
+void Ensemble::pt_set_state(const std::vector<int>& tc, int iswitch,
+                            const std::vector<uint32_t>& mt, const std::vector<double>& betas) {
+  if ((int)tc.size() != pt_.n || mt.size() != 625 || (int)betas.size() != pt_.n)
+    throw std::runtime_error("pt_set_state: size");
+  h2d(pt_.temp_chain, tc);
+  h2d(pt_.iswitch, std::vector<int>{iswitch});
+  h2d(pt_.mt, mt);
+  h2d(pt_.betas, betas);
+}
+
+void Ensemble::get_vlvr(std::vector<double>& v) const { d2h(v, ch_.vlvr, (size_t)n_ * ch_.vstride); }
+void Ensemble::set_vlvr(const std::vector<double>& v) {
+  if (v.size() != (size_t)n_ * ch_.vstride) throw std::runtime_error("set_vlvr: size");
+  h2d(ch_.vlvr, v);
+}
+void Ensemble::get_eol(std::vector<double>& e) const { d2h(e, ch_.eol, n_); }
+void Ensemble::get_terms(std::vector<double>& t) const { d2h(t, ch_.terms, (size_t)n_ * 6); }
+void Ensemble::get_acceptance(std::vector<unsigned long long>& a,
+                              std::vector<unsigned long long>& p) const {
+  d2h(a, ch_.nacc, n_);
+  d2h(p, ch_.nprop, n_);
+}
+void Ensemble::get_errors(std::vector<int>& e) const { d2h(e, ch_.err, n_); }
+void Ensemble::get_betas(std::vector<double>& b) const { d2h(b, ch_.beta, n_); }
+void Ensemble::set_betas(const std::vector<double>& b) {
+  if ((int)b.size() != n_) throw std::runtime_error("set_betas: size");
+  h2d(ch_.beta, b);
+}
+void Ensemble::get_mt(std::vector<uint32_t>& m) const { d2h(m, ch_.mt, (size_t)nmt_ * 625); }
+void Ensemble::set_mt(const std::vector<uint32_t>& m) {
+  if (m.size() != (size_t)nmt_ * 625) throw std::runtime_error("set_mt: size");
+  h2d(ch_.mt, m);
+}
+void Ensemble::get_toat(std::vector<double>& t) const { d2h(t, ch_.toat, (size_t)ntoat_ * ch_.tstride); }
+void Ensemble::set_toat(const std::vector<double>& t) {
+  if (t.size() != (size_t)ntoat_ * ch_.tstride) throw std::runtime_error("set_toat: size");
+  h2d(ch_.toat, t);
+}
+
+void Ensemble::get_coords(std::vector<double>& xyz) {
+  // a full rebuild of every chain into a coordinate buffer (state unchanged
+  // apart from the setvar call the reference's energy() also makes)
+  if (!coords_buf_)
+    check_cuda(cudaMalloc(&coords_buf_, (size_t)n_ * 3 * ch_.tstride * sizeof(double)), "malloc");
+  DChains c2 = ch_;
+  c2.coords = coords_buf_;
+  check_cuda(launch_energy(set(), c2, 0, n_, false, stream_), "coords");
+  check_cuda(cudaStreamSynchronize(stream_), "coords sync");
+  d2h(xyz, coords_buf_, (size_t)n_ * 3 * ch_.tstride);
+}
+
+void Ensemble::draw(int slot, int n, std::vector<double>& out) {
+  double* d = nullptr;
+  check_cuda(cudaMalloc(&d, std::max(n, 1) * sizeof(double)), "malloc");
+  check_cuda(launch_draw(ch_.mt, slot, n, d, stream_), "draw");
+  check_cuda(cudaStreamSynchronize(stream_), "draw sync");
+  d2h(out, d, n);
+  cudaFree(d);
+}
+
+}  // namespace smmpb200

@@ -1,0 +1,80 @@
+// Flattened, 0-based topology of one molecule as the GPU kernels read it.
+//
+// flatten() walks an assembled molecule (assembly.hpp) and emits:
+//  * rebuild data: parent atom, bond length, cos/sin of the valence angle, the
+//    atoms grouped by depth below the first backbone atom (one parallel
+//    Eyring step per depth level, bldmol.f:64-78);
+//  * variables: primary atom, base atom, the sibling atoms whose dihedral the
+//    variable shifts (setvar.f:40-56), the contiguous atom range that rotates
+//    with it (setmvs.f:168-199, the range before overlaps are removed), and the
+//    torsion-potential constants (enyshe.f:79-80);
+//  * pair work: every (atom, vdW domain) of mklist.f cut into chunks of at
+//    most 8 consecutive partners, and the 1-4 partners as explicit pairs;
+//  * solvation radii and coefficients (init_molecule.f:194-210).
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "assembly.hpp"
+
+namespace smmpb200 {
+
+constexpr int kNumTypes = 18;     // ECEPP atom classes (INCL.H mxtyat)
+constexpr int kChunk = 8;         // partners per vdW chunk
+constexpr int kMaxAtoms = 16383;  // 14-bit atom index in the packed pair words
+
+// Per type-pair constants, [ti*18+tj].  A/C of the 12-6 (or 12-10 hydrogen
+// bond) term, the halved repulsion of 1-4 pairs, and the squared distance
+// beyond which every van der Waals / H-bond term is below the FP32 guard
+// energy (pairs closer than that are evaluated in FP64 in the mixed mode).
+struct PairTable {
+  double a[kNumTypes * kNumTypes];
+  double a14[kNumTypes * kNumTypes];
+  double c[kNumTypes * kNumTypes];
+  int hb[kNumTypes * kNumTypes];
+  double guard_r2[kNumTypes * kNumTypes];
+};
+
+struct ForceField {
+  PairTable pair;
+  double conv = 166.0;     // 332/eps_s
+  double plt = 78.0, slp = 0.3;
+  int epsd = 0;
+  int itysol = 0;
+  std::vector<double> spoint;   // npnt*3 unit-sphere points
+  int npnt = 0;
+};
+
+struct MolTopo {
+  int natoms = 0, nvar = 0, nfree = 0;
+  int i1 = 0, i2 = 0, i3 = 0;          // first three backbone atoms
+  double gbpr[6] = {0, 0, 0, 0, 0, 0};
+  // atoms
+  std::vector<int> iow;                // parent atom (-1 for i1)
+  std::vector<uint8_t> type;           // 0-based ECEPP class
+  std::vector<double> charge, blen, cba, sba, toat0;
+  std::vector<double> rvdw, sigma;
+  std::vector<int> level_atoms, level_off;   // CSR by depth (level 0 = i1 only)
+  std::vector<int> residue_of_atom;
+  // variables (all torsions of the molecule, fixed ones included)
+  std::vector<int> var_atom, var_base, var_lo, var_hi, var_class, var_fixed;
+  std::vector<int> sib_off, sib;       // CSR of atoms shifted by each variable
+  std::vector<double> var_e0, var_sg, var_rn, axvr, vlvr0;
+  std::vector<int> idvr;               // free variables (0-based var index)
+  std::vector<std::string> var_name, atom_name;
+  std::vector<int> var_residue;
+  // pair work
+  std::vector<uint32_t> chunks;        // i | j0<<14 | (len-1)<<28
+  std::vector<uint32_t> pairs14;       // i | j<<14
+  long long npairs = 0;                // pair terms per full evaluation
+  // solvation
+  std::vector<int> heavy;              // atoms with rvdw > 0
+  int nres = 0;
+};
+
+// Build a MolTopo from molecule nml of an assembled system.
+MolTopo flatten(Assembly& a, int nml);
+ForceField make_forcefield(const Assembly& a);
+
+}  // namespace smmpb200

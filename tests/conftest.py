@@ -1,0 +1,184 @@
+"""Shared fixtures: paths, the CPU oracle (checker) and the product package.
+
+The oracle under oracle/ is test infrastructure: tests load it through ctypes
+to check the product's results; the product never loads it.
+"""
+import ctypes
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "smmp-svn_b200")
+DATA = os.path.join(ROOT, "tests", "golden", "smmp_data") + "/"
+GOLDEN = os.path.join(ROOT, "tests", "golden", "golden.json")
+ORACLE_SO = os.path.join(ROOT, "oracle", "liboracle_smmp.so")
+
+if PKG not in sys.path:
+    sys.path.insert(0, PKG)
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200)")
+    config.addinivalue_line("markers", "slow: runs for more than a few seconds")
+
+
+def _have_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+HAVE_GPU = _have_gpu()
+
+
+def pytest_collection_modifyitems(config, items):
+    if HAVE_GPU:
+        return
+    skip = pytest.mark.skip(reason="no CUDA GPU in this environment")
+    for it in items:
+        if "gpu" in it.keywords:
+            it.add_marker(skip)
+
+
+# ------------------------------------------------------------------ oracle
+def _build_oracle():
+    if not os.path.exists(ORACLE_SO):
+        subprocess.check_call(["make", "-C", os.path.join(ROOT, "oracle")])
+
+
+class Oracle:
+    """ctypes wrapper over oracle/liboracle_smmp.so (one system per object)."""
+
+    _lib = None
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            _build_oracle()
+            L = ctypes.CDLL(ORACLE_SO)
+            L.orc_create.restype = ctypes.c_void_p
+            L.orc_create.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+            L.orc_clone.restype = ctypes.c_void_p
+            L.orc_clone.argtypes = [ctypes.c_void_p]
+            L.orc_last_error.restype = ctypes.c_char_p
+            L.orc_grnd.restype = ctypes.c_double
+            L.orc_grnd.argtypes = [ctypes.c_void_p]
+            L.orc_set_beta.argtypes = [ctypes.c_void_p, ctypes.c_double]
+            L.orc_anneal.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                     ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+            L.orc_bench_chains.restype = ctypes.c_double
+            L.orc_bench_chains.argtypes = [ctypes.c_void_p, ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_int),
+                                           ctypes.POINTER(ctypes.c_double), ctypes.c_int,
+                                           ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+            for f in ["orc_init_molecule", "orc_energy", "orc_sizes", "orc_sweeps",
+                      "orc_sgrnd", "orc_random_start", "orc_get_vlvr", "orc_set_vlvr",
+                      "orc_get_idvr", "orc_get_coords", "orc_get_topology", "orc_partem",
+                      "orc_get_mt", "orc_destroy", "orc_get_toat", "orc_set_rndord",
+                      "orc_get_axvr", "orc_get_names"]:
+                getattr(L, f).argtypes = None
+            cls._lib = L
+        return cls._lib
+
+    def __init__(self, seq, var=None, ff="ecepp3", itysol=0, epsd=0, grpn="nh2", grpc="cooh",
+                 _handle=None):
+        L = self.lib()
+        if _handle is not None:
+            self.h = ctypes.c_void_p(_handle)
+        else:
+            h = L.orc_create(DATA.encode(), 1 if ff == "ecepp2" else 0, int(epsd), int(itysol))
+            assert h, L.orc_last_error()
+            self.h = ctypes.c_void_p(h)
+            rc = L.orc_init_molecule(self.h, seq.encode(), (var or " ").encode(), grpn.encode(),
+                                     grpc.encode())
+            assert rc == 0, L.orc_last_error()
+        sz = (ctypes.c_int * 7)()
+        L.orc_sizes(self.h, sz)
+        self.natoms, self.ntlvr, self.nvr = sz[0], sz[1], sz[2]
+        self.sizes = list(sz)
+
+    def clone(self):
+        return Oracle(None, _handle=self.lib().orc_clone(self.h))
+
+    def energy(self):
+        e = ctypes.c_double()
+        t = (ctypes.c_double * 6)()
+        rc = self.lib().orc_energy(self.h, ctypes.byref(e), t)
+        assert rc == 0, self.lib().orc_last_error()
+        return e.value, list(t)
+
+    def vlvr(self):
+        a = np.zeros(self.ntlvr)
+        self.lib().orc_get_vlvr(self.h, a.ctypes.data_as(ctypes.c_void_p))
+        return a
+
+    def set_vlvr(self, v):
+        a = np.ascontiguousarray(v, dtype=np.float64)
+        self.lib().orc_set_vlvr(self.h, a.ctypes.data_as(ctypes.c_void_p))
+
+    def idvr(self):
+        a = np.zeros(self.nvr, dtype=np.int32)
+        self.lib().orc_get_idvr(self.h, a.ctypes.data_as(ctypes.c_void_p))
+        return a
+
+    def toat(self):
+        a = np.zeros(self.natoms)
+        self.lib().orc_get_toat(self.h, a.ctypes.data_as(ctypes.c_void_p))
+        return a
+
+    def coords(self):
+        a = np.zeros(3 * self.natoms)
+        self.lib().orc_get_coords(self.h, a.ctypes.data_as(ctypes.c_void_p))
+        return a.reshape(-1, 3)
+
+    def sgrnd(self, seed):
+        self.lib().orc_sgrnd(self.h, ctypes.c_int(seed))
+
+    def grnd(self):
+        return self.lib().orc_grnd(self.h)
+
+    def set_beta(self, b):
+        self.lib().orc_set_beta(self.h, b)
+
+    def random_start(self):
+        self.lib().orc_random_start(self.h)
+
+    def sweeps(self, n, log=None):
+        eol, acz = ctypes.c_double(), ctypes.c_double()
+        ptr = log.ctypes.data_as(ctypes.c_void_p) if log is not None else None
+        rc = self.lib().orc_sweeps(self.h, ctypes.c_int(n), ctypes.byref(eol), ctypes.byref(acz),
+                                   ptr)
+        assert rc == 0, self.lib().orc_last_error()
+        return eol.value, acz.value
+
+    def pair_count(self):
+        na, nv = self.natoms, self.ntlvr
+        ai = np.zeros((na, 11), np.int32)
+        ad = np.zeros((na, 4))
+        vi = np.zeros((nv, 9), np.int32)
+        ms = np.zeros((self.sizes[6], 2), np.int32)
+        vw = np.zeros((self.sizes[4], 3), np.int32)
+        l14 = np.zeros((self.sizes[5], 2), np.int32)
+        P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        self.lib().orc_get_topology(self.h, P(ai), P(ad), P(vi), P(ms), P(vw), P(l14))
+        return int((vw[:, 1] - vw[:, 0] + 1).sum()) + len(l14)
+
+
+def seqfile(tmp_path, residues, name="chain"):
+    """Write a sequence file with the given residue names."""
+    p = tmp_path / (name + ".seq")
+    p.write_text("# %s\n%s\n" % (name, " ".join(residues)))
+    return str(p)
+
+
+@pytest.fixture
+def oracle_cls():
+    return Oracle
