@@ -103,10 +103,10 @@ void raise_kernel_errors(Ensemble& e) {
 // (main programs call sgrnd before init_molecule).  Until a molecule is on
 // the GPU it is advanced here; afterwards the GPU copy is authoritative.
 struct HostMT {
-  uint32_t mt[625];
+  uint32_t mt[kMTWords];   // device slot layout with an empty queue
   HostMT() {
     std::memset(mt, 0, sizeof mt);
-    mt[624] = 625;
+    mt[kMTIdx] = 625;
   }
   void seed(uint32_t s) {
     mt[0] = s;
@@ -311,7 +311,7 @@ int smmp_init_molecule(int iabin, const char* grpn, const char* grpc, const char
     u.mol = build_molecule(u.libdir, u.cfg, seqfile, var, grpn ? grpn : "nh2",
                            grpc ? grpc : "cooh");
     u.ens.reset(new Ensemble({u.mol}, {0}, {4357}, {u.beta}, true));
-    std::vector<uint32_t> mt(u.mt.mt, u.mt.mt + 625);
+    std::vector<uint32_t> mt(u.mt.mt, u.mt.mt + kMTWords);
     u.ens->set_mt(mt);
   });
 }
@@ -379,7 +379,7 @@ int smmp_sgrnd(int32_t seed) {
   return guard([&] {
     Universe& u = U();
     u.mt.seed((uint32_t)seed);
-    if (u.ens) u.ens->set_mt(std::vector<uint32_t>(u.mt.mt, u.mt.mt + 625));
+    if (u.ens) u.ens->set_mt(std::vector<uint32_t>(u.mt.mt, u.mt.mt + kMTWords));
   });
 }
 
@@ -829,23 +829,22 @@ int smmp_ens_restore(smmp_ens_t* e, const void* buf, uint64_t bytes) {
     get(p, end, to, h.ntoat * h.tstride);
     get(p, end, be, h.nchains);
     get(p, end, eo, h.nchains);
-    get(p, end, mt, h.nmt * 625);
+    get(p, end, mt, h.nmt * kMTWords);
     get(p, end, acc, h.nchains);
     get(p, end, prop, h.nchains);
     en.set_vlvr(vl);
     en.set_toat(to);
     en.set_betas(be);
     en.set_mt(mt);
+    en.set_acceptance(acc, prop);
     if (h.npt) {
       need(en.has_pt(), "checkpoint holds a PT state; call smmp_ens_set_pt first");
       get(p, end, tc, h.npt);
-      get(p, end, ptmt, 625);
+      get(p, end, ptmt, kMTWords);
       get(p, end, ptb, h.npt);
       en.pt_set_state(tc, (int)h.iswitch, ptmt, ptb);
     }
     (void)eo;
-    (void)acc;
-    (void)prop;
   });
 }
 

@@ -6,9 +6,17 @@ namespace smmpb200 {
 
 constexpr int kTypes = 18;
 constexpr int kTP = kTypes * kTypes;
-constexpr int kThreads = 256;            // threads per chain (one CTA per chain)
+constexpr int kThreads = 512;            // threads per chain (one CTA per chain)
 constexpr int kWarps = kThreads / 32;
 constexpr int kMaxNeighbours = 128;      // SASA neighbours per atom (per-warp buffer)
+
+// An MT19937 stream slot: 624 state words, mti, the head and tail counters
+// of a queue of tempered values already drawn from the state but not yet
+// consumed, padding, then the queue (64 doubles).  The stream a slot yields is
+// the queue in order, then grnd() of the state (twister.f:104-177).
+constexpr int kMTWords = 768;
+constexpr int kQueue = 64;
+constexpr int kMTIdx = 624, kQHead = 625, kQTail = 626, kQOff = 640;
 
 // One molecule, GPU resident (all indices 0-based, see topology.hpp).
 struct DMol {
@@ -86,7 +94,7 @@ struct DChains {
   double* toat;          // [slot * tstride + atom]  (phase-constant dihedral state)
   int tstride;
   const int* toat_slot;
-  uint32_t* mt;          // [slot * 625]: 624 words, then mti
+  uint32_t* mt;          // [slot * kMTWords] stream slots
   const int* mt_slot;
   double* beta;          // current inverse temperature of each chain
   double* eol;           // energy of the current conformation

@@ -1,20 +1,31 @@
 // sm_100a kernels of the SMMP energy-and-sweep path.
 //
 //  k_seed         per-stream MT19937 seeding (twister.f sgrnd, Knuth 69069)
-//  k_draw         draw numbers from a stream (grnd) -- RNG parity and the
-//                 host-facing grnd() entry point
+//  k_draw         draw numbers from a stream (grnd)
 //  k_random_start canonical random start (canon.f:60-67)
 //  k_energy       setvar + full Eyring rebuild + ECEPP/3 (+ SASA) energy of a
-//                 batch of conformations, one CTA each (energy.f)
+//                 set of chains, one CTA each (energy.f)
 //  k_sweep        persistent Metropolis sweeps, one CTA per chain
-//                 (metropolis.f): per proposal an in-place rotation of the
-//                 moving subtree, the full pair energy over the mklist lists,
-//                 and the acceptance test in FP64
+//                 (metropolis.f)
 //  k_exchange     parallel-tempering exchange step (partem_s.f:210-232)
 //
 // One CTA owns one chain: coordinates, dihedral state, variables and the
-// chain's MT19937 state live in shared memory for the whole launch; the
-// per-molecule topology is read through the read-only cache.
+// chain's MT19937 stream live in shared memory for the whole launch; the
+// molecule's topology is read through the read-only cache.
+//
+// The proposal loop of k_sweep is built for latency, since one chain's
+// proposals are strictly sequential:
+//  * the dihedral state follows setvar's arithmetic exactly, but the
+//    coordinates move by an in-place rotation of the variable's subtree
+//    (a full Eyring rebuild runs at the start and end of every sweep);
+//  * random numbers are tempered ahead into a per-chain queue together with
+//    their logarithms, so the acceptance test exp(-d) >= r is decided by
+//    comparing -d with log(r) (exp is evaluated only within 1e-10 of the
+//    threshold, where the comparison could differ);
+//  * while the pair energy of proposal k is evaluated, one warp prepares
+//    proposal k+1 for both possible RNG positions (k drew one or two numbers);
+//  * every warp reduces the pair sums and takes the accept/reject decision
+//    itself, so there is no serial single-thread phase.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -30,20 +41,30 @@ constexpr double kPi = 3.141592653589793;
 constexpr double kPi2 = 2.0 * kPi;
 
 // ---------------------------------------------------------------- angles
-// difang.f:12-33 / :38-60 -- wrap into (-pi, pi] with Fortran MOD (fmod).
+// Fortran MOD(d, 2*pi) (difang.f:25, :51).  For |d| < 4*pi the result is
+// d - sign(2*pi, d), exact by Sterbenz's lemma, with MOD's sign convention.
+__device__ __forceinline__ double mod2pi(double d) {
+  double a = fabs(d);
+  if (a < kPi2) return d;
+  if (a < 2.0 * kPi2) {
+    double r = __dsub_rn(d, copysign(kPi2, d));
+    return r == 0.0 ? copysign(0.0, d) : r;
+  }
+  return fmod(d, kPi2);
+}
+// difang.f:12-33 / :38-60: wrap into (-pi, pi].
 __device__ __forceinline__ double wrap_pi(double d) {
-  d = fmod(d, kPi2);
+  d = mod2pi(d);
   return fabs(d) <= kPi ? d : __dsub_rn(d, copysign(kPi2, d));
 }
 __device__ __forceinline__ double difang(double a1, double a2) { return wrap_pi(__dsub_rn(a2, a1)); }
 __device__ __forceinline__ double addang(double a1, double a2) { return wrap_pi(__dadd_rn(a1, a2)); }
 
 // ---------------------------------------------------------------- MT19937
-// State layout: 624 words followed by mti (twister.f /myblock/).
-__device__ void mt_seed(uint32_t* mt, uint32_t seed) {
-  mt[0] = seed;
-  for (int i = 1; i < 624; ++i) mt[i] = 69069u * mt[i - 1];
-  mt[624] = 624;
+__device__ void mt_seed(uint32_t* slot, uint32_t seed) {
+  slot[0] = seed;
+  for (int i = 1; i < 624; ++i) slot[i] = 69069u * slot[i - 1];
+  slot[kMTIdx] = 624;
 }
 __device__ void mt_twist(uint32_t* mt) {
   const uint32_t MATA = 0x9908B0DFu, UM = 0x80000000u, LM = 0x7fffffffu;
@@ -60,30 +81,81 @@ __device__ void mt_twist(uint32_t* mt) {
   y = (mt[623] & UM) | (mt[0] & LM);
   mt[623] = mt[396] ^ (y >> 1) ^ ((y & 1u) ? MATA : 0u);
 }
-// grnd (twister.f:104-177): tempered word / (2^32 - 1), in [0, 1].
-__device__ double mt_grnd(uint32_t* mt) {
-  uint32_t mti = mt[624];
-  if (mti >= 624) {
-    if (mti == 625) mt_seed(mt, 4357u);
-    mt_twist(mt);
-    mti = 0;
-  }
-  uint32_t y = mt[mti];
-  mt[624] = mti + 1;
+__device__ __forceinline__ double temper(uint32_t y) {
   y ^= (y >> 11);
   y ^= (y << 7) & 0x9D2C5680u;
   y ^= (y << 15) & 0xEFC60000u;
   y ^= (y >> 18);
-  return __ddiv_rn((double)y, 4294967295.0);
+  return __ddiv_rn((double)y, 4294967295.0);   // twister.f:172-176
+}
+// grnd() of the state words only (twister.f:104-177).
+__device__ double mt_grnd(uint32_t* slot) {
+  uint32_t mti = slot[kMTIdx];
+  if (mti >= 624) {
+    if (mti == 625) mt_seed(slot, 4357u);
+    mt_twist(slot);
+    mti = 0;
+  }
+  slot[kMTIdx] = mti + 1;
+  return temper(slot[mti]);
+}
+__device__ __forceinline__ double* qbuf(uint32_t* slot) { return reinterpret_cast<double*>(slot + kQOff); }
+// Next number of a stream slot: queued values first, then the state.
+__device__ double stream_next(uint32_t* slot) {
+  uint32_t h = slot[kQHead], t = slot[kQTail];
+  if (h != t) {
+    slot[kQHead] = h + 1;
+    return qbuf(slot)[h & (kQueue - 1)];
+  }
+  return mt_grnd(slot);
+}
+// Append 32 values to the queue, and their logarithms to lq (one warp).
+__device__ void rng_refill_warp(uint32_t* slot, double* lq) {
+  const int lane = threadIdx.x & 31;
+  if (lane == 0 && slot[kMTIdx] == 625) mt_seed(slot, 4357u);
+  __syncwarp();
+  uint32_t mti = slot[kMTIdx], qt = slot[kQTail];
+  double* q = qbuf(slot);
+  int n1 = min(32, 624 - (int)mti);
+  if (lane < n1) {
+    double v = temper(slot[mti + lane]);
+    int k = (qt + lane) & (kQueue - 1);
+    q[k] = v;
+    lq[k] = v > 0.0 ? log(v) : -INFINITY;
+  }
+  __syncwarp();
+  if (n1 < 32) {
+    if (lane == 0) mt_twist(slot);
+    __syncwarp();
+    int n2 = 32 - n1;
+    if (lane < n2) {
+      double v = temper(slot[lane]);
+      int k = (qt + n1 + lane) & (kQueue - 1);
+      q[k] = v;
+      lq[k] = v > 0.0 ? log(v) : -INFINITY;
+    }
+    mti = n2;
+  } else {
+    mti += 32;
+  }
+  __syncwarp();
+  if (lane == 0) {
+    slot[kMTIdx] = mti;
+    slot[kQTail] = qt + 32;
+  }
+  __syncwarp();
 }
 
 // ---------------------------------------------------------------- shared memory
+struct Proposal {
+  int jv, ivar, used;   // variable, its index in idvr, RNG values its setup consumed
+  double vold, vnew, cth, sth;
+};
+
 struct Scalars {
-  int jv, accept, busy;
-  double vold, vnew, theta_c, theta_s;
-  double ax, ay, az, px, py, pz;   // rotation axis and pivot (base atom)
-  double enew, eol;
-  double sum[5];
+  Proposal cur;
+  Proposal spec[2];      // next proposal if this one draws 1 (spec[0]) or 2 (spec[1]) numbers
+  int refill;
 };
 
 struct Smem {
@@ -93,8 +165,10 @@ struct Smem {
   double *cq;
   uint8_t* type;
   double* vlvr;
-  uint32_t* mt;
-  double* red;
+  double* et;            // torsion energy of each variable (enyshe.f:79-80)
+  uint32_t* mt;          // stream slot (kMTWords)
+  double* lq;            // log of the queued values
+  double* red;           // [kWarps][8] partial sums
   double *ta, *ta14, *tc, *tg;
   int* thb;
   double* spt;
@@ -105,7 +179,6 @@ struct Smem {
 
 __host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~size_t(15); }
 
-// Shared-memory carve-up for up to `n` atoms and `v` variables.
 __host__ __device__ inline size_t smem_layout(int n, int v, int npnt, bool sasa, Smem* s,
                                               char* base) {
   size_t off = 0;
@@ -129,7 +202,9 @@ __host__ __device__ inline size_t smem_layout(int n, int v, int npnt, bool sasa,
   t.cq = (double*)take(8 * n);
   t.type = (uint8_t*)take(n);
   t.vlvr = (double*)take(8 * (v > 0 ? v : 1));
-  t.mt = (uint32_t*)take(4 * 625);
+  t.et = (double*)take(8 * (v > 0 ? v : 1));
+  t.mt = (uint32_t*)take(4 * kMTWords);
+  t.lq = (double*)take(8 * kQueue);
   t.red = (double*)take(8 * kWarps * 8);
   t.ta = (double*)take(8 * kTP);
   t.ta14 = (double*)take(8 * kTP);
@@ -151,7 +226,13 @@ __device__ Smem carve(const DMolSet& set, bool sasa) {
   return s;
 }
 
-// Copy force-field tables and the molecule's per-atom constants.
+__device__ const DMol& stage_mol(const DMolSet& set, const DChains& ch, int c, Smem& s) {
+  if (threadIdx.x == 0) *s.mol = set.mols[ch.mol_of_chain[c]];
+  __syncthreads();
+  return *s.mol;
+}
+
+// Force-field tables and the molecule's per-atom constants.
 __device__ void load_static(const DForceField& ff, const DMol& m, Smem& s, bool sasa) {
   for (int k = threadIdx.x; k < kTP; k += blockDim.x) {
     s.ta[k] = ff.a[k];
@@ -169,12 +250,14 @@ __device__ void load_static(const DForceField& ff, const DMol& m, Smem& s, bool 
 }
 
 // ---------------------------------------------------------------- setvar
-// setvar.f:30-56 for every variable of the molecule (one thread each; each
-// variable shifts only the children of its own base, so threads never touch
-// the same atom).  Returns this thread's share of the torsion energy
-// (enyshe.f:70-80).
-__device__ double setvar_all(const DMol& m, Smem& s) {
-  double evr = 0.0;
+// setvar.f:30-56 for every variable (one thread each; a variable shifts only
+// the children of its own base, so threads never write the same atom).  The
+// torsion energy of a variable is refreshed when its dihedral moved.
+__device__ __forceinline__ double torsion_term(const DMol& m, int v, double to) {
+  double e0 = __ldg(&m.var_e0[v]);
+  return e0 != 0.0 ? e0 * (1.0 + __ldg(&m.var_sg[v]) * cos(to * __ldg(&m.var_rn[v]))) : 0.0;
+}
+__device__ void setvar_all(const DMol& m, Smem& s) {
   for (int v = threadIdx.x; v < m.nvar; v += blockDim.x) {
     int iat = __ldg(&m.var_atom[v]);
     double tsh = difang(s.toat[iat], s.vlvr[v]);
@@ -185,17 +268,14 @@ __device__ double setvar_all(const DMol& m, Smem& s) {
         double to = __dadd_rn(s.toat[jat], tsh);
         if (fabs(to) > kPi) to = __dsub_rn(to, copysign(kPi2, to));
         s.toat[jat] = to;
-        double sv, cv;
-        sincos(to, &sv, &cv);
-        s.sn[jat] = sv;
-        s.cs[jat] = cv;
       }
+      s.et[v] = torsion_term(m, v, s.toat[iat]);
     }
-    double e0 = __ldg(&m.var_e0[v]);
-    if (e0 != 0.0)
-      evr += e0 * (1.0 + __ldg(&m.var_sg[v]) * cos(s.toat[iat] * __ldg(&m.var_rn[v])));
   }
-  return evr;
+}
+__device__ void torsion_all(const DMol& m, Smem& s) {
+  for (int v = threadIdx.x; v < m.nvar; v += blockDim.x)
+    s.et[v] = torsion_term(m, v, s.toat[__ldg(&m.var_atom[v])]);
 }
 
 // ---------------------------------------------------------------- rebuild
@@ -273,8 +353,16 @@ __device__ __forceinline__ void eyring(const DMol& m, Smem& s, int i, int ia) {
 }
 
 // Full rebuild of all coordinates from the dihedral state (bldmol.f:13-93):
-// the first frame, then one parallel Eyring step per depth level.
+// sin/cos of every dihedral, the first frame, then one Eyring step per
+// depth level.
 __device__ void full_rebuild(const DMol& m, Smem& s) {
+  for (int k = threadIdx.x; k < m.natoms; k += blockDim.x) {
+    double sv, cv;
+    sincos(s.toat[k], &sv, &cv);
+    s.sn[k] = sv;
+    s.cs[k] = cv;
+  }
+  __syncthreads();
   if (threadIdx.x == 0) first_frame(m, s);
   __syncthreads();
   for (int L = 1; L < m.nlevels; ++L) {
@@ -327,17 +415,19 @@ __device__ __forceinline__ void pair_term(const FFScalars& ff, const Smem& s, in
   }
 }
 
+// Pair sums of the threads [0, nthr): vdW chunks (8 partners each) and 1-4
+// pairs, both from the mklist lists.
 template <bool F32>
-__device__ void pair_energy(const FFScalars& ff, const DMol& m, const Smem& s, double& el,
-                            double& vw, double& hb) {
-  int nwork = m.nchunks * 8;
-  for (int t = threadIdx.x; t < nwork; t += blockDim.x) {
+__device__ void pair_energy(const FFScalars& ff, const DMol& m, const Smem& s, int tid, int nthr,
+                            double& el, double& vw, double& hb) {
+  const int nwork = m.nchunks * 8;
+  for (int t = tid; t < nwork; t += nthr) {
     uint32_t w = __ldg(&m.chunks[t >> 3]);
     int l = t & 7;
     int len = int((w >> 28) & 7u) + 1;
     if (l < len) pair_term<F32>(ff, s, int(w & 0x3fffu), int((w >> 14) & 0x3fffu) + l, false, el, vw, hb);
   }
-  for (int t = threadIdx.x; t < m.n14; t += blockDim.x) {
+  for (int t = tid; t < m.n14; t += nthr) {
     uint32_t w = __ldg(&m.pairs14[t]);
     pair_term<F32>(ff, s, int(w & 0x3fffu), int(w >> 14), true, el, vw, hb);
   }
@@ -347,15 +437,16 @@ __device__ void pair_energy(const FFScalars& ff, const DMol& m, const Smem& s, d
 // enysol.f:192-306: an atom's sphere point is exposed when it lies outside
 // every neighbour sphere (neighbours: d <= r_i + r_j).  FP64 with the
 // reference's division and summation order and no fused multiply-add, so the
-// exposed-point counts are those of the reference arithmetic.  One warp per
-// heavy atom; returns this thread's share of eysl (and of the SASA).
-__device__ double sasa_energy(const FFScalars& ff, const DMol& m, Smem& s, int* err,
-                              double* asa_out) {
+// exposed-point counts are those of the reference arithmetic.  Warps
+// [w0, w0+nw) take one heavy atom at a time; returns this thread's share of
+// eysl.
+__device__ double sasa_energy(const FFScalars& ff, const DMol& m, Smem& s, int w0, int nw,
+                              int* err) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double* nb = s.nb + (size_t)warp * kMaxNeighbours * 4;
-  double eysl = 0.0, asa = 0.0;
+  double eysl = 0.0;
   const int npnt = ff.npnt;
-  for (int h = warp; h < m.nheavy; h += kWarps) {
+  for (int h = warp - w0; h < m.nheavy; h += nw) {
     int i = __ldg(&m.heavy[h]);
     double trad = __ldg(&m.rvdw[i]);
     double xi = s.x[i], yi = s.y[i], zi = s.z[i];
@@ -418,49 +509,51 @@ __device__ double sasa_energy(const FFScalars& ff, const DMol& m, Smem& s, int* 
     if (lane == 0) {
       double sdr = __ddiv_rn(__dmul_rn(__dmul_rn(4.0 * kPi, trad), trad), (double)npnt);
       double area = __dmul_rn(sdr, (double)cnt);
-      asa += area;
       eysl += __dmul_rn(area, __ldg(&m.sigma[i]));
     }
     __syncwarp();
   }
-  if (asa_out) *asa_out = asa;
   return eysl;
 }
 
 // ---------------------------------------------------------------- reduction
-// Block sum of 5 values; result valid in thread 0 (s.sc->sum).
-__device__ void block_sum5(Smem& s, double v0, double v1, double v2, double v3, double v4) {
+// Warp partials of (eyel, eyvw, eyhb, eyvr, eysl) into s.red[warp].
+__device__ __forceinline__ void warp_partials(Smem& s, double v0, double v1, double v2, double v3,
+                                              double v4) {
   double v[5] = {v0, v1, v2, v3, v4};
 #pragma unroll
   for (int k = 0; k < 5; ++k)
     for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
-  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0)
+  if ((threadIdx.x & 31) == 0) {
+    int w = threadIdx.x >> 5;
 #pragma unroll
-    for (int k = 0; k < 5; ++k) s.red[warp * 8 + k] = v[k];
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int k = 0; k < 5; ++k) {
-      double acc = 0.0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) acc += s.red[w * 8 + k];
-      s.sc->sum[k] = acc;
-    }
+    for (int k = 0; k < 5; ++k) s.red[w * 8 + k] = v[k];
   }
 }
-
-// Full evaluation of the current coordinates: per-thread partials of
-// (eyel, eyvw, eyhb, eysl) plus the torsion share passed in; block-reduced.
-template <bool F32>
-__device__ void evaluate(const FFScalars& ff, const DMol& m, Smem& s, double evr, int* err) {
-  double el = 0.0, vw = 0.0, hb = 0.0, sl = 0.0;
-  pair_energy<F32>(ff, m, s, el, vw, hb);
-  if (ff.itysol > 0) sl = sasa_energy(ff, m, s, err, nullptr);
-  block_sum5(s, el, vw, hb, evr, sl);
+// Every warp sums the warp partials the same way (call after a barrier).
+__device__ __forceinline__ void all_sums(const Smem& s, double* out) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    double v = lane < kWarps ? s.red[lane * 8 + k] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    out[k] = v;
+  }
 }
-
 __device__ __forceinline__ double total_of(const double* sum) {
   // energy.f: eysm = eyel + eyvw + eyhb + eyvr, then + eysl
   return ((sum[0] + sum[1]) + sum[2]) + sum[3] + sum[4];
+}
+
+// Full evaluation of the current coordinates by the whole block; partials in
+// s.red (read them with all_sums after a barrier).
+template <bool F32>
+__device__ void evaluate_block(const FFScalars& ff, const DMol& m, Smem& s, int* err) {
+  double el = 0.0, vw = 0.0, hb = 0.0, sl = 0.0, vr = 0.0;
+  pair_energy<F32>(ff, m, s, threadIdx.x, blockDim.x, el, vw, hb);
+  for (int v = threadIdx.x; v < m.nvar; v += blockDim.x) vr += s.et[v];
+  if (ff.itysol > 0) sl = sasa_energy(ff, m, s, 0, kWarps, err);
+  warp_partials(s, el, vw, hb, vr, sl);
 }
 
 // Sampling weight (canon.f:135-149, mulcan_par_mod.f90:380-410), FP64 with
@@ -479,21 +572,42 @@ __device__ __forceinline__ void set_err(int* err, int code) {
   if (*err == 0) *err = code;
 }
 
+// Prepare a proposal (metropolis.f:42-66) from queue position `pos`:
+// variable, new value and the cos/sin of the rotation it implies.
+__device__ void make_proposal(const DMol& m, const Smem& s, int p, uint32_t pos, bool rndord,
+                              Proposal& out) {
+  const double* q = qbuf(s.mt);
+  uint32_t k = pos;
+  int ivar = p;
+  if (rndord) {
+    ivar = (int)__dmul_rn((double)m.nfree, q[k & (kQueue - 1)]);
+    if (ivar >= m.nfree) ivar = m.nfree - 1;
+    ++k;
+  }
+  int jv = __ldg(&m.idvr[ivar]);
+  double vold = s.vlvr[jv];
+  double dv = __dmul_rn(__ldg(&m.axvr[jv]), __dsub_rn(q[k & (kQueue - 1)], 0.5));
+  ++k;
+  double vnew = addang(vold, dv);
+  double sv, cv;
+  sincos(difang(vold, vnew), &sv, &cv);
+  out.jv = jv;
+  out.ivar = ivar;
+  out.used = (int)(k - pos);
+  out.vold = vold;
+  out.vnew = vnew;
+  out.cth = cv;
+  out.sth = sv;
+}
+
 // Load the chain's state into shared memory.
 __device__ void load_chain(const DChains& ch, const DMol& m, int c, Smem& s) {
   const double* tg = ch.toat + (size_t)ch.toat_slot[c] * ch.tstride;
-  for (int k = threadIdx.x; k < m.natoms; k += blockDim.x) {
-    double t = tg[k];
-    s.toat[k] = t;
-    double sv, cv;
-    sincos(t, &sv, &cv);
-    s.sn[k] = sv;
-    s.cs[k] = cv;
-  }
+  for (int k = threadIdx.x; k < m.natoms; k += blockDim.x) s.toat[k] = tg[k];
   const double* vg = ch.vlvr + (size_t)c * ch.vstride;
   for (int k = threadIdx.x; k < m.nvar; k += blockDim.x) s.vlvr[k] = vg[k];
-  const uint32_t* mg = ch.mt + (size_t)ch.mt_slot[c] * 625;
-  for (int k = threadIdx.x; k < 625; k += blockDim.x) s.mt[k] = mg[k];
+  const uint32_t* mg = ch.mt + (size_t)ch.mt_slot[c] * kMTWords;
+  for (int k = threadIdx.x; k < kMTWords; k += blockDim.x) s.mt[k] = mg[k];
 }
 
 __device__ void store_chain(const DChains& ch, const DMol& m, int c, Smem& s) {
@@ -501,8 +615,8 @@ __device__ void store_chain(const DChains& ch, const DMol& m, int c, Smem& s) {
   for (int k = threadIdx.x; k < m.natoms; k += blockDim.x) tg[k] = s.toat[k];
   double* vg = ch.vlvr + (size_t)c * ch.vstride;
   for (int k = threadIdx.x; k < m.nvar; k += blockDim.x) vg[k] = s.vlvr[k];
-  uint32_t* mg = ch.mt + (size_t)ch.mt_slot[c] * 625;
-  for (int k = threadIdx.x; k < 625; k += blockDim.x) mg[k] = s.mt[k];
+  uint32_t* mg = ch.mt + (size_t)ch.mt_slot[c] * kMTWords;
+  for (int k = threadIdx.x; k < kMTWords; k += blockDim.x) mg[k] = s.mt[k];
   if (ch.coords) {
     double* cg = ch.coords + (size_t)c * 3 * ch.tstride;
     for (int k = threadIdx.x; k < m.natoms; k += blockDim.x) {
@@ -513,18 +627,29 @@ __device__ void store_chain(const DChains& ch, const DMol& m, int c, Smem& s) {
   }
 }
 
+__device__ void write_terms(const DChains& ch, int c, const double* sum) {
+  double* t = ch.terms + (size_t)c * 6;
+  for (int k = 0; k < 5; ++k) t[k] = sum[k];
+  t[5] = ((sum[0] + sum[1]) + sum[2]) + sum[3];
+}
+
 }  // namespace
 
 // ============================================================================ kernels
 
 __global__ void k_seed(uint32_t* mt, const int* seeds, int nslots) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < nslots) mt_seed(mt + (size_t)i * 625, (uint32_t)seeds[i]);
+  if (i < nslots) {
+    uint32_t* slot = mt + (size_t)i * kMTWords;
+    mt_seed(slot, (uint32_t)seeds[i]);
+    slot[kQHead] = 0;
+    slot[kQTail] = 0;
+  }
 }
 
 __global__ void k_draw(uint32_t* mt, int slot, int n, double* out) {
   if (threadIdx.x == 0 && blockIdx.x == 0)
-    for (int i = 0; i < n; ++i) out[i] = mt_grnd(mt + (size_t)slot * 625);
+    for (int i = 0; i < n; ++i) out[i] = stream_next(mt + (size_t)slot * kMTWords);
 }
 
 // canon.f:60-67 random start, chains visited in the given order so that a
@@ -534,21 +659,14 @@ __global__ void k_random_start(DMolSet set, DChains ch, const int* order, int n)
   for (int q = 0; q < n; ++q) {
     int c = order[q];
     const DMol& m = set.mols[ch.mol_of_chain[c]];
-    uint32_t* mt = ch.mt + (size_t)ch.mt_slot[c] * 625;
+    uint32_t* slot = ch.mt + (size_t)ch.mt_slot[c] * kMTWords;
     double* vl = ch.vlvr + (size_t)c * ch.vstride;
     for (int i = 0; i < m.nfree; ++i) {
       int iv = m.idvr[i];
-      double dv = __dmul_rn(m.axvr[iv], __dsub_rn(mt_grnd(mt), 0.5));
+      double dv = __dmul_rn(m.axvr[iv], __dsub_rn(stream_next(slot), 0.5));
       vl[iv] = addang(kPi, dv);
     }
   }
-}
-
-// Copy the chain's molecule descriptor into shared memory (thread 0).
-__device__ const DMol& stage_mol(const DMolSet& set, const DChains& ch, int c, Smem& s) {
-  if (threadIdx.x == 0) *s.mol = set.mols[ch.mol_of_chain[c]];
-  __syncthreads();
-  return *s.mol;
 }
 
 // energy(): setvar + rebuild + energy for chains [first, first+gridDim.x).
@@ -563,18 +681,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_energy(DMolSet set, DChains ch,
   load_static(*set.ff, m, s, sasa);
   load_chain(ch, m, c, s);
   __syncthreads();
-  double evr = setvar_all(m, s);
+  setvar_all(m, s);
   __syncthreads();
+  torsion_all(m, s);
   full_rebuild(m, s);
-  evaluate<F32>(set.f, m, s, evr, &ch.err[c]);
+  evaluate_block<F32>(set.f, m, s, &ch.err[c]);
   __syncthreads();
+  double sum[5];
+  all_sums(s, sum);
   if (threadIdx.x == 0) {
-    const double* sum = s.sc->sum;
     double e = total_of(sum);
     ch.eol[c] = e;
-    double* t = ch.terms + (size_t)c * 6;
-    for (int k = 0; k < 5; ++k) t[k] = sum[k];
-    t[5] = ((sum[0] + sum[1]) + sum[2]) + sum[3];
+    write_terms(ch, c, sum);
     if (!isfinite(e)) set_err(&ch.err[c], kErrNonFinite);
   }
   store_chain(ch, m, c, s);
@@ -590,9 +708,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_energy(DMolSet set, DChains ch,
 // after the setvar call the reference makes there.
 template <bool F32>
 __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, DWeight w, int first,
-                                                    int nsweeps, int flags, double check_tol) {
-  int c = first + blockIdx.x;
+                                                       int nsweeps, int flags, double check_tol) {
+  const int c = first + blockIdx.x;
   const bool sasa = set.f.itysol > 0;
+  const bool rndord = (flags & kFlagRndOrd) != 0;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int spec_warp = kWarps - 1;            // prepares the next proposal
+  const int nthr_pairs = (kWarps - 1) * 32;    // the other warps evaluate pairs
   Smem s = carve(set, sasa);
   Scalars& sc = *s.sc;
   const DMol& m = stage_mol(set, ch, c, s);
@@ -602,63 +724,61 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
   int* err = &ch.err[c];
   unsigned long long nacc = 0, nprop = 0;
   __syncthreads();
+  // logs of the values already queued, then fill the queue
+  if (warp == spec_warp) {
+    uint32_t h = s.mt[kQHead], t = s.mt[kQTail];
+    const double* q = qbuf(s.mt);
+    for (uint32_t k = h + lane; k < t; k += 32) {
+      double v = q[k & (kQueue - 1)];
+      s.lq[k & (kQueue - 1)] = v > 0.0 ? log(v) : -INFINITY;
+    }
+    __syncwarp();
+    while (s.mt[kQTail] - s.mt[kQHead] < 24) rng_refill_warp(s.mt, s.lq);
+  }
+  torsion_all(m, s);
+  __syncthreads();
+  uint32_t head = s.mt[kQHead];   // identical in every thread from here on
+  double eol = ch.eol[c], enew = 0.0;
+  bool fresh = false;
 
-  bool fresh = false;   // coordinates and sc.enew hold the current conformation
   for (int sw = 0; sw < nsweeps; ++sw) {
     if (flags & kFlagExtraSetvar) {   // partem_s.f:194-198: setvar(i, vlvr) first
       setvar_all(m, s);
       __syncthreads();
-      full_rebuild(m, s);
       fresh = false;
     }
-    // eol = energy() (metropolis.f:35)
-    double evr = setvar_all(m, s);
+    // ---- eol = energy() (metropolis.f:35)
+    setvar_all(m, s);
     __syncthreads();
     if (!fresh) {
       full_rebuild(m, s);
-      evaluate<F32>(set.f, m, s, evr, err);
+      evaluate_block<F32>(set.f, m, s, err);
       __syncthreads();
-      if (threadIdx.x == 0) sc.enew = total_of(sc.sum);
+      double sum[5];
+      all_sums(s, sum);
+      enew = total_of(sum);
     }
-    if (threadIdx.x == 0) sc.eol = sc.enew;
+    eol = enew;
+    if (m.nfree > 0 && threadIdx.x == 0) {
+      make_proposal(m, s, 0, head, rndord, sc.cur);
+      s.vlvr[sc.cur.jv] = sc.cur.vnew;
+      sc.refill = 0;
+    }
     __syncthreads();
 
     for (int p = 0; p < m.nfree; ++p) {
-      // ---- proposal (thread 0): variable, step, rotation of its subtree
-      if (threadIdx.x == 0) {
-        int ivar = (flags & kFlagRndOrd) ? (int)(m.nfree * mt_grnd(s.mt)) : p;
-        if (ivar >= m.nfree) ivar = m.nfree - 1;
-        int jv = __ldg(&m.idvr[ivar]);
-        double vold = s.vlvr[jv];
-        double dv = __dmul_rn(__ldg(&m.axvr[jv]), __dsub_rn(mt_grnd(s.mt), 0.5));
-        double vnew = addang(vold, dv);
-        s.vlvr[jv] = vnew;
-        sc.jv = jv;
-        sc.vold = vold;
-        double th = difang(vold, vnew);
-        double sv, cv;
-        sincos(th, &sv, &cv);
-        sc.theta_s = sv;
-        sc.theta_c = cv;
-        int b = __ldg(&m.var_base[jv]), a = __ldg(&m.iow[b]);
-        double ax = s.x[b] - s.x[a], ay = s.y[b] - s.y[a], az = s.z[b] - s.z[a];
-        double inv = rsqrt(ax * ax + ay * ay + az * az);
-        sc.ax = ax * inv;
-        sc.ay = ay * inv;
-        sc.az = az * inv;
-        sc.px = s.x[b];
-        sc.py = s.y[b];
-        sc.pz = s.z[b];
-      }
-      __syncthreads();
-      // ---- setvar for all variables (exact dihedral state) + torsion energy
-      double evr2 = setvar_all(m, s);
-      // ---- rotate the subtree of jv about its bond (right-hand rule, +theta)
+      const Proposal cur = sc.cur;
+      const int lo = __ldg(&m.var_lo[cur.jv]), hi = __ldg(&m.var_hi[cur.jv]);
+      // ---- phase A: exact dihedral state + torsion terms; rotate the subtree
+      setvar_all(m, s);
       {
-        int jv = sc.jv;
-        int lo = __ldg(&m.var_lo[jv]), hi = __ldg(&m.var_hi[jv]);
-        double kx = sc.ax, ky = sc.ay, kz = sc.az, cth = sc.theta_c, sth = sc.theta_s;
-        double px = sc.px, py = sc.py, pz = sc.pz;
+        int b = __ldg(&m.var_base[cur.jv]), a = __ldg(&m.iow[b]);
+        double px = s.x[b], py = s.y[b], pz = s.z[b];
+        double kx = px - s.x[a], ky = py - s.y[a], kz = pz - s.z[a];
+        double inv = rsqrt(kx * kx + ky * ky + kz * kz);
+        kx *= inv;
+        ky *= inv;
+        kz *= inv;
         for (int k = lo + threadIdx.x; k <= hi; k += blockDim.x) {
           double vx = s.x[k] - px, vy = s.y[k] - py, vz = s.z[k] - pz;
           s.bx[k] = s.x[k];
@@ -666,71 +786,102 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
           s.bz[k] = s.z[k];
           double kd = kx * vx + ky * vy + kz * vz;
           double cx = ky * vz - kz * vy, cy = kz * vx - kx * vz, cz = kx * vy - ky * vx;
-          double f = kd * (1.0 - cth);
-          s.x[k] = px + vx * cth + cx * sth + kx * f;
-          s.y[k] = py + vy * cth + cy * sth + ky * f;
-          s.z[k] = pz + vz * cth + cz * sth + kz * f;
+          double f = kd * (1.0 - cur.cth);
+          s.x[k] = px + vx * cur.cth + cx * cur.sth + kx * f;
+          s.y[k] = py + vy * cur.cth + cy * cur.sth + ky * f;
+          s.z[k] = pz + vz * cur.cth + cz * cur.sth + kz * f;
         }
       }
       __syncthreads();
-      evaluate<F32>(set.f, m, s, evr2, err);
+      // ---- phase B: pair energy; the last warp prepares proposal p+1
+      if (warp != spec_warp) {
+        double el = 0.0, vw = 0.0, hb = 0.0, vr = 0.0, sl = 0.0;
+        pair_energy<F32>(set.f, m, s, threadIdx.x, nthr_pairs, el, vw, hb);
+        for (int v = threadIdx.x; v < m.nvar; v += nthr_pairs) vr += s.et[v];
+        if (sasa) sl = sasa_energy(set.f, m, s, 0, kWarps - 1, err);
+        warp_partials(s, el, vw, hb, vr, sl);
+      } else {
+        if (sc.refill) rng_refill_warp(s.mt, s.lq);
+        if (lane < 2 && p + 1 < m.nfree)
+          make_proposal(m, s, p + 1, head + cur.used + lane, rndord, sc.spec[lane]);
+        if (lane == 0)
+          for (int k = 0; k < 5; ++k) s.red[spec_warp * 8 + k] = 0.0;
+      }
       __syncthreads();
-      // ---- acceptance (metropolis.f:72-87)
-      if (threadIdx.x == 0) {
-        double enw = total_of(sc.sum);
-        double delta = __dsub_rn(weight(w, beta, enw), weight(w, beta, sc.eol));
-        int up = 0;
-        if (delta <= 0.0) {
+      // ---- phase C: every warp sums and decides (metropolis.f:72-87)
+      double sum[5];
+      all_sums(s, sum);
+      const double enw = total_of(sum);
+      double delta = __dsub_rn(weight(w, beta, enw), weight(w, beta, eol));
+      int up, drew;
+      if (delta <= 0.0) {
+        up = 1;
+        drew = 0;
+      } else {
+        drew = 1;
+        uint32_t k = (head + cur.used) & (kQueue - 1);
+        double rd = qbuf(s.mt)[k], lrd = s.lq[k];
+        double d = fmin(delta, 100.0);
+        double margin = -d - lrd;
+        if (margin > 1e-10)
           up = 1;
-        } else {
-          double rd = mt_grnd(s.mt);
-          delta = fmin(delta, 100.0);
-          if (exp(-delta) >= rd) up = 1;
-        }
-        if (up)
-          sc.eol = enw;
+        else if (margin < -1e-10)
+          up = 0;
         else
-          s.vlvr[sc.jv] = sc.vold;
-        if (!isfinite(enw)) set_err(err, kErrNonFinite);
-        sc.accept = up;
-        ++nprop;
-        nacc += up;
+          up = exp(-d) >= rd ? 1 : 0;
       }
-      __syncthreads();
-      if (!sc.accept) {
-        int jv = sc.jv;
-        int lo = __ldg(&m.var_lo[jv]), hi = __ldg(&m.var_hi[jv]);
+      if (up) {
+        eol = enw;
+      } else {
         for (int k = lo + threadIdx.x; k <= hi; k += blockDim.x) {
           s.x[k] = s.bx[k];
           s.y[k] = s.by[k];
           s.z[k] = s.bz[k];
         }
       }
+      head += cur.used + drew;
+      ++nprop;
+      nacc += up;
+      if (threadIdx.x == 0) {
+        if (!up) s.vlvr[cur.jv] = cur.vold;
+        if (!isfinite(enw)) set_err(err, kErrNonFinite);
+        if (p + 1 < m.nfree) {
+          Proposal nx = sc.spec[drew];
+          if (nx.jv == cur.jv) make_proposal(m, s, p + 1, head, rndord, nx);   // same variable again
+          sc.cur = nx;
+          s.vlvr[nx.jv] = nx.vnew;
+        }
+        sc.refill = (s.mt[kQTail] - head) < 24 ? 1 : 0;
+      }
       __syncthreads();
     }
     // ---- closing energy() and consistency check (metropolis.f:172-179)
-    double evr3 = setvar_all(m, s);
+    if (warp == spec_warp && s.mt[kQTail] - head < 24) rng_refill_warp(s.mt, s.lq);
+    setvar_all(m, s);
     __syncthreads();
     full_rebuild(m, s);
-    evaluate<F32>(set.f, m, s, evr3, err);
+    evaluate_block<F32>(set.f, m, s, err);
     __syncthreads();
-    if (threadIdx.x == 0) {
-      double enw = total_of(sc.sum);
-      sc.enew = enw;
-      if (!(flags & kFlagNoCheck) && fabs(sc.eol - enw) > check_tol && sc.eol < 100000.0)
-        set_err(err, kErrConsistency);
-      double* t = ch.terms + (size_t)c * 6;
-      for (int k = 0; k < 5; ++k) t[k] = sc.sum[k];
-      t[5] = ((sc.sum[0] + sc.sum[1]) + sc.sum[2]) + sc.sum[3];
+    {
+      double sum[5];
+      all_sums(s, sum);
+      enew = total_of(sum);
+      if (threadIdx.x == 0) {
+        if (!(flags & kFlagNoCheck) && fabs(eol - enew) > check_tol && eol < 100000.0)
+          set_err(err, kErrConsistency);
+        write_terms(ch, c, sum);
+      }
     }
     __syncthreads();
     fresh = true;
   }
   if (threadIdx.x == 0) {
-    ch.eol[c] = sc.eol;
+    ch.eol[c] = eol;
     ch.nacc[c] += nacc;
     ch.nprop[c] += nprop;
+    s.mt[kQHead] = head;
   }
+  __syncthreads();
   store_chain(ch, m, c, s);
 }
 
@@ -763,7 +914,7 @@ __global__ void k_exchange(DChains ch, int* temp_chain, const double* betas, int
       double delta = __dsub_rn(-__dmul_rn(bi, ejn), __dmul_rn(bj, ein));
       delta = __dadd_rn(delta, __dmul_rn(bi, ein));
       delta = __dadd_rn(delta, __dmul_rn(bj, ejn));
-      double ra = mt_grnd(mt);
+      double ra = stream_next(mt);
       stats[2 * (i - 1)] += 1;
       if (ra <= exp(delta)) {
         temp_chain[i - 1] = jn;

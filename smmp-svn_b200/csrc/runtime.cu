@@ -186,7 +186,7 @@ Ensemble::Ensemble(std::vector<std::shared_ptr<Molecule>> mols, std::vector<int>
   h2d(dms, mslot);
   ch_.toat_slot = dts;
   ch_.mt_slot = dms;
-  ch_.mt = dalloc<uint32_t>(allocs_, (size_t)nmt_ * 625);
+  ch_.mt = dalloc<uint32_t>(allocs_, (size_t)nmt_ * kMTWords);
   ch_.beta = dalloc<double>(allocs_, n_);
   ch_.eol = dalloc<double>(allocs_, n_);
   ch_.terms = dalloc<double>(allocs_, (size_t)n_ * 6);
@@ -294,7 +294,7 @@ void Ensemble::set_pt(const std::vector<double>& betas, int wrap, int exchange_s
   pt_.wrap = wrap;
   pt_.temp_chain = dalloc<int>(allocs_, n_);
   pt_.betas = dalloc<double>(allocs_, n_);
-  pt_.mt = dalloc<uint32_t>(allocs_, 625);
+  pt_.mt = dalloc<uint32_t>(allocs_, kMTWords);
   pt_.iswitch = dalloc<int>(allocs_, 1);
   pt_.stats = dalloc<unsigned long long>(allocs_, 2 * n_);
   std::vector<int> tc(n_);
@@ -373,12 +373,12 @@ void Ensemble::pt_get_state(std::vector<int>& tc, int& iswitch, std::vector<uint
   std::vector<int> sw;
   d2h(sw, pt_.iswitch, 1);
   iswitch = sw[0];
-  d2h(mt, pt_.mt, 625);
+  d2h(mt, pt_.mt, kMTWords);
   d2h(betas, pt_.betas, pt_.n);
 }
 void Ensemble::pt_set_state(const std::vector<int>& tc, int iswitch,
                             const std::vector<uint32_t>& mt, const std::vector<double>& betas) {
-  if ((int)tc.size() != pt_.n || mt.size() != 625 || (int)betas.size() != pt_.n)
+  if ((int)tc.size() != pt_.n || mt.size() != (size_t)kMTWords || (int)betas.size() != pt_.n)
     throw std::runtime_error("pt_set_state: size");
   h2d(pt_.temp_chain, tc);
   h2d(pt_.iswitch, std::vector<int>{iswitch});
@@ -399,14 +399,20 @@ void Ensemble::get_acceptance(std::vector<unsigned long long>& a,
   d2h(p, ch_.nprop, n_);
 }
 void Ensemble::get_errors(std::vector<int>& e) const { d2h(e, ch_.err, n_); }
+void Ensemble::set_acceptance(const std::vector<unsigned long long>& acc,
+                              const std::vector<unsigned long long>& prop) {
+  if ((int)acc.size() != n_ || (int)prop.size() != n_) throw std::runtime_error("set_acceptance: size");
+  h2d(ch_.nacc, acc);
+  h2d(ch_.nprop, prop);
+}
 void Ensemble::get_betas(std::vector<double>& b) const { d2h(b, ch_.beta, n_); }
 void Ensemble::set_betas(const std::vector<double>& b) {
   if ((int)b.size() != n_) throw std::runtime_error("set_betas: size");
   h2d(ch_.beta, b);
 }
-void Ensemble::get_mt(std::vector<uint32_t>& m) const { d2h(m, ch_.mt, (size_t)nmt_ * 625); }
+void Ensemble::get_mt(std::vector<uint32_t>& m) const { d2h(m, ch_.mt, (size_t)nmt_ * kMTWords); }
 void Ensemble::set_mt(const std::vector<uint32_t>& m) {
-  if (m.size() != (size_t)nmt_ * 625) throw std::runtime_error("set_mt: size");
+  if (m.size() != (size_t)nmt_ * kMTWords) throw std::runtime_error("set_mt: size");
   h2d(ch_.mt, m);
 }
 void Ensemble::get_toat(std::vector<double>& t) const { d2h(t, ch_.toat, (size_t)ntoat_ * ch_.tstride); }

@@ -54,7 +54,7 @@ struct PTState {
   int wrap = 1;         // replica n pairs with replica 1 (partem_s.f:222)
   int* temp_chain = nullptr;          // device [n]
   double* betas = nullptr;            // device [n], beta of each label
-  uint32_t* mt = nullptr;             // device [625] exchange stream
+  uint32_t* mt = nullptr;             // device stream slot (kMTWords) of the exchanges
   int* iswitch = nullptr;             // device
   unsigned long long* stats = nullptr;   // device [2n] attempts/accepts per pair
 };
@@ -105,10 +105,12 @@ class Ensemble {
   void get_acceptance(std::vector<unsigned long long>& acc,
                       std::vector<unsigned long long>& prop) const;
   void get_errors(std::vector<int>& e) const;
+  void set_acceptance(const std::vector<unsigned long long>& acc,
+                      const std::vector<unsigned long long>& prop);
   void get_coords(std::vector<double>& xyz);       // [chain*3*tstride]
   void get_betas(std::vector<double>& b) const;
   void set_betas(const std::vector<double>& b);
-  void get_mt(std::vector<uint32_t>& mt) const;   // [slot*625]
+  void get_mt(std::vector<uint32_t>& mt) const;   // [slot*kMTWords]
   void set_mt(const std::vector<uint32_t>& mt);
   void get_toat(std::vector<double>& t) const;
   void set_toat(const std::vector<double>& t);
