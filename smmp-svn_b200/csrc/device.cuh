@@ -20,7 +20,7 @@ constexpr int kMTIdx = 624, kQHead = 625, kQTail = 626, kQOff = 640;
 
 // One molecule, GPU resident (all indices 0-based, see topology.hpp).
 struct DMol {
-  int natoms, nvar, nfree, nchunks, n14, nheavy, nlevels, nres;
+  int natoms, nvar, nfree, nchunks, n14, nheavy, nlevels, nres, nsib;
   int i1, i2, i3;
   double gbpr[6];
   const int* iow;
@@ -71,6 +71,8 @@ struct DMolSet {
   const DMol* mols;          // device array
   int nmols;
   int max_atoms, max_vars;   // shared-memory sizing
+  int stage_bytes;           // shared-memory pool for the staged topology
+  int stage_lists;           // 1: the pair lists are staged too (they fit)
   const DForceField* ff;     // device
   FFScalars f;
 };

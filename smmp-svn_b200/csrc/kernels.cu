@@ -171,10 +171,14 @@ struct Smem {
   double* red;           // [kWarps][8] partial sums
   double *ta, *ta14, *tc, *tg;
   int* thb;
+  float4* p4;            // FP32 pair path: {x_hi, y_hi, z_hi, charge}
+  float4* l4;            //                 {x_lo, y_lo, z_lo, 0}, x = x_hi + x_lo
+  float4* tab4;          // {A, A14, C, +-guard r^2}; negative guard: H-bond pair
   double* spt;
   double* nb;
   Scalars* sc;
   DMol* mol;
+  char* pool;            // staged topology (see stage_mol)
 };
 
 __host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~size_t(15); }
@@ -211,10 +215,14 @@ __host__ __device__ inline size_t smem_layout(int n, int v, int npnt, bool sasa,
   t.tc = (double*)take(8 * kTP);
   t.tg = (double*)take(8 * kTP);
   t.thb = (int*)take(4 * kTP);
+  t.p4 = (float4*)take(16 * n);
+  t.l4 = (float4*)take(16 * n);
+  t.tab4 = (float4*)take(16 * kTP);
   t.spt = (double*)take(sasa ? 8 * 3 * npnt : 8);
   t.nb = (double*)take(sasa ? 8 * 4 * kWarps * kMaxNeighbours : 8);
   t.sc = (Scalars*)take(sizeof(Scalars));
   t.mol = (DMol*)take(sizeof(DMol));
+  t.pool = take(0);
   if (s) *s = t;
   return off;
 }
@@ -226,8 +234,73 @@ __device__ Smem carve(const DMolSet& set, bool sasa) {
   return s;
 }
 
+// Bytes of the staged topology of one molecule (host and device agree).
+__host__ __device__ inline size_t stage_size(int natoms, int nvar, int nsib, int nlevels, int nfree,
+                                             int nchunks, int n14, int nheavy, bool lists) {
+  size_t b = 0;
+  auto a = [&](size_t n) { b = align16(b + n); };
+  a(4 * natoms);            // iow
+  a(4 * natoms);            // level_atoms
+  a(4 * (nlevels + 1));     // level_off
+  a(8 * natoms * 3);        // blen, cba, sba
+  a(4 * nvar * 4);          // var_atom, var_base, var_lo, var_hi
+  a(4 * (nvar + 1));        // sib_off
+  a(4 * (nsib > 0 ? nsib : 1));
+  a(8 * nvar * 4);          // var_e0, var_sg, var_rn, axvr
+  a(4 * (nfree > 0 ? nfree : 1));
+  a(4 * (nheavy > 0 ? nheavy : 1));
+  a(8 * natoms * 2);        // rvdw, sigma
+  if (lists) {
+    a(4 * (nchunks > 0 ? nchunks : 1));
+    a(4 * (n14 > 0 ? n14 : 1));
+  }
+  return b;
+}
+
+// Copy the chain's molecule descriptor and its per-proposal topology into
+// shared memory; the staged descriptor points at the shared copies, so the
+// proposal loop never waits on a global-memory round trip.  The pair lists
+// are staged when they fit (set.stage_lists), else read from global memory.
+template <class T>
+__device__ const T* stage_array(const T* src, int n, char*& pool) {
+  T* dst = reinterpret_cast<T*>(pool);
+  for (int k = threadIdx.x; k < n; k += blockDim.x) dst[k] = src[k];
+  pool += align16(sizeof(T) * (size_t)(n > 0 ? n : 1));
+  return dst;
+}
 __device__ const DMol& stage_mol(const DMolSet& set, const DChains& ch, int c, Smem& s) {
   if (threadIdx.x == 0) *s.mol = set.mols[ch.mol_of_chain[c]];
+  __syncthreads();
+  DMol g = *s.mol;
+  __syncthreads();
+  char* pool = s.pool;
+  DMol m = g;
+  m.iow = stage_array(g.iow, g.natoms, pool);
+  m.level_atoms = stage_array(g.level_atoms, g.natoms, pool);
+  m.level_off = stage_array(g.level_off, g.nlevels + 1, pool);
+  m.blen = stage_array(g.blen, g.natoms, pool);
+  m.cba = stage_array(g.cba, g.natoms, pool);
+  m.sba = stage_array(g.sba, g.natoms, pool);
+  m.var_atom = stage_array(g.var_atom, g.nvar, pool);
+  m.var_base = stage_array(g.var_base, g.nvar, pool);
+  m.var_lo = stage_array(g.var_lo, g.nvar, pool);
+  m.var_hi = stage_array(g.var_hi, g.nvar, pool);
+  m.sib_off = stage_array(g.sib_off, g.nvar + 1, pool);
+  m.sib = stage_array(g.sib, g.nsib, pool);
+  m.var_e0 = stage_array(g.var_e0, g.nvar, pool);
+  m.var_sg = stage_array(g.var_sg, g.nvar, pool);
+  m.var_rn = stage_array(g.var_rn, g.nvar, pool);
+  m.axvr = stage_array(g.axvr, g.nvar, pool);
+  m.idvr = stage_array(g.idvr, g.nfree, pool);
+  m.heavy = stage_array(g.heavy, g.nheavy, pool);
+  m.rvdw = stage_array(g.rvdw, g.natoms, pool);
+  m.sigma = stage_array(g.sigma, g.natoms, pool);
+  if (set.stage_lists) {
+    m.chunks = stage_array(g.chunks, g.nchunks, pool);
+    m.pairs14 = stage_array(g.pairs14, g.n14, pool);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *s.mol = m;
   __syncthreads();
   return *s.mol;
 }
@@ -240,13 +313,24 @@ __device__ void load_static(const DForceField& ff, const DMol& m, Smem& s, bool 
     s.tc[k] = ff.c[k];
     s.tg[k] = ff.guard_r2[k];
     s.thb[k] = ff.hb[k];
+    float g = (float)ff.guard_r2[k];
+    s.tab4[k] = make_float4((float)ff.a[k], (float)ff.a14[k], (float)ff.c[k], ff.hb[k] ? -g : g);
   }
   for (int k = threadIdx.x; k < m.natoms; k += blockDim.x) {
-    s.cq[k] = __ldg(&m.charge[k]);
-    s.type[k] = __ldg(&m.type[k]);
+    s.cq[k] = m.charge[k];
+    s.type[k] = m.type[k];
   }
   if (sasa)
     for (int k = threadIdx.x; k < 3 * ff.npnt; k += blockDim.x) s.spt[k] = ff.spoint[k];
+}
+
+// FP32 copy of atom k's position as a hi+lo pair of floats, so that FP32
+// differences of two positions keep FP64-difference accuracy.
+__device__ __forceinline__ void f32_copy(Smem& s, int k) {
+  double x = s.x[k], y = s.y[k], z = s.z[k];
+  float xh = (float)x, yh = (float)y, zh = (float)z;
+  s.p4[k] = make_float4(xh, yh, zh, (float)s.cq[k]);
+  s.l4[k] = make_float4((float)(x - (double)xh), (float)(y - (double)yh), (float)(z - (double)zh), 0.f);
 }
 
 // ---------------------------------------------------------------- setvar
@@ -254,17 +338,17 @@ __device__ void load_static(const DForceField& ff, const DMol& m, Smem& s, bool 
 // the children of its own base, so threads never write the same atom).  The
 // torsion energy of a variable is refreshed when its dihedral moved.
 __device__ __forceinline__ double torsion_term(const DMol& m, int v, double to) {
-  double e0 = __ldg(&m.var_e0[v]);
-  return e0 != 0.0 ? e0 * (1.0 + __ldg(&m.var_sg[v]) * cos(to * __ldg(&m.var_rn[v]))) : 0.0;
+  double e0 = m.var_e0[v];
+  return e0 != 0.0 ? e0 * (1.0 + m.var_sg[v] * cos(to * m.var_rn[v])) : 0.0;
 }
 __device__ void setvar_all(const DMol& m, Smem& s) {
   for (int v = threadIdx.x; v < m.nvar; v += blockDim.x) {
-    int iat = __ldg(&m.var_atom[v]);
+    int iat = m.var_atom[v];
     double tsh = difang(s.toat[iat], s.vlvr[v]);
     if (tsh != 0.0) {
-      int b = __ldg(&m.sib_off[v]), e = __ldg(&m.sib_off[v + 1]);
+      int b = m.sib_off[v], e = m.sib_off[v + 1];
       for (int k = b; k < e; ++k) {
-        int jat = __ldg(&m.sib[k]);
+        int jat = m.sib[k];
         double to = __dadd_rn(s.toat[jat], tsh);
         if (fabs(to) > kPi) to = __dsub_rn(to, copysign(kPi2, to));
         s.toat[jat] = to;
@@ -275,7 +359,7 @@ __device__ void setvar_all(const DMol& m, Smem& s) {
 }
 __device__ void torsion_all(const DMol& m, Smem& s) {
   for (int v = threadIdx.x; v < m.nvar; v += blockDim.x)
-    s.et[v] = torsion_term(m, v, s.toat[__ldg(&m.var_atom[v])]);
+    s.et[v] = torsion_term(m, v, s.toat[m.var_atom[v]]);
 }
 
 // ---------------------------------------------------------------- rebuild
@@ -296,8 +380,8 @@ __device__ void first_frame(const DMol& m, Smem& s) {
   double z1 = ca * sg + sa * sb * cg, z2 = sa * sg - ca * sb * cg, z3 = cb * cg;
   d = sqrt(z1 * z1 + z2 * z2 + z3 * z3);
   ag[0][2] = z1 / d; ag[1][2] = z2 / d; ag[2][2] = z3 / d;
-  double ct2 = s.cs[i2], st2 = s.sn[i2], sa2 = __ldg(&m.sba[i2]);
-  x1 = -__ldg(&m.cba[i2]);
+  double ct2 = s.cs[i2], st2 = s.sn[i2], sa2 = m.sba[i2];
+  x1 = -m.cba[i2];
   x2 = -sa2 * ct2;
   x3 = -sa2 * st2;
   double dx = sqrt(x1 * x1 + x2 * x2 + x3 * x3);
@@ -329,7 +413,7 @@ __device__ void first_frame(const DMol& m, Smem& s) {
 // Eyring step (bldmol.f:175-242): atom i from the frame of its parent ia.
 __device__ __forceinline__ void eyring(const DMol& m, Smem& s, int i, int ia) {
   double ct = s.cs[i], st = s.sn[i];
-  double ca = __ldg(&m.cba[i]), sa = __ldg(&m.sba[i]), bl = __ldg(&m.blen[i]);
+  double ca = m.cba[i], sa = m.sba[i], bl = m.blen[i];
   double x1 = s.fx[3 * ia], x2 = s.fx[3 * ia + 1], x3 = s.fx[3 * ia + 2];
   double z1 = s.fz[3 * ia], z2 = s.fz[3 * ia + 1], z3 = s.fz[3 * ia + 2];
   double y1 = z2 * x3 - z3 * x2, y2 = z3 * x1 - z1 * x3, y3 = z1 * x2 - z2 * x1;
@@ -366,13 +450,15 @@ __device__ void full_rebuild(const DMol& m, Smem& s) {
   if (threadIdx.x == 0) first_frame(m, s);
   __syncthreads();
   for (int L = 1; L < m.nlevels; ++L) {
-    int b = __ldg(&m.level_off[L]), e = __ldg(&m.level_off[L + 1]);
+    int b = m.level_off[L], e = m.level_off[L + 1];
     for (int k = b + threadIdx.x; k < e; k += blockDim.x) {
-      int a = __ldg(&m.level_atoms[k]);
-      eyring(m, s, a, __ldg(&m.iow[a]));
+      int a = m.level_atoms[k];
+      eyring(m, s, a, m.iow[a]);
     }
     __syncthreads();
   }
+  for (int k = threadIdx.x; k < m.natoms; k += blockDim.x) f32_copy(s, k);
+  __syncthreads();
 }
 
 // ---------------------------------------------------------------- pair energy
@@ -415,22 +501,97 @@ __device__ __forceinline__ void pair_term(const FFScalars& ff, const Smem& s, in
   }
 }
 
+// Kahan-compensated FP32 accumulator.
+struct KSum {
+  float s = 0.f, c = 0.f;
+  __device__ __forceinline__ void add(float v) {
+    float y = v - c;
+    float t = s + y;
+    c = (t - s) - y;
+    s = t;
+  }
+  __device__ __forceinline__ double value() const { return (double)s - (double)c; }
+};
+
+// FP32 pair term from the hi+lo coordinates; pairs closer than the guard
+// distance of their types go through the FP64 path.  Coulomb accumulates
+// q_i q_j / r (the factor conv is applied to the sum).
+__device__ __forceinline__ void pair32(const FFScalars& ff, const Smem& s, int i, int j, bool is14,
+                                       KSum& el, KSum& vw, KSum& hb, double& el64, double& vw64,
+                                       double& hb64) {
+  const float4 pi = s.p4[i], pj = s.p4[j], li = s.l4[i], lj = s.l4[j];
+  float dx = (pj.x - pi.x) + (lj.x - li.x);
+  float dy = (pj.y - pi.y) + (lj.y - li.y);
+  float dz = (pj.z - pi.z) + (lj.z - li.z);
+  float r2 = dx * dx + dy * dy + dz * dz;
+  const float4 pr = s.tab4[s.type[i] * kTypes + s.type[j]];
+  if (r2 < fabsf(pr.w)) {
+    double e, v, h;
+    e = v = h = 0.0;
+    pair_term<false>(ff, s, i, j, is14, e, v, h);
+    el64 += e;
+    vw64 += v;
+    hb64 += h;
+    return;
+  }
+  float ri = rsqrtf(r2);
+  float r2i = ri * ri;
+  float r6i = r2i * r2i * r2i;
+  el.add(pi.w * pj.w * ri);
+  float A = is14 ? pr.y : pr.x;
+  if (pr.w >= 0.f)
+    vw.add(A * r6i * r6i - pr.z * r6i);
+  else
+    hb.add(A * r6i * r6i - pr.z * r6i * r2i * r2i);
+}
+
 // Pair sums of the threads [0, nthr): vdW chunks (8 partners each) and 1-4
 // pairs, both from the mklist lists.
 template <bool F32>
 __device__ void pair_energy(const FFScalars& ff, const DMol& m, const Smem& s, int tid, int nthr,
                             double& el, double& vw, double& hb) {
   const int nwork = m.nchunks * 8;
-  for (int t = tid; t < nwork; t += nthr) {
-    uint32_t w = __ldg(&m.chunks[t >> 3]);
+  if (!F32) {
+    for (int t = tid; t < nwork; t += nthr) {
+      uint32_t w = m.chunks[t >> 3];
+      int l = t & 7;
+      int len = int((w >> 28) & 7u) + 1;
+      if (l < len) pair_term<false>(ff, s, int(w & 0x3fffu), int((w >> 14) & 0x3fffu) + l, false, el, vw, hb);
+    }
+    for (int t = tid; t < m.n14; t += nthr) {
+      uint32_t w = m.pairs14[t];
+      pair_term<false>(ff, s, int(w & 0x3fffu), int(w >> 14), true, el, vw, hb);
+    }
+    return;
+  }
+  if (ff.epsd) {   // sigmoidal dielectric: FP64 terms
+    pair_energy<false>(ff, m, s, tid, nthr, el, vw, hb);
+    return;
+  }
+  KSum ke, kv, kh;
+  double e64 = 0.0, v64 = 0.0, h64 = 0.0;
+  int t = tid;
+  for (; t + nthr < nwork; t += 2 * nthr) {
+    uint32_t w0 = m.chunks[t >> 3], w1 = m.chunks[(t + nthr) >> 3];
+    int l0 = t & 7, l1 = (t + nthr) & 7;
+    if (l0 <= int((w0 >> 28) & 7u))
+      pair32(ff, s, int(w0 & 0x3fffu), int((w0 >> 14) & 0x3fffu) + l0, false, ke, kv, kh, e64, v64, h64);
+    if (l1 <= int((w1 >> 28) & 7u))
+      pair32(ff, s, int(w1 & 0x3fffu), int((w1 >> 14) & 0x3fffu) + l1, false, ke, kv, kh, e64, v64, h64);
+  }
+  for (; t < nwork; t += nthr) {
+    uint32_t w = m.chunks[t >> 3];
     int l = t & 7;
-    int len = int((w >> 28) & 7u) + 1;
-    if (l < len) pair_term<F32>(ff, s, int(w & 0x3fffu), int((w >> 14) & 0x3fffu) + l, false, el, vw, hb);
+    if (l <= int((w >> 28) & 7u))
+      pair32(ff, s, int(w & 0x3fffu), int((w >> 14) & 0x3fffu) + l, false, ke, kv, kh, e64, v64, h64);
   }
-  for (int t = tid; t < m.n14; t += nthr) {
-    uint32_t w = __ldg(&m.pairs14[t]);
-    pair_term<F32>(ff, s, int(w & 0x3fffu), int(w >> 14), true, el, vw, hb);
+  for (int u = tid; u < m.n14; u += nthr) {
+    uint32_t w = m.pairs14[u];
+    pair32(ff, s, int(w & 0x3fffu), int(w >> 14), true, ke, kv, kh, e64, v64, h64);
   }
+  el += ff.conv * ke.value() + e64;
+  vw += kv.value() + v64;
+  hb += kh.value() + h64;
 }
 
 // ---------------------------------------------------------------- SASA
@@ -447,8 +608,8 @@ __device__ double sasa_energy(const FFScalars& ff, const DMol& m, Smem& s, int w
   double eysl = 0.0;
   const int npnt = ff.npnt;
   for (int h = warp - w0; h < m.nheavy; h += nw) {
-    int i = __ldg(&m.heavy[h]);
-    double trad = __ldg(&m.rvdw[i]);
+    int i = m.heavy[h];
+    double trad = m.rvdw[i];
     double xi = s.x[i], yi = s.y[i], zi = s.z[i];
     int nn = 0;
     for (int base = 0; base < m.nheavy; base += 32) {
@@ -456,9 +617,9 @@ __device__ double sasa_energy(const FFScalars& ff, const DMol& m, Smem& s, int w
       bool take = false;
       double dx = 0, dy = 0, dz = 0, rb2 = 0;
       if (hj < m.nheavy) {
-        int j = __ldg(&m.heavy[hj]);
+        int j = m.heavy[hj];
         if (j != i) {
-          double rj = __ldg(&m.rvdw[j]);
+          double rj = m.rvdw[j];
           double ex = xi - s.x[j], ey = yi - s.y[j], ez = zi - s.z[j];
           double lim = trad + rj;
           // cheap pre-test with margin; the exact test below decides
@@ -509,7 +670,7 @@ __device__ double sasa_energy(const FFScalars& ff, const DMol& m, Smem& s, int w
     if (lane == 0) {
       double sdr = __ddiv_rn(__dmul_rn(__dmul_rn(4.0 * kPi, trad), trad), (double)npnt);
       double area = __dmul_rn(sdr, (double)cnt);
-      eysl += __dmul_rn(area, __ldg(&m.sigma[i]));
+      eysl += __dmul_rn(area, m.sigma[i]);
     }
     __syncwarp();
   }
@@ -522,8 +683,9 @@ __device__ __forceinline__ void warp_partials(Smem& s, double v0, double v1, dou
                                               double v4) {
   double v[5] = {v0, v1, v2, v3, v4};
 #pragma unroll
-  for (int k = 0; k < 5; ++k)
-    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int k = 0; k < 5; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
   if ((threadIdx.x & 31) == 0) {
     int w = threadIdx.x >> 5;
 #pragma unroll
@@ -533,12 +695,17 @@ __device__ __forceinline__ void warp_partials(Smem& s, double v0, double v1, dou
 // Every warp sums the warp partials the same way (call after a barrier).
 __device__ __forceinline__ void all_sums(const Smem& s, double* out) {
   const int lane = threadIdx.x & 31;
+  double v[5];
 #pragma unroll
-  for (int k = 0; k < 5; ++k) {
-    double v = lane < kWarps ? s.red[lane * 8 + k] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    out[k] = v;
-  }
+  for (int k = 0; k < 5; ++k) v[k] = lane < kWarps ? s.red[lane * 8 + k] : 0.0;
+  // full butterfly: every lane of every warp ends with the same bits, since
+  // each round adds two partial sums in either order (a + b == b + a)
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int k = 0; k < 5; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+#pragma unroll
+  for (int k = 0; k < 5; ++k) out[k] = v[k];
 }
 __device__ __forceinline__ double total_of(const double* sum) {
   // energy.f: eysm = eyel + eyvw + eyhb + eyvr, then + eysl
@@ -584,9 +751,9 @@ __device__ void make_proposal(const DMol& m, const Smem& s, int p, uint32_t pos,
     if (ivar >= m.nfree) ivar = m.nfree - 1;
     ++k;
   }
-  int jv = __ldg(&m.idvr[ivar]);
+  int jv = m.idvr[ivar];
   double vold = s.vlvr[jv];
-  double dv = __dmul_rn(__ldg(&m.axvr[jv]), __dsub_rn(q[k & (kQueue - 1)], 0.5));
+  double dv = __dmul_rn(m.axvr[jv], __dsub_rn(q[k & (kQueue - 1)], 0.5));
   ++k;
   double vnew = addang(vold, dv);
   double sv, cv;
@@ -768,11 +935,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
 
     for (int p = 0; p < m.nfree; ++p) {
       const Proposal cur = sc.cur;
-      const int lo = __ldg(&m.var_lo[cur.jv]), hi = __ldg(&m.var_hi[cur.jv]);
+      const int lo = m.var_lo[cur.jv], hi = m.var_hi[cur.jv];
       // ---- phase A: exact dihedral state + torsion terms; rotate the subtree
       setvar_all(m, s);
       {
-        int b = __ldg(&m.var_base[cur.jv]), a = __ldg(&m.iow[b]);
+        int b = m.var_base[cur.jv], a = m.iow[b];
         double px = s.x[b], py = s.y[b], pz = s.z[b];
         double kx = px - s.x[a], ky = py - s.y[a], kz = pz - s.z[a];
         double inv = rsqrt(kx * kx + ky * ky + kz * kz);
@@ -790,6 +957,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
           s.x[k] = px + vx * cur.cth + cx * cur.sth + kx * f;
           s.y[k] = py + vy * cur.cth + cy * cur.sth + ky * f;
           s.z[k] = pz + vz * cur.cth + cz * cur.sth + kz * f;
+          if (F32) f32_copy(s, k);
         }
       }
       __syncthreads();
@@ -837,6 +1005,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
           s.x[k] = s.bx[k];
           s.y[k] = s.by[k];
           s.z[k] = s.bz[k];
+          if (F32) f32_copy(s, k);
         }
       }
       head += cur.used + drew;
@@ -856,7 +1025,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       __syncthreads();
     }
     // ---- closing energy() and consistency check (metropolis.f:172-179)
-    if (warp == spec_warp && s.mt[kQTail] - head < 24) rng_refill_warp(s.mt, s.lq);
+    if (warp == spec_warp) {
+      const bool low = __shfl_sync(0xffffffffu, (s.mt[kQTail] - head) < 24u ? 1 : 0, 0) != 0;
+      if (low) rng_refill_warp(s.mt, s.lq);
+    }
     setvar_all(m, s);
     __syncthreads();
     full_rebuild(m, s);
@@ -929,7 +1101,12 @@ __global__ void k_exchange(DChains ch, int* temp_chain, const double* betas, int
 // ============================================================================ host wrappers
 
 size_t sweep_smem_bytes(const DMolSet& set) {
-  return smem_layout(set.max_atoms, set.max_vars, set.f.npnt, set.f.itysol > 0, nullptr, nullptr);
+  return smem_layout(set.max_atoms, set.max_vars, set.f.npnt, set.f.itysol > 0, nullptr, nullptr) +
+         (size_t)set.stage_bytes;
+}
+
+size_t stage_bytes_of(const DMol& d, bool lists) {
+  return stage_size(d.natoms, d.nvar, d.nsib, d.nlevels, d.nfree, d.nchunks, d.n14, d.nheavy, lists);
 }
 
 cudaError_t launch_seed(uint32_t* mt, const int* seeds, int nslots, cudaStream_t st) {

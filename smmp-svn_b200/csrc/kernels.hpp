@@ -9,6 +9,8 @@
 namespace smmpb200 {
 
 size_t sweep_smem_bytes(const DMolSet& set);
+// Shared-memory pool a molecule needs when its topology is staged.
+size_t stage_bytes_of(const DMol& d, bool lists);
 
 cudaError_t launch_seed(uint32_t* mt, const int* seeds, int nslots, cudaStream_t st);
 cudaError_t launch_draw(uint32_t* mt, int slot, int n, double* out, cudaStream_t st);

@@ -99,6 +99,7 @@ DeviceSet::DeviceSet(const std::vector<std::shared_ptr<Molecule>>& mols) {
     d.nheavy = (int)t.heavy.size();
     d.nlevels = (int)t.level_off.size() - 1;
     d.nres = t.nres;
+    d.nsib = (int)t.sib.size();
     d.i1 = t.i1;
     d.i2 = t.i2;
     d.i3 = t.i3;
@@ -141,6 +142,19 @@ DeviceSet::DeviceSet(const std::vector<std::shared_ptr<Molecule>>& mols) {
   set_.max_vars = max_vars;
   set_.ff = dff;
   set_.f = FFScalars{ff.conv, ff.plt, ff.slp, ff.epsd, ff.itysol, ff.npnt};
+  // stage the pair lists too when the largest molecule's copy fits
+  const size_t budget = 200 * 1024;
+  size_t with_lists = 0, without = 0;
+  for (const DMol& d : dm) {
+    with_lists = std::max(with_lists, stage_bytes_of(d, true));
+    without = std::max(without, stage_bytes_of(d, false));
+  }
+  set_.stage_lists = 1;
+  set_.stage_bytes = (int)with_lists;
+  if (sweep_smem_bytes(set_) > budget) {
+    set_.stage_lists = 0;
+    set_.stage_bytes = (int)without;
+  }
   size_t sm = sweep_smem_bytes(set_);
   if (sm > 227 * 1024)
     throw std::runtime_error("DeviceSet: molecule too large for one CTA's shared memory");

@@ -7,7 +7,8 @@ import ctypes
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libsmmp_b200.so")
+# SMMP_B200_LIB selects another build of the library (e.g. a debug build).
+LIB_PATH = os.environ.get("SMMP_B200_LIB") or os.path.join(_HERE, "libsmmp_b200.so")
 
 c_int = ctypes.c_int
 c_double = ctypes.c_double
