@@ -140,6 +140,22 @@ def cpu_baseline(target_seconds=15.0):
                       % (NREP, nsw, t)}
 
 
+def max_over_ranks(values, world, device=None):
+    """Element-wise max of per-rank timings (the job takes as long as its
+    slowest rank)."""
+    import torch
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def job_rate(units_per_rank, world, ms):
+    """Whole-job throughput: units all ranks processed / slowest rank's time."""
+    return units_per_rank * world / (ms / 1000.0)
+
+
 # ------------------------------------------------------------------ our arm
 def run_ours(args, rank, world):
     import numpy as np
@@ -217,13 +233,9 @@ def run_ours(args, rank, world):
         raise SystemExit("kernel error words: %s" % errors.tolist())
 
     # max over ranks
-    vals = torch.tensor([ms, e2e_ms, sweep_kernel_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(vals, op=torch.distributed.ReduceOp.MAX)
-    ms, e2e_ms, sweep_kernel_ms = vals.tolist()
-    sweeps_total = NREP * SWEEPS_PER_STEP * args.steps * world
-    value = sweeps_total / (ms / 1000.0)
-    e2e_value = NREP * SWEEPS_PER_STEP * e2e_steps * world / (e2e_ms / 1000.0)
+    ms, e2e_ms, sweep_kernel_ms = max_over_ranks([ms, e2e_ms, sweep_kernel_ms], world, "cuda")
+    value = job_rate(NREP * SWEEPS_PER_STEP * args.steps, world, ms)
+    e2e_value = job_rate(NREP * SWEEPS_PER_STEP * e2e_steps, world, e2e_ms)
 
     # roofline: algorithmic HBM bytes per launch of the sweep kernel
     # (16 B coordinates per atom + 8 B per dihedral + 8 B energy, per
@@ -285,8 +297,8 @@ def run_reference(args, rank, world):
     seeds = (ctypes.c_int * NREP)(*[31433 + 1000 * k for k in range(NREP)])
     betas = (ctypes.c_double * NREP)(*[1.0 / (t * GAS) for t in temperatures()])
     out = (ctypes.c_double * NREP)()
-    # each step: every replica 2 sweeps (a bounded sample of the workload)
-    per = 2
+    # each step: every replica 20 sweeps (a bounded sample of the workload)
+    per = 20
     for _ in range(args.warmup):
         L.orc_bench_chains(h, NREP, seeds, betas, 1, cores, out)
     total = 0.0
