@@ -149,7 +149,9 @@ __device__ void rng_refill_warp(uint32_t* slot, double* lq) {
 // ---------------------------------------------------------------- shared memory
 struct Proposal {
   int jv, ivar, used;   // variable, its index in idvr, RNG values its setup consumed
+  int b, a;             // base atom of the rotation and its parent (axis a -> b)
   double vold, vnew, cth, sth;
+  double enew, eold;    // torsion energy of jv at its new / current dihedral
 };
 
 struct Scalars {
@@ -234,25 +236,36 @@ __device__ Smem carve(const DMolSet& set, bool sasa) {
   return s;
 }
 
-// Bytes of the staged topology of one molecule (host and device agree).
+// Bytes of the staged topology of one molecule: one 16-byte-aligned block per
+// array, in the order stage_mol copies them (host sizing and device staging
+// must agree exactly).
 __host__ __device__ inline size_t stage_size(int natoms, int nvar, int nsib, int nlevels, int nfree,
                                              int nchunks, int n14, int nheavy, bool lists) {
   size_t b = 0;
-  auto a = [&](size_t n) { b = align16(b + n); };
-  a(4 * natoms);            // iow
-  a(4 * natoms);            // level_atoms
-  a(4 * (nlevels + 1));     // level_off
-  a(8 * natoms * 3);        // blen, cba, sba
-  a(4 * nvar * 4);          // var_atom, var_base, var_lo, var_hi
-  a(4 * (nvar + 1));        // sib_off
-  a(4 * (nsib > 0 ? nsib : 1));
-  a(8 * nvar * 4);          // var_e0, var_sg, var_rn, axvr
-  a(4 * (nfree > 0 ? nfree : 1));
-  a(4 * (nheavy > 0 ? nheavy : 1));
-  a(8 * natoms * 2);        // rvdw, sigma
+  auto a = [&](size_t elem, int n) { b += align16(elem * (size_t)(n > 0 ? n : 1)); };
+  a(4, natoms);        // iow
+  a(4, natoms);        // level_atoms
+  a(4, nlevels + 1);   // level_off
+  a(8, natoms);        // blen
+  a(8, natoms);        // cba
+  a(8, natoms);        // sba
+  a(4, nvar);          // var_atom
+  a(4, nvar);          // var_base
+  a(4, nvar);          // var_lo
+  a(4, nvar);          // var_hi
+  a(4, nvar + 1);      // sib_off
+  a(4, nsib);          // sib
+  a(8, nvar);          // var_e0
+  a(8, nvar);          // var_sg
+  a(8, nvar);          // var_rn
+  a(8, nvar);          // axvr
+  a(4, nfree);         // idvr
+  a(4, nheavy);        // heavy
+  a(8, natoms);        // rvdw
+  a(8, natoms);        // sigma
   if (lists) {
-    a(4 * (nchunks > 0 ? nchunks : 1));
-    a(4 * (n14 > 0 ? n14 : 1));
+    a(4, nchunks);     // chunks
+    a(4, n14);         // pairs14
   }
   return b;
 }
@@ -261,11 +274,24 @@ __host__ __device__ inline size_t stage_size(int natoms, int nvar, int nsib, int
 // shared memory; the staged descriptor points at the shared copies, so the
 // proposal loop never waits on a global-memory round trip.  The pair lists
 // are staged when they fit (set.stage_lists), else read from global memory.
+__device__ __forceinline__ unsigned dynamic_smem_bytes() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(r));
+  return r;
+}
+// Copy n elements into the pool; copies nothing (and leaves the source in
+// place) if the block would pass `end`, so a sizing error can never write
+// outside the CTA's shared memory.
 template <class T>
-__device__ const T* stage_array(const T* src, int n, char*& pool) {
+__device__ const T* stage_array(const T* src, int n, char*& pool, const char* end, bool& ok) {
+  size_t bytes = align16(sizeof(T) * (size_t)(n > 0 ? n : 1));
+  if (!ok || pool + bytes > end) {
+    ok = false;
+    return src;
+  }
   T* dst = reinterpret_cast<T*>(pool);
   for (int k = threadIdx.x; k < n; k += blockDim.x) dst[k] = src[k];
-  pool += align16(sizeof(T) * (size_t)(n > 0 ? n : 1));
+  pool += bytes;
   return dst;
 }
 __device__ const DMol& stage_mol(const DMolSet& set, const DChains& ch, int c, Smem& s) {
@@ -273,31 +299,34 @@ __device__ const DMol& stage_mol(const DMolSet& set, const DChains& ch, int c, S
   __syncthreads();
   DMol g = *s.mol;
   __syncthreads();
+  extern __shared__ __align__(16) char smem_raw[];
   char* pool = s.pool;
+  const char* end = smem_raw + dynamic_smem_bytes();
+  bool ok = true;
   DMol m = g;
-  m.iow = stage_array(g.iow, g.natoms, pool);
-  m.level_atoms = stage_array(g.level_atoms, g.natoms, pool);
-  m.level_off = stage_array(g.level_off, g.nlevels + 1, pool);
-  m.blen = stage_array(g.blen, g.natoms, pool);
-  m.cba = stage_array(g.cba, g.natoms, pool);
-  m.sba = stage_array(g.sba, g.natoms, pool);
-  m.var_atom = stage_array(g.var_atom, g.nvar, pool);
-  m.var_base = stage_array(g.var_base, g.nvar, pool);
-  m.var_lo = stage_array(g.var_lo, g.nvar, pool);
-  m.var_hi = stage_array(g.var_hi, g.nvar, pool);
-  m.sib_off = stage_array(g.sib_off, g.nvar + 1, pool);
-  m.sib = stage_array(g.sib, g.nsib, pool);
-  m.var_e0 = stage_array(g.var_e0, g.nvar, pool);
-  m.var_sg = stage_array(g.var_sg, g.nvar, pool);
-  m.var_rn = stage_array(g.var_rn, g.nvar, pool);
-  m.axvr = stage_array(g.axvr, g.nvar, pool);
-  m.idvr = stage_array(g.idvr, g.nfree, pool);
-  m.heavy = stage_array(g.heavy, g.nheavy, pool);
-  m.rvdw = stage_array(g.rvdw, g.natoms, pool);
-  m.sigma = stage_array(g.sigma, g.natoms, pool);
+  m.iow = stage_array(g.iow, g.natoms, pool, end, ok);
+  m.level_atoms = stage_array(g.level_atoms, g.natoms, pool, end, ok);
+  m.level_off = stage_array(g.level_off, g.nlevels + 1, pool, end, ok);
+  m.blen = stage_array(g.blen, g.natoms, pool, end, ok);
+  m.cba = stage_array(g.cba, g.natoms, pool, end, ok);
+  m.sba = stage_array(g.sba, g.natoms, pool, end, ok);
+  m.var_atom = stage_array(g.var_atom, g.nvar, pool, end, ok);
+  m.var_base = stage_array(g.var_base, g.nvar, pool, end, ok);
+  m.var_lo = stage_array(g.var_lo, g.nvar, pool, end, ok);
+  m.var_hi = stage_array(g.var_hi, g.nvar, pool, end, ok);
+  m.sib_off = stage_array(g.sib_off, g.nvar + 1, pool, end, ok);
+  m.sib = stage_array(g.sib, g.nsib, pool, end, ok);
+  m.var_e0 = stage_array(g.var_e0, g.nvar, pool, end, ok);
+  m.var_sg = stage_array(g.var_sg, g.nvar, pool, end, ok);
+  m.var_rn = stage_array(g.var_rn, g.nvar, pool, end, ok);
+  m.axvr = stage_array(g.axvr, g.nvar, pool, end, ok);
+  m.idvr = stage_array(g.idvr, g.nfree, pool, end, ok);
+  m.heavy = stage_array(g.heavy, g.nheavy, pool, end, ok);
+  m.rvdw = stage_array(g.rvdw, g.natoms, pool, end, ok);
+  m.sigma = stage_array(g.sigma, g.natoms, pool, end, ok);
   if (set.stage_lists) {
-    m.chunks = stage_array(g.chunks, g.nchunks, pool);
-    m.pairs14 = stage_array(g.pairs14, g.n14, pool);
+    m.chunks = stage_array(g.chunks, g.nchunks, pool, end, ok);
+    m.pairs14 = stage_array(g.pairs14, g.n14, pool, end, ok);
   }
   __syncthreads();
   if (threadIdx.x == 0) *s.mol = m;
@@ -334,29 +363,32 @@ __device__ __forceinline__ void f32_copy(Smem& s, int k) {
 }
 
 // ---------------------------------------------------------------- setvar
-// setvar.f:30-56 for every variable (one thread each; a variable shifts only
-// the children of its own base, so threads never write the same atom).  The
-// torsion energy of a variable is refreshed when its dihedral moved.
+// setvar.f:30-56 for every variable (one lane per variable; a variable shifts
+// only the children of its own base, so lanes never write the same atom).
 __device__ __forceinline__ double torsion_term(const DMol& m, int v, double to) {
   double e0 = m.var_e0[v];
   return e0 != 0.0 ? e0 * (1.0 + m.var_sg[v] * cos(to * m.var_rn[v])) : 0.0;
 }
-__device__ void setvar_all(const DMol& m, Smem& s) {
-  for (int v = threadIdx.x; v < m.nvar; v += blockDim.x) {
-    int iat = m.var_atom[v];
-    double tsh = difang(s.toat[iat], s.vlvr[v]);
-    if (tsh != 0.0) {
-      int b = m.sib_off[v], e = m.sib_off[v + 1];
-      for (int k = b; k < e; ++k) {
-        int jat = m.sib[k];
-        double to = __dadd_rn(s.toat[jat], tsh);
-        if (fabs(to) > kPi) to = __dsub_rn(to, copysign(kPi2, to));
-        s.toat[jat] = to;
-      }
-      s.et[v] = torsion_term(m, v, s.toat[iat]);
+__device__ __forceinline__ void setvar_one(const DMol& m, Smem& s, int v) {
+  int iat = m.var_atom[v];
+  double tsh = difang(s.toat[iat], s.vlvr[v]);
+  if (tsh != 0.0) {
+    int b = m.sib_off[v], e = m.sib_off[v + 1];
+    for (int k = b; k < e; ++k) {
+      int jat = m.sib[k];
+      double to = __dadd_rn(s.toat[jat], tsh);
+      if (fabs(to) > kPi) to = __dsub_rn(to, copysign(kPi2, to));
+      s.toat[jat] = to;
     }
   }
 }
+__device__ void setvar_all(const DMol& m, Smem& s) {
+  for (int v = threadIdx.x; v < m.nvar; v += blockDim.x) setvar_one(m, s, v);
+}
+__device__ void setvar_warp(const DMol& m, Smem& s) {
+  for (int v = threadIdx.x & 31; v < m.nvar; v += 32) setvar_one(m, s, v);
+}
+// Torsion energy of every variable (enyshe.f:70-80) from the dihedral state.
 __device__ void torsion_all(const DMol& m, Smem& s) {
   for (int v = threadIdx.x; v < m.nvar; v += blockDim.x)
     s.et[v] = torsion_term(m, v, s.toat[m.var_atom[v]]);
@@ -758,13 +790,22 @@ __device__ void make_proposal(const DMol& m, const Smem& s, int p, uint32_t pos,
   double vnew = addang(vold, dv);
   double sv, cv;
   sincos(difang(vold, vnew), &sv, &cv);
+  // dihedral of the primary atom after this proposal's setvar (setvar.f:40-53)
+  int iat = m.var_atom[jv];
+  double t0 = s.toat[iat];
+  double to = __dadd_rn(t0, difang(t0, vnew));
+  if (fabs(to) > kPi) to = __dsub_rn(to, copysign(kPi2, to));
   out.jv = jv;
   out.ivar = ivar;
   out.used = (int)(k - pos);
+  out.b = m.var_base[jv];
+  out.a = m.iow[out.b];
   out.vold = vold;
   out.vnew = vnew;
   out.cth = cv;
   out.sth = sv;
+  out.enew = torsion_term(m, jv, to);
+  out.eold = s.et[jv];
 }
 
 // Load the chain's state into shared memory.
@@ -880,7 +921,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
   const bool sasa = set.f.itysol > 0;
   const bool rndord = (flags & kFlagRndOrd) != 0;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int spec_warp = kWarps - 1;            // prepares the next proposal
+  const int spec_warp = kWarps - 1;            // setvar replay + next proposal
   const int nthr_pairs = (kWarps - 1) * 32;    // the other warps evaluate pairs
   Smem s = carve(set, sasa);
   Scalars& sc = *s.sc;
@@ -902,10 +943,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
     __syncwarp();
     while (s.mt[kQTail] - s.mt[kQHead] < 24) rng_refill_warp(s.mt, s.lq);
   }
-  torsion_all(m, s);
   __syncthreads();
   uint32_t head = s.mt[kQHead];   // identical in every thread from here on
-  double eol = ch.eol[c], enew = 0.0;
+  double eol = ch.eol[c], enew = 0.0, etor = 0.0;
   bool fresh = false;
 
   for (int sw = 0; sw < nsweeps; ++sw) {
@@ -918,12 +958,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
     setvar_all(m, s);
     __syncthreads();
     if (!fresh) {
+      torsion_all(m, s);
       full_rebuild(m, s);
       evaluate_block<F32>(set.f, m, s, err);
       __syncthreads();
       double sum[5];
       all_sums(s, sum);
       enew = total_of(sum);
+      etor = sum[3];
     }
     eol = enew;
     if (m.nfree > 0 && threadIdx.x == 0) {
@@ -936,12 +978,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
     for (int p = 0; p < m.nfree; ++p) {
       const Proposal cur = sc.cur;
       const int lo = m.var_lo[cur.jv], hi = m.var_hi[cur.jv];
-      // ---- phase A: exact dihedral state + torsion terms; rotate the subtree
-      setvar_all(m, s);
+      // ---- phase A: rotate the subtree of cur.jv about its bond (+theta)
       {
-        int b = m.var_base[cur.jv], a = m.iow[b];
-        double px = s.x[b], py = s.y[b], pz = s.z[b];
-        double kx = px - s.x[a], ky = py - s.y[a], kz = pz - s.z[a];
+        double px = s.x[cur.b], py = s.y[cur.b], pz = s.z[cur.b];
+        double kx = px - s.x[cur.a], ky = py - s.y[cur.a], kz = pz - s.z[cur.a];
         double inv = rsqrt(kx * kx + ky * ky + kz * kz);
         kx *= inv;
         ky *= inv;
@@ -961,25 +1001,30 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
         }
       }
       __syncthreads();
-      // ---- phase B: pair energy; the last warp prepares proposal p+1
+      // ---- phase B: pair energy; the last warp replays this proposal's
+      // setvar call on the dihedral state and prepares proposal p+1
       if (warp != spec_warp) {
-        double el = 0.0, vw = 0.0, hb = 0.0, vr = 0.0, sl = 0.0;
+        double el = 0.0, vw = 0.0, hb = 0.0, sl = 0.0;
         pair_energy<F32>(set.f, m, s, threadIdx.x, nthr_pairs, el, vw, hb);
-        for (int v = threadIdx.x; v < m.nvar; v += nthr_pairs) vr += s.et[v];
         if (sasa) sl = sasa_energy(set.f, m, s, 0, kWarps - 1, err);
-        warp_partials(s, el, vw, hb, vr, sl);
+        double v = ((el + vw) + hb) + sl;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) s.red[warp * 8] = v;
       } else {
+        setvar_warp(m, s);
+        __syncwarp();
         if (sc.refill) rng_refill_warp(s.mt, s.lq);
         if (lane < 2 && p + 1 < m.nfree)
           make_proposal(m, s, p + 1, head + cur.used + lane, rndord, sc.spec[lane]);
-        if (lane == 0)
-          for (int k = 0; k < 5; ++k) s.red[spec_warp * 8 + k] = 0.0;
       }
       __syncthreads();
       // ---- phase C: every warp sums and decides (metropolis.f:72-87)
-      double sum[5];
-      all_sums(s, sum);
-      const double enw = total_of(sum);
+      double epair = 0.0;
+      for (int k = 0; k < kWarps - 1; ++k) epair += s.red[k * 8];
+      // every value read here was written before the last barrier
+      const double etor_new = (etor - cur.eold) + cur.enew;
+      const double enw = epair + etor_new;
       double delta = __dsub_rn(weight(w, beta, enw), weight(w, beta, eol));
       int up, drew;
       if (delta <= 0.0) {
@@ -1000,6 +1045,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       }
       if (up) {
         eol = enw;
+        etor = etor_new;
       } else {
         for (int k = lo + threadIdx.x; k <= hi; k += blockDim.x) {
           s.x[k] = s.bx[k];
@@ -1012,7 +1058,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       ++nprop;
       nacc += up;
       if (threadIdx.x == 0) {
-        if (!up) s.vlvr[cur.jv] = cur.vold;
+        if (up)
+          s.et[cur.jv] = cur.enew;
+        else
+          s.vlvr[cur.jv] = cur.vold;
         if (!isfinite(enw)) set_err(err, kErrNonFinite);
         if (p + 1 < m.nfree) {
           Proposal nx = sc.spec[drew];
@@ -1031,6 +1080,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
     }
     setvar_all(m, s);
     __syncthreads();
+    torsion_all(m, s);
     full_rebuild(m, s);
     evaluate_block<F32>(set.f, m, s, err);
     __syncthreads();
@@ -1038,6 +1088,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       double sum[5];
       all_sums(s, sum);
       enew = total_of(sum);
+      etor = sum[3];
       if (threadIdx.x == 0) {
         if (!(flags & kFlagNoCheck) && fabs(eol - enew) > check_tol && eol < 100000.0)
           set_err(err, kErrConsistency);

@@ -21,7 +21,10 @@ double guard_r2(double a, double c, int hb, double g) {
 
 ForceField make_forcefield(const Assembly& a) {
   ForceField ff;
-  const double g = 1.0;   // kcal/mol: pairs that can exceed it stay in FP64
+  // Pairs whose van der Waals / H-bond terms can exceed g kcal/mol (clashes)
+  // are evaluated in FP64; below it the FP32 rounding of a term (~1e-7
+  // relative) stays under 1e-5 kcal/mol.
+  const double g = 100.0;
   for (int i = 0; i < kNumTypes; ++i)
     for (int j = 0; j < kNumTypes; ++j) {
       int k = i * kNumTypes + j;

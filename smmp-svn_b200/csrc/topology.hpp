@@ -27,7 +27,8 @@ constexpr int kMaxAtoms = 16383;  // 14-bit atom index in the packed pair words
 // Per type-pair constants, [ti*18+tj].  A/C of the 12-6 (or 12-10 hydrogen
 // bond) term, the halved repulsion of 1-4 pairs, and the squared distance
 // beyond which every van der Waals / H-bond term is below the FP32 guard
-// energy (pairs closer than that are evaluated in FP64 in the mixed mode).
+// energy of 100 kcal/mol (closer pairs are evaluated in FP64 in the mixed
+// mode).
 struct PairTable {
   double a[kNumTypes * kNumTypes];
   double a14[kNumTypes * kNumTypes];
