@@ -49,6 +49,12 @@ struct DMol {
   const uint32_t* pairs14;
   const int* heavy;
   const int* residue_of_atom;
+  // dense pair set (topology.hpp)
+  const unsigned long long* near_mask;
+  const unsigned long long* near14;
+  const uint32_t* tiles;
+  const int* tile_off;
+  int ntiles;
 };
 
 // Force field constants read by every chain (copied to shared memory).

@@ -130,6 +130,15 @@ DeviceSet::DeviceSet(const std::vector<std::shared_ptr<Molecule>>& mols) {
     d.pairs14 = upload(t.pairs14.empty() ? std::vector<uint32_t>{0} : t.pairs14);
     d.heavy = upload(t.heavy.empty() ? std::vector<int>{0} : t.heavy);
     d.residue_of_atom = upload(t.residue_of_atom);
+    {
+      std::vector<unsigned long long> nm(t.near_mask.begin(), t.near_mask.end()),
+          n14(t.near14.begin(), t.near14.end());
+      d.near_mask = upload(nm);
+      d.near14 = upload(n14);
+    }
+    d.tiles = upload(t.tiles);
+    d.tile_off = upload(t.tile_off);
+    d.ntiles = (int)t.tiles.size();
     dm.push_back(d);
     max_atoms = std::max(max_atoms, t.natoms);
     max_vars = std::max(max_vars, t.nvar);

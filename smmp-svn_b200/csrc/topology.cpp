@@ -175,6 +175,43 @@ MolTopo flatten(Assembly& a, int nml) {
       t.npairs += 1;
     }
   }
+  // dense form of the same pair set
+  t.near_mask.assign(n, 0);
+  t.near14.assign(n, 0);
+  long long far = 0;
+  for (uint32_t w : t.chunks) {
+    int i = int(w & 0x3fffu), j0 = int((w >> 14) & 0x3fffu), len = int((w >> 28) & 7u) + 1;
+    for (int j = j0; j < j0 + len; ++j) {
+      int lo = std::min(i, j), d = std::abs(i - j);
+      if (d == 0) fail("flatten: self pair in the lists");
+      if (d <= kNearWindow) {
+        uint64_t bit = 1ull << (d - 1);
+        if (t.near_mask[lo] & bit) fail("flatten: pair listed twice");
+        t.near_mask[lo] |= bit;
+      } else {
+        ++far;
+      }
+    }
+  }
+  for (uint32_t w : t.pairs14) {
+    int i = int(w & 0x3fffu), j = int(w >> 14);
+    int lo = std::min(i, j), d = std::abs(i - j);
+    if (d == 0 || d > kNearWindow) fail("flatten: 1-4 pair outside the near window");
+    uint64_t bit = 1ull << (d - 1);
+    if ((t.near14[lo] | t.near_mask[lo]) & bit) fail("flatten: pair listed twice");
+    t.near14[lo] |= bit;
+  }
+  long long far_all = 0;
+  for (int i = 0; i < n; ++i) far_all += std::max(0, n - 1 - i - kNearWindow);
+  if (far != far_all) fail("flatten: a distant pair is missing from the lists");
+  const int nb = (n + 31) / 32;
+  t.tile_off.push_back(0);
+  for (int bi = 0; bi < nb; ++bi)
+    for (int bj = bi; bj < nb; ++bj) {
+      t.tiles.push_back(uint32_t(bi) | (uint32_t(bj) << 16));
+      int cols = std::min(32, n - 32 * bj);
+      t.tile_off.push_back(t.tile_off.back() + cols);
+    }
   return t;
 }
 

@@ -23,6 +23,7 @@ namespace smmpb200 {
 constexpr int kNumTypes = 18;     // ECEPP atom classes (INCL.H mxtyat)
 constexpr int kChunk = 8;         // partners per vdW chunk
 constexpr int kMaxAtoms = 16383;  // 14-bit atom index in the packed pair words
+constexpr int kNearWindow = 64;   // pairs (i, i+1..i+64) carry explicit flags
 
 // Per type-pair constants, [ti*18+tj].  A/C of the 12-6 (or 12-10 hydrogen
 // bond) term, the halved repulsion of 1-4 pairs, and the squared distance
@@ -69,6 +70,14 @@ struct MolTopo {
   std::vector<uint32_t> chunks;        // i | j0<<14 | (len-1)<<28
   std::vector<uint32_t> pairs14;       // i | j<<14
   long long npairs = 0;                // pair terms per full evaluation
+  // The same pair set as a dense upper triangle: for atom i, bit k of
+  // near_mask[i] / near14[i] marks pair (i, i+1+k) as a normal / 1-4 pair;
+  // every pair more than kNearWindow apart is a normal pair (checked).  The
+  // triangle is cut into 32x32 tiles (tiles[t] = bi | bj<<16, bi <= bj);
+  // tile_off[t] is the first work item of tile t, one item per j column.
+  std::vector<uint64_t> near_mask, near14;
+  std::vector<uint32_t> tiles;
+  std::vector<int> tile_off;
   // solvation
   std::vector<int> heavy;              // atoms with rvdw > 0
   int nres = 0;
