@@ -38,7 +38,7 @@ extern "C" {
 /* Per-chain error words reported by the kernels (smmp_ens_errors). */
 #define SMMP_KERR_NONFINITE 1     /* NaN/Inf energy */
 #define SMMP_KERR_CONSISTENCY 2   /* |E_incremental - E_fresh| > tolerance at sweep end */
-#define SMMP_KERR_NEIGHBOURS 3    /* SASA neighbour buffer overflow */
+#define SMMP_KERR_NEIGHBOURS 3    /* reserved, never set: an atom with more SASA neighbours than the per-warp buffer holds is scanned directly */
 #define SMMP_KERR_TIMEOUT 4       /* a bounded wait gave up */
 
 /* Switches of the reference's COMMON blocks /epar_l/ (sh2, epsd, ientyp),

@@ -8,7 +8,7 @@ constexpr int kTypes = 18;
 constexpr int kTP = kTypes * kTypes;
 constexpr int kThreads = 512;            // threads per chain (one CTA per chain)
 constexpr int kWarps = kThreads / 32;
-constexpr int kMaxNeighbours = 128;      // SASA neighbours per atom (per-warp buffer)
+constexpr int kMaxNeighbours = 96;       // SASA neighbours per atom (per-warp buffer)
 
 // An MT19937 stream slot: 624 state words, mti, the head and tail counters
 // of a queue of tempered values already drawn from the state but not yet
@@ -124,7 +124,7 @@ enum ErrorCode : int {
   kErrNone = 0,
   kErrNonFinite = 1,      // NaN/Inf energy
   kErrConsistency = 2,    // |E_incremental - E_fresh| above tolerance at sweep end
-  kErrNeighbours = 3,     // SASA neighbour buffer overflow
+  kErrNeighbours = 3,     // reserved: a crowded SASA atom is scanned directly instead
   kErrTimeout = 4,        // a bounded wait gave up
 };
 

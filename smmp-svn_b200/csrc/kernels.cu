@@ -162,7 +162,7 @@ struct Scalars {
 
 struct Smem {
   double *x, *y, *z, *bx, *by, *bz;
-  double *toat, *sn, *cs;
+  double* toat;
   double *fx, *fz;
   double *cq;
   uint8_t* type;
@@ -197,15 +197,23 @@ __host__ __device__ inline size_t smem_layout(int n, int v, int npnt, bool sasa,
   t.x = (double*)take(8 * n);
   t.y = (double*)take(8 * n);
   t.z = (double*)take(8 * n);
-  t.bx = (double*)take(8 * n);
-  t.by = (double*)take(8 * n);
-  t.bz = (double*)take(8 * n);
   t.toat = (double*)take(8 * n);
-  t.sn = (double*)take(8 * n);
-  t.cs = (double*)take(8 * n);
-  t.fx = (double*)take(24 * n);
-  t.fz = (double*)take(24 * n);
   t.cq = (double*)take(8 * n);
+  // The rebuild frames (fx, fz) share one region with the proposal-only
+  // buffers (backup coordinates and FP32 copies): the rebuild overwrites them
+  // and refreshes the FP32 copies when it finishes.  Every sub-array starts
+  // on a 16-byte boundary (float4 accesses).
+  const size_t a8 = align16(8 * (size_t)n);
+  char* region = take(3 * a8 + 32 * (size_t)n);
+  if (base) {
+    t.bx = (double*)region;
+    t.by = (double*)(region + a8);
+    t.bz = (double*)(region + 2 * a8);
+    t.p4 = (float4*)(region + 3 * a8);
+    t.l4 = (float4*)(region + 3 * a8 + 16 * (size_t)n);
+    t.fx = (double*)region;                  // 24n bytes <= 3 * a8
+    t.fz = (double*)(region + 3 * a8);       // 24n bytes <= 32n
+  }
   t.type = (uint8_t*)take(n);
   t.vlvr = (double*)take(8 * (v > 0 ? v : 1));
   t.et = (double*)take(8 * (v > 0 ? v : 1));
@@ -217,8 +225,6 @@ __host__ __device__ inline size_t smem_layout(int n, int v, int npnt, bool sasa,
   t.tc = (double*)take(8 * kTP);
   t.tg = (double*)take(8 * kTP);
   t.thb = (int*)take(4 * kTP);
-  t.p4 = (float4*)take(16 * n);
-  t.l4 = (float4*)take(16 * n);
   t.tab4 = (float4*)take(16 * kTP);
   t.spt = (double*)take(sasa ? 8 * 3 * npnt : 8);
   t.nb = (double*)take(sasa ? 8 * 4 * kWarps * kMaxNeighbours : 8);
@@ -412,13 +418,15 @@ __device__ void first_frame(const DMol& m, Smem& s) {
   double z1 = ca * sg + sa * sb * cg, z2 = sa * sg - ca * sb * cg, z3 = cb * cg;
   d = sqrt(z1 * z1 + z2 * z2 + z3 * z3);
   ag[0][2] = z1 / d; ag[1][2] = z2 / d; ag[2][2] = z3 / d;
-  double ct2 = s.cs[i2], st2 = s.sn[i2], sa2 = m.sba[i2];
+  double st2, ct2, st3, ct3;
+  sincos(s.toat[i2], &st2, &ct2);
+  sincos(s.toat[i3], &st3, &ct3);
+  double sa2 = m.sba[i2];
   x1 = -m.cba[i2];
   x2 = -sa2 * ct2;
   x3 = -sa2 * st2;
   double dx = sqrt(x1 * x1 + x2 * x2 + x3 * x3);
   x1 /= dx; x2 /= dx; x3 /= dx;
-  double st3 = s.sn[i3], ct3 = s.cs[i3];
   z1 = -st3 * (st2 * x3 + ct2 * x2);
   z2 = st3 * ct2 * x1 + ct3 * st2;
   z3 = st3 * st2 * x1 - ct3 * ct2;
@@ -444,7 +452,8 @@ __device__ void first_frame(const DMol& m, Smem& s) {
 
 // Eyring step (bldmol.f:175-242): atom i from the frame of its parent ia.
 __device__ __forceinline__ void eyring(const DMol& m, Smem& s, int i, int ia) {
-  double ct = s.cs[i], st = s.sn[i];
+  double st, ct;
+  sincos(s.toat[i], &st, &ct);
   double ca = m.cba[i], sa = m.sba[i], bl = m.blen[i];
   double x1 = s.fx[3 * ia], x2 = s.fx[3 * ia + 1], x3 = s.fx[3 * ia + 2];
   double z1 = s.fz[3 * ia], z2 = s.fz[3 * ia + 1], z3 = s.fz[3 * ia + 2];
@@ -469,16 +478,9 @@ __device__ __forceinline__ void eyring(const DMol& m, Smem& s, int i, int ia) {
 }
 
 // Full rebuild of all coordinates from the dihedral state (bldmol.f:13-93):
-// sin/cos of every dihedral, the first frame, then one Eyring step per
-// depth level.
+// the first frame, then one Eyring step per depth level (each step takes the
+// sin/cos of its own dihedral).
 __device__ void full_rebuild(const DMol& m, Smem& s) {
-  for (int k = threadIdx.x; k < m.natoms; k += blockDim.x) {
-    double sv, cv;
-    sincos(s.toat[k], &sv, &cv);
-    s.sn[k] = sv;
-    s.cs[k] = cv;
-  }
-  __syncthreads();
   if (threadIdx.x == 0) first_frame(m, s);
   __syncthreads();
   for (int L = 1; L < m.nlevels; ++L) {
@@ -633,6 +635,36 @@ __device__ void pair_energy(const FFScalars& ff, const DMol& m, const Smem& s, i
 // exposed-point counts are those of the reference arithmetic.  Warps
 // [w0, w0+nw) take one heavy atom at a time; returns this thread's share of
 // eysl.
+// Is heavy atom j a neighbour of atom i (enysol.f:232-250: the spheres of
+// radius rvdw overlap), and its offset / squared radius in units of trad.
+__device__ __forceinline__ bool sasa_neighbour(const DMol& m, const Smem& s, int i, int j,
+                                               double trad, double xi, double yi, double zi,
+                                               double& dx, double& dy, double& dz, double& rb2) {
+  if (j == i) return false;
+  double rj = m.rvdw[j];
+  double ex = xi - s.x[j], ey = yi - s.y[j], ez = zi - s.z[j];
+  double lim = trad + rj;
+  // cheap pre-test with margin; the exact test below decides
+  if (ex * ex + ey * ey + ez * ez > lim * lim * 1.0000001 + 1e-12) return false;
+  dx = __ddiv_rn(ex, trad);
+  dy = __ddiv_rn(ey, trad);
+  dz = __ddiv_rn(ez, trad);
+  double dd = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+  double akrad = __ddiv_rn(rj, trad);
+  double dr = __dadd_rn(1.0, akrad);
+  dr = __dmul_rn(dr, dr);
+  rb2 = __dmul_rn(akrad, akrad);
+  return dd <= dr;
+}
+
+// Is the surface point (s0, s1, s2) inside the neighbour sphere (enysol.f:267-275).
+__device__ __forceinline__ bool sasa_buried(double s0, double s1, double s2, double dx, double dy,
+                                            double dz, double rb2) {
+  double t0 = __dadd_rn(dx, s0), t1 = __dadd_rn(dy, s1), t2 = __dadd_rn(dz, s2);
+  double sdd = __dadd_rn(__dadd_rn(__dmul_rn(t0, t0), __dmul_rn(t1, t1)), __dmul_rn(t2, t2));
+  return sdd <= rb2;
+}
+
 __device__ double sasa_energy(const FFScalars& ff, const DMol& m, Smem& s, int w0, int nw,
                               int* err) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -646,28 +678,9 @@ __device__ double sasa_energy(const FFScalars& ff, const DMol& m, Smem& s, int w
     int nn = 0;
     for (int base = 0; base < m.nheavy; base += 32) {
       int hj = base + lane;
-      bool take = false;
       double dx = 0, dy = 0, dz = 0, rb2 = 0;
-      if (hj < m.nheavy) {
-        int j = m.heavy[hj];
-        if (j != i) {
-          double rj = m.rvdw[j];
-          double ex = xi - s.x[j], ey = yi - s.y[j], ez = zi - s.z[j];
-          double lim = trad + rj;
-          // cheap pre-test with margin; the exact test below decides
-          if (ex * ex + ey * ey + ez * ez <= lim * lim * 1.0000001 + 1e-12) {
-            dx = __ddiv_rn(ex, trad);
-            dy = __ddiv_rn(ey, trad);
-            dz = __ddiv_rn(ez, trad);
-            double dd = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-            double akrad = __ddiv_rn(rj, trad);
-            double dr = __dadd_rn(1.0, akrad);
-            dr = __dmul_rn(dr, dr);
-            take = dd <= dr;
-            rb2 = __dmul_rn(akrad, akrad);
-          }
-        }
-      }
+      bool take = hj < m.nheavy &&
+                  sasa_neighbour(m, s, i, m.heavy[hj], trad, xi, yi, zi, dx, dy, dz, rb2);
       unsigned mask = __ballot_sync(0xffffffffu, take);
       int pos = nn + __popc(mask & ((1u << lane) - 1u));
       if (take && pos < kMaxNeighbours) {
@@ -678,25 +691,35 @@ __device__ double sasa_energy(const FFScalars& ff, const DMol& m, Smem& s, int w
       }
       nn += __popc(mask);
     }
-    if (nn > kMaxNeighbours) {
-      if (lane == 0) atomicCAS(err, 0, (int)kErrNeighbours);
-      nn = kMaxNeighbours;
-    }
     __syncwarp();
     int cnt = 0;
-    for (int p = lane; p < npnt; p += 32) {
-      double s0 = s.spt[3 * p], s1 = s.spt[3 * p + 1], s2 = s.spt[3 * p + 2];
-      bool exposed = true;
-      for (int k = 0; k < nn; ++k) {
-        double t0 = __dadd_rn(nb[4 * k], s0), t1 = __dadd_rn(nb[4 * k + 1], s1),
-               t2 = __dadd_rn(nb[4 * k + 2], s2);
-        double sdd = __dadd_rn(__dadd_rn(__dmul_rn(t0, t0), __dmul_rn(t1, t1)), __dmul_rn(t2, t2));
-        if (sdd <= nb[4 * k + 3]) {
-          exposed = false;
-          break;
+    if (nn <= kMaxNeighbours) {
+      for (int p = lane; p < npnt; p += 32) {
+        double s0 = s.spt[3 * p], s1 = s.spt[3 * p + 1], s2 = s.spt[3 * p + 2];
+        bool exposed = true;
+        for (int k = 0; k < nn; ++k) {
+          if (sasa_buried(s0, s1, s2, nb[4 * k], nb[4 * k + 1], nb[4 * k + 2], nb[4 * k + 3])) {
+            exposed = false;
+            break;
+          }
         }
+        cnt += exposed;
       }
-      cnt += exposed;
+    } else {
+      // More neighbours than the buffer holds (crowded, clashing
+      // conformations): test each point against every heavy atom directly,
+      // with the same arithmetic, so the count is the same.
+      for (int p = lane; p < npnt; p += 32) {
+        double s0 = s.spt[3 * p], s1 = s.spt[3 * p + 1], s2 = s.spt[3 * p + 2];
+        bool exposed = true;
+        for (int hj = 0; hj < m.nheavy && exposed; ++hj) {
+          double dx, dy, dz, rb2;
+          if (sasa_neighbour(m, s, i, m.heavy[hj], trad, xi, yi, zi, dx, dy, dz, rb2) &&
+              sasa_buried(s0, s1, s2, dx, dy, dz, rb2))
+            exposed = false;
+        }
+        cnt += exposed;
+      }
     }
     for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
     if (lane == 0) {
@@ -914,6 +937,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_energy(DMolSet set, DChains ch,
 // evaluates every pair of the lists.  The start of sweep k+1 reuses the
 // coordinates and energy of the check that closed sweep k (same variables),
 // after the setvar call the reference makes there.
+// Atom t of the set a proposal moves: the subtree [lo, lo+span) or, when
+// `flip`, every other atom.
+__device__ __forceinline__ int moved_atom(int t, int lo, int span, bool flip) {
+  return flip ? (t < lo ? t : t + span) : lo + t;
+}
+
 template <bool F32>
 __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, DWeight w, int first,
                                                        int nsweeps, int flags, double check_tol) {
@@ -978,15 +1007,25 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
     for (int p = 0; p < m.nfree; ++p) {
       const Proposal cur = sc.cur;
       const int lo = m.var_lo[cur.jv], hi = m.var_hi[cur.jv];
+      // The rebuild holds the first three backbone atoms in place (setgbl):
+      // when the subtree holds i3 (the dihedral about i1-i2), the rest of the
+      // molecule turns by -theta instead, so the coordinates keep the
+      // rebuild's orientation (the SASA test points are fixed in space).
+      const bool flip = lo <= m.i3 && m.i3 <= hi;
+      const int span = hi - lo + 1;
+      const int nmoved = flip ? m.natoms - span : span;
       // ---- phase A: rotate the subtree of cur.jv about its bond (+theta)
       {
+        const double sth = flip ? -cur.sth : cur.sth;
         double px = s.x[cur.b], py = s.y[cur.b], pz = s.z[cur.b];
         double kx = px - s.x[cur.a], ky = py - s.y[cur.a], kz = pz - s.z[cur.a];
         double inv = rsqrt(kx * kx + ky * ky + kz * kz);
         kx *= inv;
         ky *= inv;
         kz *= inv;
-        for (int k = lo + threadIdx.x; k <= hi; k += blockDim.x) {
+        for (int t = threadIdx.x; t < nmoved; t += blockDim.x) {
+          const int k = moved_atom(t, lo, span, flip);
+          if (flip && (k == cur.a || k == cur.b)) continue;   // on the axis
           double vx = s.x[k] - px, vy = s.y[k] - py, vz = s.z[k] - pz;
           s.bx[k] = s.x[k];
           s.by[k] = s.y[k];
@@ -994,9 +1033,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
           double kd = kx * vx + ky * vy + kz * vz;
           double cx = ky * vz - kz * vy, cy = kz * vx - kx * vz, cz = kx * vy - ky * vx;
           double f = kd * (1.0 - cur.cth);
-          s.x[k] = px + vx * cur.cth + cx * cur.sth + kx * f;
-          s.y[k] = py + vy * cur.cth + cy * cur.sth + ky * f;
-          s.z[k] = pz + vz * cur.cth + cz * cur.sth + kz * f;
+          s.x[k] = px + vx * cur.cth + cx * sth + kx * f;
+          s.y[k] = py + vy * cur.cth + cy * sth + ky * f;
+          s.z[k] = pz + vz * cur.cth + cz * sth + kz * f;
           if (F32) f32_copy(s, k);
         }
       }
@@ -1047,7 +1086,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
         eol = enw;
         etor = etor_new;
       } else {
-        for (int k = lo + threadIdx.x; k <= hi; k += blockDim.x) {
+        for (int t = threadIdx.x; t < nmoved; t += blockDim.x) {
+          const int k = moved_atom(t, lo, span, flip);
+          if (flip && (k == cur.a || k == cur.b)) continue;
           s.x[k] = s.bx[k];
           s.y[k] = s.by[k];
           s.z[k] = s.bz[k];

@@ -164,9 +164,15 @@ DeviceSet::DeviceSet(const std::vector<std::shared_ptr<Molecule>>& mols) {
     set_.stage_lists = 0;
     set_.stage_bytes = (int)without;
   }
-  size_t sm = sweep_smem_bytes(set_);
-  if (sm > 227 * 1024)
+  // A large molecule stages only the leading topology arrays that fit; the
+  // kernel reads the rest from global memory (stage_mol stops at the first
+  // array past the end of the pool).
+  const size_t limit = 227 * 1024;
+  set_.stage_bytes = 0;
+  size_t state = sweep_smem_bytes(set_);
+  if (state > limit)
     throw std::runtime_error("DeviceSet: molecule too large for one CTA's shared memory");
+  set_.stage_bytes = (int)std::min(set_.stage_lists ? with_lists : without, limit - state);
 }
 
 DeviceSet::~DeviceSet() {

@@ -117,6 +117,8 @@ MolTopo flatten(Assembly& a, int nml) {
   for (int v = ifivr; v < ifivr + nv; ++v) {
     if (a.ityvr[v] != 3) fail("flatten: only torsion variables exist in the ECEPP libraries");
     int iat = a.iatvr[v], iow = a.iowat[iat];
+    if (A(iow) == t.i1)
+      fail("flatten: a variable turns about the first backbone atom, which has no parent bond");
     t.var_atom.push_back(A(iat));
     t.var_base.push_back(A(iow));
     for (int j = 1; j <= a.nbdat[iow]; ++j) {
