@@ -1,21 +1,28 @@
-"""Benchmark: MC sweeps/s of parallel tempering of Met-enkephalin on one B200.
+"""Benchmark: MC sweeps/s of the energy-and-sweep path on one B200.
 
-Workload (the headline configuration): 64 replicas of Met-enkephalin
-(Tyr-Gly-Gly-Phe-Met, nh2/cooh ends, 75 atoms, 24 free dihedrals), ECEPP/3 in
-vacuum, temperatures geometric 100-1000 K, neighbour exchange after every
-sweep, seeded uniform random start.  Inputs are synthetic (seeded random
-starts of the reference's own Met-enkephalin deck).
+Default workload (the headline configuration): parallel tempering of 64
+replicas of Met-enkephalin (Tyr-Gly-Gly-Phe-Met, nh2/cooh ends, 75 atoms, 24
+free dihedrals), ECEPP/3 in vacuum, temperatures geometric 100-1000 K,
+neighbour exchange after every sweep, seeded uniform random start.  Inputs are
+synthetic (seeded random starts of the reference's own Met-enkephalin deck).
 
-A step is one CUDA-graph launch of SWEEPS_PER_STEP parallel-tempering sweeps
-(each: one sweep of every replica, then one exchange).  value = replica sweeps
-per second of the whole job.  Every step is timed with CUDA events on the
-stream the kernels run on; L2 is flushed (a 256 MiB write) between steps.
+A step is one CUDA-graph launch of 16 parallel-tempering sweeps (each: one
+sweep of every replica, then one exchange).  value = replica sweeps per second
+of the whole job.  Every step is timed with CUDA events on the stream the
+kernels run on; L2 is flushed (a 256 MiB write) between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload pt_enkefa64|polyala256|protein60_pt128]
+
+The other workloads measure the larger configurations with the same timing
+rules: 256 independent Ace-Ala_n-NMe chains (n uniform in 10..40, seeded) with
+SASA solvation at 300 K, and parallel tempering of a 60-residue protein drawn
+from the natural amino-acid composition (926 atoms, 365 dihedrals) with SASA,
+128 replicas geometric 250-600 K.
 
 --impl reference times the reference's algorithm on the host cores: the CPU
 oracle (a C++ restatement of the Fortran, which no Fortran compiler here can
-build) running the same replicas with all host threads.
+build) running the same chains with all host threads.
 """
 import argparse
 import ctypes
@@ -24,6 +31,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -32,23 +40,123 @@ DATA = os.path.join(ROOT, "tests", "golden", "smmp_data") + "/"
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 ORACLE_SO = os.path.join(ROOT, "oracle", "liboracle_smmp.so")
 
-NREP = 64
-TMIN, TMAX = 100.0, 1000.0
-SWEEPS_PER_STEP = 16
 METRIC = "MC sweeps/s (all replicas, 1 B200): plain vs batched+surrogate, ΔE≤1e-3"
 GAS = 1.98773e-3
 
 
-def temperatures(n=NREP):
-    return [TMIN * (TMAX / TMIN) ** (k / (n - 1)) for k in range(n)]
+def geometric(tmin, tmax, n):
+    return [tmin * (tmax / tmin) ** (k / (n - 1)) for k in range(n)]
 
 
-def config(extra=None):
-    c = {"workload": "parallel tempering, Met-enkephalin (75 atoms, 24 dihedrals), "
-                     "64 replicas 100-1000 K geometric, ECEPP/3 vacuum, exchange every sweep",
-         "replicas": NREP, "sweeps_per_step": SWEEPS_PER_STEP, "atoms": 75, "dihedrals": 24,
-         "pair_terms_per_evaluation": 2498, "pair_precision": "fp32 terms, fp64 guard+sum",
-         "l2": "flushed (256 MiB write) between timed steps", "parallelism": "replicas"}
+# ------------------------------------------------------------------ workloads
+class Workload:
+    """One benchmark configuration: its molecules, chains, temperatures and
+    what one timed step does."""
+    name = ""
+    sweeps_per_step = 1
+    pt = False
+    itysol = 0
+
+    def molecule_files(self):
+        """[(seqfile, varfile or None)] of the distinct molecules."""
+        raise NotImplementedError
+
+    def chain_mol(self):
+        raise NotImplementedError
+
+    def temperatures(self):
+        raise NotImplementedError
+
+    def seeds(self, rank):
+        return [31433 + 1000 * k + 100000 * rank for k in range(len(self.chain_mol()))]
+
+    def describe(self):
+        raise NotImplementedError
+
+
+class PTEnkefa64(Workload):
+    name = "pt_enkefa64"
+    sweeps_per_step = 16
+    pt = True
+
+    def molecule_files(self):
+        return [(DATA + "enkefa.seq", DATA + "enkefa.var")]
+
+    def chain_mol(self):
+        return [0] * 64
+
+    def temperatures(self):
+        return geometric(100.0, 1000.0, 64)
+
+    def describe(self):
+        return {"workload": "parallel tempering, Met-enkephalin (75 atoms, 24 dihedrals), "
+                            "64 replicas 100-1000 K geometric, ECEPP/3 vacuum, exchange every sweep",
+                "replicas": 64, "sweeps_per_step": self.sweeps_per_step, "atoms": 75,
+                "dihedrals": 24, "pair_terms_per_evaluation": 2498}
+
+
+class Polyala256(Workload):
+    name = "polyala256"
+    sweeps_per_step = 4
+    itysol = 1
+
+    def __init__(self):
+        from smmp.sequences import polyala_lengths
+        self.lengths = polyala_lengths(256, seed=12345)
+        self.distinct = sorted(set(self.lengths))
+
+    def molecule_files(self):
+        from smmp.sequences import polyala, write_seq
+        d = tempfile.mkdtemp(prefix="smmp_bench_")
+        return [(write_seq(os.path.join(d, "ala%d.seq" % n), polyala(n), "ala%d" % n), None)
+                for n in self.distinct]
+
+    def chain_mol(self):
+        return [self.distinct.index(n) for n in self.lengths]
+
+    def temperatures(self):
+        return [300.0] * 256
+
+    def describe(self):
+        return {"workload": "256 independent chains Ace-Ala_n-NMe, n uniform 10-40 (seed 12345), "
+                            "ECEPP/3 + SASA solvation (itysol 1), 300 K canonical",
+                "chains": 256, "sweeps_per_step": self.sweeps_per_step,
+                "mean_residues": sum(self.lengths) / 256.0}
+
+
+class Protein60PT128(Workload):
+    name = "protein60_pt128"
+    sweeps_per_step = 2
+    pt = True
+    itysol = 1
+
+    def molecule_files(self):
+        from smmp.sequences import natural_protein, write_seq
+        d = tempfile.mkdtemp(prefix="smmp_bench_")
+        return [(write_seq(os.path.join(d, "protein60.seq"), natural_protein(60), "protein60"),
+                 None)]
+
+    def chain_mol(self):
+        return [0] * 128
+
+    def temperatures(self):
+        return geometric(250.0, 600.0, 128)
+
+    def describe(self):
+        return {"workload": "parallel tempering, 60-residue protein of natural composition "
+                            "(seed 2024; 926 atoms, 365 dihedrals), ECEPP/3 + SASA solvation, "
+                            "128 replicas 250-600 K geometric, exchange every sweep",
+                "replicas": 128, "sweeps_per_step": self.sweeps_per_step, "atoms": 926,
+                "dihedrals": 365, "pair_terms_per_evaluation": 425508}
+
+
+WORKLOADS = {w.name: w for w in (PTEnkefa64, Polyala256, Protein60PT128)}
+
+
+def config(wl, extra=None):
+    c = wl.describe()
+    c.update({"pair_precision": "fp32 terms, fp64 guard+sum",
+              "l2": "flushed (256 MiB write) between timed steps", "parallelism": "replicas"})
     if extra:
         c.update(extra)
     return c
@@ -115,29 +223,64 @@ def oracle_lib():
     return L
 
 
-def cpu_baseline(target_seconds=15.0):
-    """The reference algorithm (CPU oracle, FP64) on the same replicas over all
-    host threads, on a bounded number of sweeps per replica."""
-    L = oracle_lib()
-    h = ctypes.c_void_p(L.orc_create(DATA.encode(), 0, 0, 0))
-    rc = L.orc_init_molecule(h, (DATA + "enkefa.seq").encode(), (DATA + "enkefa.var").encode(),
-                             b"nh2", b"cooh")
-    assert rc == 0
-    L.orc_sgrnd(h, ctypes.c_int(31433))
-    L.orc_random_start(h)
-    cores = os.cpu_count() or 1
-    seeds = (ctypes.c_int * NREP)(*[31433 + 1000 * k for k in range(NREP)])
-    betas = (ctypes.c_double * NREP)(*[1.0 / (t * GAS) for t in temperatures()])
-    out = (ctypes.c_double * NREP)()
-    # calibrate on one thread-worth of work, then size the sample
-    t = L.orc_bench_chains(h, min(cores, NREP), seeds, betas, 2, cores, out)
-    per_sweep_round = t / 2.0 * (NREP / min(cores, NREP))
-    nsw = max(2, int(target_seconds / max(per_sweep_round, 1e-6)))
-    t = L.orc_bench_chains(h, NREP, seeds, betas, nsw, cores, out)
-    value = NREP * nsw / t
-    return {"value": value, "unit": "sweeps/s", "cores": cores, "kind": "port",
-            "sample": "%d replicas x %d sweeps of the same workload (no exchanges), %.1f s"
-                      % (NREP, nsw, t)}
+class OracleChains:
+    """The reference algorithm (CPU oracle, FP64) on the workload's chains,
+    every host thread busy: one handle per distinct molecule, seeded random
+    start."""
+
+    def __init__(self, wl, files):
+        self.L = oracle_lib()
+        self.cores = os.cpu_count() or 1
+        self.handles = []
+        for seq, var in files:
+            h = ctypes.c_void_p(self.L.orc_create(DATA.encode(), 0, 0, wl.itysol))
+            rc = self.L.orc_init_molecule(h, seq.encode(), (var or " ").encode(), b"nh2", b"cooh")
+            assert rc == 0
+            self.L.orc_sgrnd(h, ctypes.c_int(31433))
+            self.L.orc_random_start(h)
+            self.handles.append(h)
+        self.cm = wl.chain_mol()
+        self.temps = wl.temperatures()
+
+    def run(self, mol, nchains, nsweeps):
+        """Seconds for nchains chains of molecule `mol` x nsweeps on all threads."""
+        chains = [c for c, m in enumerate(self.cm) if m == mol]
+        chains = (chains * (1 + nchains // max(1, len(chains))))[:nchains]
+        seeds = (ctypes.c_int * nchains)(*[31433 + 1000 * c for c in chains])
+        betas = (ctypes.c_double * nchains)(*[1.0 / (self.temps[c] * GAS) for c in chains])
+        out = (ctypes.c_double * nchains)()
+        return self.L.orc_bench_chains(self.handles[mol], nchains, seeds, betas, nsweeps,
+                                       self.cores, out)
+
+    def sample(self, target_seconds):
+        """(chain sweeps per second, description, seconds) from one bounded
+        sample.  One molecule: all chains for as many sweeps as fit
+        target_seconds.  Several: for each molecule, `cores` chains (every
+        thread busy) for one sweep; each molecule's per-chain-sweep cost is
+        weighted by its number of chains in the workload."""
+        n = len(self.handles)
+        nchains = len(self.cm)
+        if n == 1:
+            probe = self.run(0, min(self.cores, nchains), 1)
+            per_round = probe * max(1, nchains // self.cores)
+            nsw = max(1, int(target_seconds / max(per_round, 1e-6)))
+            t = self.run(0, nchains, nsw)
+            return nchains * nsw / t, "%d chains x %d sweeps, %.1f s" % (nchains, nsw, t), t
+        cost = 0.0
+        total = 0.0
+        for m in range(n):
+            t = self.run(m, self.cores, 1)
+            total += t
+            cost += self.cm.count(m) * t / self.cores
+        return nchains / cost, ("%d chains x 1 sweep of each of %d molecules, weighted by the "
+                                "workload's chain counts, %.1f s" % (self.cores, n, total)), total
+
+
+def cpu_baseline(wl, files, target_seconds=15.0):
+    oc = OracleChains(wl, files)
+    value, sample, _ = oc.sample(target_seconds)
+    return {"value": value, "unit": "sweeps/s", "cores": oc.cores, "kind": "port",
+            "sample": sample + " (no exchanges)"}
 
 
 def max_over_ranks(values, world, device=None):
@@ -158,26 +301,35 @@ def job_rate(units_per_rank, world, ms):
 
 # ------------------------------------------------------------------ our arm
 def run_ours(args, rank, world):
-    import numpy as np
     import torch
     from smmp.ensemble import Ensemble, Molecule
 
+    wl = WORKLOADS[args.workload]()
+    spp = wl.sweeps_per_step
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
     if world > 1:
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    mol = Molecule(DATA + "enkefa.seq", DATA + "enkefa.var", libdir=DATA)
-    temps = temperatures()
-    betas = [1.0 / (t * GAS) for t in temps]
-    seeds = [31433 + 1000 * k + 100000 * rank for k in range(NREP)]
-    ens = Ensemble([mol], [0] * NREP, seeds, betas, fp32=True)
+    files = wl.molecule_files()
+    mols = [Molecule(seq, var, libdir=DATA, itysol=wl.itysol) for seq, var in files]
+    cm = wl.chain_mol()
+    nch = len(cm)
+    betas = [1.0 / (t * GAS) for t in wl.temperatures()]
+    ens = Ensemble(mols, cm, wl.seeds(rank), betas, fp32=True)
     stream = torch.cuda.Stream()
     ens.set_stream(stream.cuda_stream)
     ens.random_start()
-    ens.set_pt(betas, wrap=False, exchange_seed=4711 + rank)
+    if wl.pt:
+        ens.set_pt(betas, wrap=False, exchange_seed=4711 + rank)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def step():
+        if wl.pt:
+            ens.pt_sweeps(spp, graph_chunk=spp)
+        else:
+            ens.sweeps(spp)
 
     def barrier():
         torch.cuda.synchronize()
@@ -186,7 +338,7 @@ def run_ours(args, rank, world):
         torch.cuda.synchronize()
 
     for _ in range(args.warmup):
-        ens.pt_sweeps(SWEEPS_PER_STEP, graph_chunk=SWEEPS_PER_STEP)
+        step()
     # ---- device-timed region: K steps, each bracketed by events on the stream
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
@@ -196,12 +348,12 @@ def run_ours(args, rank, world):
             with torch.cuda.stream(stream):
                 flush.zero_()
                 starts[k].record(stream)
-            ens.pt_sweeps(SWEEPS_PER_STEP, graph_chunk=SWEEPS_PER_STEP)
+            step()
             ends[k].record(stream)
         barrier()
     ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
     # ---- roofline: the sweep kernel alone, one launch per sweep, event-timed
-    n_roof = 50
+    n_roof = 50 if wl.name == "pt_enkefa64" else 8
     rs = [torch.cuda.Event(enable_timing=True) for _ in range(n_roof)]
     re_ = [torch.cuda.Event(enable_timing=True) for _ in range(n_roof)]
     for k in range(n_roof):
@@ -213,17 +365,17 @@ def run_ours(args, rank, world):
     torch.cuda.synchronize()
     sweep_kernel_ms = statistics.mean(a.elapsed_time(b) for a, b in zip(rs, re_))
     # ---- end-to-end through the C ABI with host buffers every step
-    vl = torch.empty((NREP, ens.vstride), dtype=torch.float64, pin_memory=True).numpy()
+    vl = torch.empty((nch, ens.vstride), dtype=torch.float64, pin_memory=True).numpy()
     vl[:] = ens.vlvr()
-    e2e_steps = max(10, args.steps // 4)
+    e2e_steps = max(10, args.steps // 4) if wl.name == "pt_enkefa64" else max(3, args.steps // 4)
     barrier()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     t0.record(stream)
     for _ in range(e2e_steps):
         ens.set_vlvr(vl)                                   # H2D of the step's state
-        ens.pt_sweeps(SWEEPS_PER_STEP, graph_chunk=SWEEPS_PER_STEP)
-        e_host = ens.energies()                            # D2H of the result
+        step()
+        ens.energies()                                     # D2H of the result
         vl[:] = ens.vlvr()                                 # D2H of the new state
     t1.record(stream)
     barrier()
@@ -234,14 +386,13 @@ def run_ours(args, rank, world):
 
     # max over ranks
     ms, e2e_ms, sweep_kernel_ms = max_over_ranks([ms, e2e_ms, sweep_kernel_ms], world, "cuda")
-    value = job_rate(NREP * SWEEPS_PER_STEP * args.steps, world, ms)
-    e2e_value = job_rate(NREP * SWEEPS_PER_STEP * e2e_steps, world, e2e_ms)
+    value = job_rate(nch * spp * args.steps, world, ms)
+    e2e_value = job_rate(nch * spp * e2e_steps, world, e2e_ms)
 
     # roofline: algorithmic HBM bytes per launch of the sweep kernel
     # (16 B coordinates per atom + 8 B per dihedral + 8 B energy, per
-    # evaluation; nvr evaluations per sweep; 64 replicas per launch)
-    natoms, nvr = 75, 24
-    bytes_per_launch = NREP * nvr * (16 * natoms + 8 * nvr + 8)
+    # evaluation; one evaluation per free dihedral per sweep; every chain)
+    bytes_per_launch = sum(mols[m].nvr * (16 * mols[m].natoms + 8 * mols[m].nvr + 8) for m in cm)
     achieved = bytes_per_launch / (sweep_kernel_ms / 1000.0) / 1e9
     peak, peak_src = 6650.0, "fallback"
     if os.path.exists(PEAKS):
@@ -252,7 +403,7 @@ def run_ours(args, rank, world):
             pass
     traffic = None
     tf = os.path.join(ROOT, "profiles", "k_sweep_traffic.json")
-    if os.path.exists(tf):
+    if wl.name == "pt_enkefa64" and os.path.exists(tf):
         try:
             traffic = json.load(open(tf)).get("bytes_per_launch")
         except Exception:
@@ -262,12 +413,14 @@ def run_ours(args, rank, world):
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 pair terms / f64 rebuild+acceptance",
-        "data": "synthetic (seeded random starts of the reference's Met-enkephalin deck)",
-        "config": config(),
+        "data": ("synthetic (seeded random starts of the reference's Met-enkephalin deck)"
+                 if wl.name == "pt_enkefa64"
+                 else "synthetic (seeded sequences, seeded random starts)"),
+        "config": config(wl),
         "e2e": {"value": e2e_value, "unit": "sweeps/s",
                 "h2d_bytes_per_step": int(vl.nbytes),
-                "d2h_bytes_per_step": int(vl.nbytes + 8 * NREP)},
-        "gpu_launches": args.steps * SWEEPS_PER_STEP * 2,
+                "d2h_bytes_per_step": int(vl.nbytes + 8 * nch)},
+        "gpu_launches": args.steps * (spp * 2 if wl.pt else 1),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_source": peak_src, "kernel": "k_sweep<true>",
@@ -276,7 +429,7 @@ def run_ours(args, rank, world):
         "clocks": clk.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_baseline()
+        line["cpu_baseline"] = cpu_baseline(wl, files)
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
@@ -287,33 +440,39 @@ def run_ours(args, rank, world):
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    L = oracle_lib()
-    h = ctypes.c_void_p(L.orc_create(DATA.encode(), 0, 0, 0))
-    assert L.orc_init_molecule(h, (DATA + "enkefa.seq").encode(), (DATA + "enkefa.var").encode(),
-                               b"nh2", b"cooh") == 0
-    L.orc_sgrnd(h, ctypes.c_int(31433))
-    L.orc_random_start(h)
-    cores = os.cpu_count() or 1
-    seeds = (ctypes.c_int * NREP)(*[31433 + 1000 * k for k in range(NREP)])
-    betas = (ctypes.c_double * NREP)(*[1.0 / (t * GAS) for t in temperatures()])
-    out = (ctypes.c_double * NREP)()
-    # each step: every replica 20 sweeps (a bounded sample of the workload)
-    per = 20
-    for _ in range(args.warmup):
-        L.orc_bench_chains(h, NREP, seeds, betas, 1, cores, out)
+    wl = WORKLOADS[args.workload]()
+    files = wl.molecule_files()
+    oc = OracleChains(wl, files)
+    nch = len(wl.chain_mol())
+    enk = wl.name == "pt_enkefa64"
+    # each step: a bounded sample of the workload (every replica 20 sweeps for
+    # Met-enkephalin; the per-molecule sample of OracleChains otherwise)
+    for _ in range(args.warmup if enk else 0):
+        oc.run(0, nch, 1)
     total = 0.0
+    units = 0.0
+    sample = ""
     for _ in range(args.steps):
-        total += L.orc_bench_chains(h, NREP, seeds, betas, per, cores, out)
-    value = NREP * per * args.steps / total
+        if enk:
+            per = 20
+            total += oc.run(0, nch, per)
+            units += nch * per
+            sample = "%d replicas x %d sweeps per step, %d steps" % (nch, per, args.steps)
+        else:
+            rate, sample, t = oc.sample(5.0)
+            total += t
+            units += rate * t
+    value = units / total
+    extra = {"pair_precision": "fp64 (reference arithmetic)"}
+    if enk:
+        extra["sweeps_per_step"] = 20
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "sweeps/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total * 1000.0 / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config(
-            {"sweeps_per_step": per, "pair_precision": "fp64 (reference arithmetic)"}),
-        "cpu_baseline": {"value": value, "unit": "sweeps/s", "cores": cores, "kind": "port",
-                         "sample": "%d replicas x %d sweeps per step, %d steps"
-                                   % (NREP, per, args.steps)},
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config(wl, extra),
+        "cpu_baseline": {"value": value, "unit": "sweeps/s", "cores": oc.cores, "kind": "port",
+                         "sample": sample},
         "e2e": {"value": value, "unit": "sweeps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0}}), flush=True)
 
@@ -324,6 +483,7 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="pt_enkefa64", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
