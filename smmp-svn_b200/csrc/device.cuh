@@ -9,6 +9,7 @@ constexpr int kTP = kTypes * kTypes;
 constexpr int kThreads = 512;            // threads per chain (one CTA per chain)
 constexpr int kWarps = kThreads / 32;
 constexpr int kMaxNeighbours = 96;       // SASA neighbours per atom (per-warp buffer)
+constexpr int kSasaQueue = 64;           // SASA neighbour candidates queued per warp
 
 // An MT19937 stream slot: 624 state words, mti, the head and tail counters
 // of a queue of tempered values already drawn from the state but not yet
@@ -50,11 +51,9 @@ struct DMol {
   const int* heavy;
   const int* residue_of_atom;
   // dense pair set (topology.hpp)
-  const unsigned long long* near_mask;
+  const unsigned long long* near_mask;   // row form of the pair set (rows != 0)
   const unsigned long long* near14;
-  const uint32_t* tiles;
-  const int* tile_off;
-  int ntiles;
+  int rows;
 };
 
 // Force field constants read by every chain (copied to shared memory).
@@ -79,6 +78,7 @@ struct DMolSet {
   int max_atoms, max_vars;   // shared-memory sizing
   int stage_bytes;           // shared-memory pool for the staged topology
   int stage_lists;           // 1: the pair lists are staged too (they fit)
+  int any_rows;              // 1: some molecule evaluates its pairs by rows
   const DForceField* ff;     // device
   FFScalars f;
 };

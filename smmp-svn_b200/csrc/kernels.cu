@@ -177,7 +177,9 @@ struct Smem {
   float4* l4;            //                 {x_lo, y_lo, z_lo, 0}, x = x_hi + x_lo
   float4* tab4;          // {A, A14, C, +-guard r^2}; negative guard: H-bond pair
   double* spt;
-  double* nb;
+  float4* nbf;           // SASA neighbours per warp: (dx, dy, dz, rb2) in FP32
+  int* nbj;              // and their atom index (for the exact FP64 re-test)
+  int* sq;               // SASA neighbour candidates per warp (kSasaQueue)
   Scalars* sc;
   DMol* mol;
   char* pool;            // staged topology (see stage_mol)
@@ -227,7 +229,9 @@ __host__ __device__ inline size_t smem_layout(int n, int v, int npnt, bool sasa,
   t.thb = (int*)take(4 * kTP);
   t.tab4 = (float4*)take(16 * kTP);
   t.spt = (double*)take(sasa ? 8 * 3 * npnt : 8);
-  t.nb = (double*)take(sasa ? 8 * 4 * kWarps * kMaxNeighbours : 8);
+  t.nbf = (float4*)take(sasa ? 16 * kWarps * kMaxNeighbours : 16);
+  t.nbj = (int*)take(sasa ? 4 * kWarps * kMaxNeighbours : 4);
+  t.sq = (int*)take(sasa ? 4 * kWarps * kSasaQueue : 4);
   t.sc = (Scalars*)take(sizeof(Scalars));
   t.mol = (DMol*)take(sizeof(DMol));
   t.pool = take(0);
@@ -246,15 +250,10 @@ __device__ Smem carve(const DMolSet& set, bool sasa) {
 // array, in the order stage_mol copies them (host sizing and device staging
 // must agree exactly).
 __host__ __device__ inline size_t stage_size(int natoms, int nvar, int nsib, int nlevels, int nfree,
-                                             int nchunks, int n14, int nheavy, bool lists) {
+                                             int nchunks, int n14, int nheavy, bool rows,
+                                             bool lists) {
   size_t b = 0;
   auto a = [&](size_t elem, int n) { b += align16(elem * (size_t)(n > 0 ? n : 1)); };
-  a(4, natoms);        // iow
-  a(4, natoms);        // level_atoms
-  a(4, nlevels + 1);   // level_off
-  a(8, natoms);        // blen
-  a(8, natoms);        // cba
-  a(8, natoms);        // sba
   a(4, nvar);          // var_atom
   a(4, nvar);          // var_base
   a(4, nvar);          // var_lo
@@ -266,9 +265,19 @@ __host__ __device__ inline size_t stage_size(int natoms, int nvar, int nsib, int
   a(8, nvar);          // var_rn
   a(8, nvar);          // axvr
   a(4, nfree);         // idvr
+  if (rows) {
+    a(8, natoms);      // near_mask
+    a(8, natoms);      // near14
+  }
   a(4, nheavy);        // heavy
   a(8, natoms);        // rvdw
   a(8, natoms);        // sigma
+  a(4, natoms);        // iow
+  a(4, natoms);        // level_atoms
+  a(4, nlevels + 1);   // level_off
+  a(8, natoms);        // blen
+  a(8, natoms);        // cba
+  a(8, natoms);        // sba
   if (lists) {
     a(4, nchunks);     // chunks
     a(4, n14);         // pairs14
@@ -310,12 +319,8 @@ __device__ const DMol& stage_mol(const DMolSet& set, const DChains& ch, int c, S
   const char* end = smem_raw + dynamic_smem_bytes();
   bool ok = true;
   DMol m = g;
-  m.iow = stage_array(g.iow, g.natoms, pool, end, ok);
-  m.level_atoms = stage_array(g.level_atoms, g.natoms, pool, end, ok);
-  m.level_off = stage_array(g.level_off, g.nlevels + 1, pool, end, ok);
-  m.blen = stage_array(g.blen, g.natoms, pool, end, ok);
-  m.cba = stage_array(g.cba, g.natoms, pool, end, ok);
-  m.sba = stage_array(g.sba, g.natoms, pool, end, ok);
+  // per-proposal arrays first: a molecule too large for the whole pool keeps
+  // the rebuild arrays (used twice per sweep) in global memory
   m.var_atom = stage_array(g.var_atom, g.nvar, pool, end, ok);
   m.var_base = stage_array(g.var_base, g.nvar, pool, end, ok);
   m.var_lo = stage_array(g.var_lo, g.nvar, pool, end, ok);
@@ -327,9 +332,19 @@ __device__ const DMol& stage_mol(const DMolSet& set, const DChains& ch, int c, S
   m.var_rn = stage_array(g.var_rn, g.nvar, pool, end, ok);
   m.axvr = stage_array(g.axvr, g.nvar, pool, end, ok);
   m.idvr = stage_array(g.idvr, g.nfree, pool, end, ok);
+  if (g.rows) {
+    m.near_mask = stage_array(g.near_mask, g.natoms, pool, end, ok);
+    m.near14 = stage_array(g.near14, g.natoms, pool, end, ok);
+  }
   m.heavy = stage_array(g.heavy, g.nheavy, pool, end, ok);
   m.rvdw = stage_array(g.rvdw, g.natoms, pool, end, ok);
   m.sigma = stage_array(g.sigma, g.natoms, pool, end, ok);
+  m.iow = stage_array(g.iow, g.natoms, pool, end, ok);
+  m.level_atoms = stage_array(g.level_atoms, g.natoms, pool, end, ok);
+  m.level_off = stage_array(g.level_off, g.nlevels + 1, pool, end, ok);
+  m.blen = stage_array(g.blen, g.natoms, pool, end, ok);
+  m.cba = stage_array(g.cba, g.natoms, pool, end, ok);
+  m.sba = stage_array(g.sba, g.natoms, pool, end, ok);
   if (set.stage_lists) {
     m.chunks = stage_array(g.chunks, g.nchunks, pool, end, ok);
     m.pairs14 = stage_array(g.pairs14, g.n14, pool, end, ok);
@@ -360,12 +375,14 @@ __device__ void load_static(const DForceField& ff, const DMol& m, Smem& s, bool 
 }
 
 // FP32 copy of atom k's position as a hi+lo pair of floats, so that FP32
-// differences of two positions keep FP64-difference accuracy.
+// differences of two positions keep FP64-difference accuracy; p4.w holds the
+// charge and l4.w the atom type (as int bits).
 __device__ __forceinline__ void f32_copy(Smem& s, int k) {
   double x = s.x[k], y = s.y[k], z = s.z[k];
   float xh = (float)x, yh = (float)y, zh = (float)z;
   s.p4[k] = make_float4(xh, yh, zh, (float)s.cq[k]);
-  s.l4[k] = make_float4((float)(x - (double)xh), (float)(y - (double)yh), (float)(z - (double)zh), 0.f);
+  s.l4[k] = make_float4((float)(x - (double)xh), (float)(y - (double)yh), (float)(z - (double)zh),
+                        __int_as_float((int)s.type[k]));
 }
 
 // ---------------------------------------------------------------- setvar
@@ -579,11 +596,131 @@ __device__ __forceinline__ void pair32(const FFScalars& ff, const Smem& s, int i
     hb.add(A * r6i * r6i - pr.z * r6i * r2i * r2i);
 }
 
-// Pair sums of the threads [0, nthr): vdW chunks (8 partners each) and 1-4
-// pairs, both from the mklist lists.
-template <bool F32>
+// FP64 term of a clashing pair, out of line: it is rare, and keeping it out
+// of the FP32 loop keeps that loop's registers free.
+__device__ __noinline__ void pair_term_clash(const FFScalars& ff, const Smem& s, int i, int j,
+                                             bool is14, double* acc) {
+  pair_term<false>(ff, s, i, j, is14, acc[0], acc[1], acc[2]);
+}
+
+// One FP32 pair term of the row loop: t = {Coulomb, 12-6, 12-10} for pair
+// (i, j), zero unless `use`; a clashing pair (closer than its guard) goes
+// to the FP64 sums a64 instead.  j must be a valid atom even when !use.
+template <bool TOTAL>
+__device__ __forceinline__ void row_term(const FFScalars& ff, const Smem& s, int i, int j,
+                                         bool use, bool is14, const float4& pi, const float4& li,
+                                         float qi, const float4* trow, double* a64, float* t) {
+  const float4 pj = s.p4[j], lj = s.l4[j];
+  const float dx = (pj.x - pi.x) + (lj.x - li.x);
+  const float dy = (pj.y - pi.y) + (lj.y - li.y);
+  const float dz = (pj.z - pi.z) + (lj.z - li.z);
+  const float r2 = dx * dx + dy * dy + dz * dz;
+  const float4 pr = trow[__float_as_int(lj.w)];
+  const bool clash = r2 < fabsf(pr.w);
+  if (use && clash) pair_term_clash(ff, s, i, j, is14, a64);
+  const float ri = rsqrtf(r2);
+  const float r2i = ri * ri;
+  const float r6i = r2i * r2i * r2i;
+  const bool ishb = pr.w < 0.f;
+  const float rc = ishb ? r6i * r2i * r2i : r6i;
+  const float elj = (is14 ? pr.y : pr.x) * r6i * r6i - pr.z * rc;
+  const bool keep = use && !clash;
+  t[0] = keep ? qi * pj.w * ri : 0.f;
+  if (TOTAL) {
+    t[1] = keep ? elj : 0.f;
+  } else {
+    t[1] = keep && !ishb ? elj : 0.f;
+    t[2] = keep && ishb ? elj : 0.f;
+  }
+}
+
+// Pair sums by rows, for molecules whose pair set has the row form (m.rows):
+// warp w of the warps [0, nw) takes rows i = w, w+nw, ...; in one pass over a
+// row, lane l takes partner j = j0 + l, so the 32 partners of a pass are
+// consecutive atoms (one conflict-free float4 load each) and atom i's data
+// stays in registers.  The first two passes read the near-window masks of
+// row i; every later partner is a normal pair.  With TOTAL the three sums
+// are returned added together in `el` (the sweep's proposals need only the
+// total).
+template <bool F32, bool TOTAL>
+__device__ void pair_rows(const FFScalars& ff, const DMol& m, const Smem& s, int nw, double& el,
+                          double& vw, double& hb) {
+  const int lane = threadIdx.x & 31, n = m.natoms;
+  if (!F32 || ff.epsd) {
+    for (int i = (threadIdx.x >> 5); i < n - 1; i += nw) {
+      const unsigned long long nm = m.near_mask[i], n14 = m.near14[i];
+      for (int j0 = i + 1; j0 < n; j0 += 32) {
+        const int j = j0 + lane, d = j0 - i - 1;
+        bool use = j < n, is14 = false;
+        if (d < 64) {
+          const uint32_t bn = (uint32_t)(nm >> d), b14 = (uint32_t)(n14 >> d);
+          use = use && (((bn | b14) >> lane) & 1u);
+          is14 = ((b14 >> lane) & 1u) != 0;
+        }
+        if (use) pair_term<false>(ff, s, i, j, is14, el, vw, hb);
+      }
+    }
+    if (TOTAL) {
+      el = (el + vw) + hb;
+      vw = hb = 0.0;
+    }
+    return;
+  }
+  KSum ke, kv, kh;
+  double a64[3] = {0.0, 0.0, 0.0};
+  const float convf = (float)ff.conv;
+  auto add = [&](const float (&t)[3]) {
+    if (TOTAL) {
+      ke.add(t[0] + t[1]);
+    } else {
+      ke.add(t[0]);
+      kv.add(t[1]);
+      kh.add(t[2]);
+    }
+  };
+  for (int i = (threadIdx.x >> 5); i < n - 1; i += nw) {
+    const float4 pi = s.p4[i], li = s.l4[i];
+    const float qi = convf * pi.w;
+    const float4* trow = s.tab4 + __float_as_int(li.w) * kTypes;
+    float t[3];
+    {   // partners i+1 .. i+64: the near-window masks
+      const unsigned long long nm = m.near_mask[i], n14 = m.near14[i];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int j = i + 1 + 32 * h + lane;
+        const uint32_t bn = (uint32_t)(nm >> (32 * h)), b14 = (uint32_t)(n14 >> (32 * h));
+        const bool use = j < n && (((bn | b14) >> lane) & 1u);
+        const bool is14 = ((b14 >> lane) & 1u) != 0;
+        row_term<TOTAL>(ff, s, i, use ? j : i + 1, use, is14, pi, li, qi, trow, a64, t);
+        add(t);
+      }
+    }
+    // every later partner is a normal pair
+    for (int j = i + 65 + lane; j < n + lane; j += 32) {
+      const bool use = j < n;
+      row_term<TOTAL>(ff, s, i, use ? j : i + 1, use, false, pi, li, qi, trow, a64, t);
+      add(t);
+    }
+  }
+  if (TOTAL) {
+    el += ((ke.value() + a64[0]) + a64[1]) + a64[2];
+  } else {
+    el += ke.value() + a64[0];
+    vw += kv.value() + a64[1];
+    hb += kh.value() + a64[2];
+  }
+}
+
+// Pair sums of the threads [0, nthr): by rows when the molecule has the row
+// form (kernels built with ROWS), else vdW chunks (8 partners each) and 1-4
+// pairs from the mklist lists.
+template <bool F32, bool ROWS>
 __device__ void pair_energy(const FFScalars& ff, const DMol& m, const Smem& s, int tid, int nthr,
                             double& el, double& vw, double& hb) {
+  if (ROWS && m.rows) {
+    pair_rows<F32, false>(ff, m, s, nthr >> 5, el, vw, hb);
+    return;
+  }
   const int nwork = m.nchunks * 8;
   if (!F32) {
     for (int t = tid; t < nwork; t += nthr) {
@@ -599,7 +736,7 @@ __device__ void pair_energy(const FFScalars& ff, const DMol& m, const Smem& s, i
     return;
   }
   if (ff.epsd) {   // sigmoidal dielectric: FP64 terms
-    pair_energy<false>(ff, m, s, tid, nthr, el, vw, hb);
+    pair_energy<false, ROWS>(ff, m, s, tid, nthr, el, vw, hb);
     return;
   }
   KSum ke, kv, kh;
@@ -635,26 +772,37 @@ __device__ void pair_energy(const FFScalars& ff, const DMol& m, const Smem& s, i
 // exposed-point counts are those of the reference arithmetic.  Warps
 // [w0, w0+nw) take one heavy atom at a time; returns this thread's share of
 // eysl.
+// Cheap pre-test with a margin for "heavy atom j may be a neighbour of i";
+// sasa_exact decides.
+__device__ __forceinline__ bool sasa_near(const DMol& m, const Smem& s, int j, double trad,
+                                          double xi, double yi, double zi) {
+  double ex = xi - s.x[j], ey = yi - s.y[j], ez = zi - s.z[j];
+  double lim = trad + m.rvdw[j];
+  return ex * ex + ey * ey + ez * ez <= lim * lim * 1.0000001 + 1e-12;
+}
+
 // Is heavy atom j a neighbour of atom i (enysol.f:232-250: the spheres of
 // radius rvdw overlap), and its offset / squared radius in units of trad.
-__device__ __forceinline__ bool sasa_neighbour(const DMol& m, const Smem& s, int i, int j,
-                                               double trad, double xi, double yi, double zi,
-                                               double& dx, double& dy, double& dz, double& rb2) {
-  if (j == i) return false;
+__device__ __forceinline__ bool sasa_exact(const DMol& m, const Smem& s, int j, double trad,
+                                           double xi, double yi, double zi, double& dx,
+                                           double& dy, double& dz, double& rb2) {
   double rj = m.rvdw[j];
-  double ex = xi - s.x[j], ey = yi - s.y[j], ez = zi - s.z[j];
-  double lim = trad + rj;
-  // cheap pre-test with margin; the exact test below decides
-  if (ex * ex + ey * ey + ez * ez > lim * lim * 1.0000001 + 1e-12) return false;
-  dx = __ddiv_rn(ex, trad);
-  dy = __ddiv_rn(ey, trad);
-  dz = __ddiv_rn(ez, trad);
+  dx = __ddiv_rn(xi - s.x[j], trad);
+  dy = __ddiv_rn(yi - s.y[j], trad);
+  dz = __ddiv_rn(zi - s.z[j], trad);
   double dd = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
   double akrad = __ddiv_rn(rj, trad);
   double dr = __dadd_rn(1.0, akrad);
   dr = __dmul_rn(dr, dr);
   rb2 = __dmul_rn(akrad, akrad);
   return dd <= dr;
+}
+
+__device__ __forceinline__ bool sasa_neighbour(const DMol& m, const Smem& s, int i, int j,
+                                               double trad, double xi, double yi, double zi,
+                                               double& dx, double& dy, double& dz, double& rb2) {
+  return j != i && sasa_near(m, s, j, trad, xi, yi, zi) &&
+         sasa_exact(m, s, j, trad, xi, yi, zi, dx, dy, dz, rb2);
 }
 
 // Is the surface point (s0, s1, s2) inside the neighbour sphere (enysol.f:267-275).
@@ -665,46 +813,97 @@ __device__ __forceinline__ bool sasa_buried(double s0, double s1, double s2, dou
   return sdd <= rb2;
 }
 
+constexpr float kSasaMargin = 1e-4f;
+
 __device__ double sasa_energy(const FFScalars& ff, const DMol& m, Smem& s, int w0, int nw,
                               int* err) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  double* nb = s.nb + (size_t)warp * kMaxNeighbours * 4;
+  float4* nbf = s.nbf + (size_t)warp * kMaxNeighbours;
+  int* nbj = s.nbj + (size_t)warp * kMaxNeighbours;
+  int* q = s.sq + warp * kSasaQueue;
   double eysl = 0.0;
   const int npnt = ff.npnt;
   for (int h = warp - w0; h < m.nheavy; h += nw) {
     int i = m.heavy[h];
     double trad = m.rvdw[i];
     double xi = s.x[i], yi = s.y[i], zi = s.z[i];
-    int nn = 0;
-    for (int base = 0; base < m.nheavy; base += 32) {
-      int hj = base + lane;
+    // Candidates that pass the cheap pre-test are queued, and the exact
+    // test (four FP64 divisions) runs on full warps of queued candidates.
+    int nn = 0, nq = 0;
+    auto exact32 = [&](int cnt) {
+      const int j = lane < cnt ? q[lane] : 0;
       double dx = 0, dy = 0, dz = 0, rb2 = 0;
-      bool take = hj < m.nheavy &&
-                  sasa_neighbour(m, s, i, m.heavy[hj], trad, xi, yi, zi, dx, dy, dz, rb2);
-      unsigned mask = __ballot_sync(0xffffffffu, take);
-      int pos = nn + __popc(mask & ((1u << lane) - 1u));
+      const bool take = lane < cnt && sasa_exact(m, s, j, trad, xi, yi, zi, dx, dy, dz, rb2);
+      const unsigned mask = __ballot_sync(0xffffffffu, take);
+      const int pos = nn + __popc(mask & ((1u << lane) - 1u));
       if (take && pos < kMaxNeighbours) {
-        nb[4 * pos] = dx;
-        nb[4 * pos + 1] = dy;
-        nb[4 * pos + 2] = dz;
-        nb[4 * pos + 3] = rb2;
+        nbf[pos] = make_float4((float)dx, (float)dy, (float)dz, (float)rb2);
+        nbj[pos] = j;
       }
       nn += __popc(mask);
+    };
+    for (int base = 0; base < m.nheavy; base += 32) {
+      const int hj = base + lane;
+      const int j = hj < m.nheavy ? m.heavy[hj] : i;
+      const bool cand = j != i && sasa_near(m, s, j, trad, xi, yi, zi);
+      const unsigned mask = __ballot_sync(0xffffffffu, cand);
+      if (cand) q[nq + __popc(mask & ((1u << lane) - 1u))] = j;   // nq < 32: fits
+      nq += __popc(mask);
+      __syncwarp();
+      if (nq >= 32) {
+        exact32(32);
+        const int rest = nq - 32;
+        const int v = lane < rest ? q[32 + lane] : 0;
+        __syncwarp();
+        if (lane < rest) q[lane] = v;
+        __syncwarp();
+        nq = rest;
+      }
     }
+    if (nq > 0) exact32(nq);
     __syncwarp();
     int cnt = 0;
     if (nn <= kMaxNeighbours) {
-      for (int p = lane; p < npnt; p += 32) {
-        double s0 = s.spt[3 * p], s1 = s.spt[3 * p + 1], s2 = s.spt[3 * p + 2];
-        bool exposed = true;
-        for (int k = 0; k < nn; ++k) {
-          if (sasa_buried(s0, s1, s2, nb[4 * k], nb[4 * k + 1], nb[4 * k + 2], nb[4 * k + 3])) {
-            exposed = false;
-            break;
+      // FP32 test with a margin; a point within the margin of a sphere is
+      // re-tested in FP64 with the reference's arithmetic.  With neighbour
+      // offsets below 3 radii (radii within a factor 2, checked on the
+      // host) and unit points, the FP32 error of sdd is below 2e-5.  Each
+      // lane takes its (up to) four points through the neighbour list
+      // together, so the four tests are independent work.
+      constexpr int R = 4;   // points per lane: npnt <= 128
+      float f[R][3];
+      unsigned buried = 0, valid = 0;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int p = lane + 32 * r;
+        const bool ok = p < npnt;
+        valid |= ok ? (1u << r) : 0u;
+        f[r][0] = ok ? (float)s.spt[3 * p] : 0.f;
+        f[r][1] = ok ? (float)s.spt[3 * p + 1] : 0.f;
+        f[r][2] = ok ? (float)s.spt[3 * p + 2] : 0.f;
+      }
+      unsigned done = ~valid & 0xfu;
+      for (int k = 0; k < nn && done != 0xfu; ++k) {
+        const float4 c = nbf[k];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          if (done & (1u << r)) continue;
+          const float t0 = c.x + f[r][0], t1 = c.y + f[r][1], t2 = c.z + f[r][2];
+          const float sdd = t0 * t0 + t1 * t1 + t2 * t2;
+          bool b = sdd < c.w - kSasaMargin;
+          if (!b && sdd <= c.w + kSasaMargin) {
+            const int p = lane + 32 * r;
+            double dx, dy, dz, rb2;
+            sasa_exact(m, s, nbj[k], trad, xi, yi, zi, dx, dy, dz, rb2);
+            b = sasa_buried(s.spt[3 * p], s.spt[3 * p + 1], s.spt[3 * p + 2], dx, dy, dz, rb2);
+          }
+          if (b) {
+            buried |= 1u << r;
+            done |= 1u << r;
           }
         }
-        cnt += exposed;
       }
+      cnt = __popc(valid & ~buried);
     } else {
       // More neighbours than the buffer holds (crowded, clashing
       // conformations): test each point against every heavy atom directly,
@@ -769,12 +968,12 @@ __device__ __forceinline__ double total_of(const double* sum) {
 
 // Full evaluation of the current coordinates by the whole block; partials in
 // s.red (read them with all_sums after a barrier).
-template <bool F32>
+template <bool F32, bool ROWS, bool SASA>
 __device__ void evaluate_block(const FFScalars& ff, const DMol& m, Smem& s, int* err) {
   double el = 0.0, vw = 0.0, hb = 0.0, sl = 0.0, vr = 0.0;
-  pair_energy<F32>(ff, m, s, threadIdx.x, blockDim.x, el, vw, hb);
+  pair_energy<F32, ROWS>(ff, m, s, threadIdx.x, blockDim.x, el, vw, hb);
   for (int v = threadIdx.x; v < m.nvar; v += blockDim.x) vr += s.et[v];
-  if (ff.itysol > 0) sl = sasa_energy(ff, m, s, 0, kWarps, err);
+  if (SASA) sl = sasa_energy(ff, m, s, 0, kWarps, err);
   warp_partials(s, el, vw, hb, vr, sl);
 }
 
@@ -903,10 +1102,10 @@ __global__ void k_random_start(DMolSet set, DChains ch, const int* order, int n)
 // energy(): setvar + rebuild + energy for chains [first, first+gridDim.x).
 // The dihedral state is updated in place exactly as the reference's energy()
 // does; terms and eol of each chain receive the result.
-template <bool F32>
+template <bool F32, bool ROWS, bool SASA>
 __global__ void __launch_bounds__(kThreads, 1) k_energy(DMolSet set, DChains ch, int first) {
   int c = first + blockIdx.x;
-  const bool sasa = set.f.itysol > 0;
+  const bool sasa = SASA;
   Smem s = carve(set, sasa);
   const DMol& m = stage_mol(set, ch, c, s);
   load_static(*set.ff, m, s, sasa);
@@ -916,7 +1115,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_energy(DMolSet set, DChains ch,
   __syncthreads();
   torsion_all(m, s);
   full_rebuild(m, s);
-  evaluate_block<F32>(set.f, m, s, &ch.err[c]);
+  evaluate_block<F32, ROWS, SASA>(set.f, m, s, &ch.err[c]);
   __syncthreads();
   double sum[5];
   all_sums(s, sum);
@@ -943,11 +1142,14 @@ __device__ __forceinline__ int moved_atom(int t, int lo, int span, bool flip) {
   return flip ? (t < lo ? t : t + span) : lo + t;
 }
 
-template <bool F32>
+// Kernels are built per (F32, ROWS, SASA): a launch whose molecules have no
+// row form, or that runs without solvation, carries none of that code (and
+// none of its registers).
+template <bool F32, bool ROWS, bool SASA>
 __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, DWeight w, int first,
                                                        int nsweeps, int flags, double check_tol) {
   const int c = first + blockIdx.x;
-  const bool sasa = set.f.itysol > 0;
+  const bool sasa = SASA;
   const bool rndord = (flags & kFlagRndOrd) != 0;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int spec_warp = kWarps - 1;            // setvar replay + next proposal
@@ -989,7 +1191,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
     if (!fresh) {
       torsion_all(m, s);
       full_rebuild(m, s);
-      evaluate_block<F32>(set.f, m, s, err);
+      evaluate_block<F32, ROWS, SASA>(set.f, m, s, err);
       __syncthreads();
       double sum[5];
       all_sums(s, sum);
@@ -1044,7 +1246,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       // setvar call on the dihedral state and prepares proposal p+1
       if (warp != spec_warp) {
         double el = 0.0, vw = 0.0, hb = 0.0, sl = 0.0;
-        pair_energy<F32>(set.f, m, s, threadIdx.x, nthr_pairs, el, vw, hb);
+        if (ROWS && m.rows)
+          pair_rows<F32, true>(set.f, m, s, kWarps - 1, el, vw, hb);
+        else
+          pair_energy<F32, false>(set.f, m, s, threadIdx.x, nthr_pairs, el, vw, hb);
         if (sasa) sl = sasa_energy(set.f, m, s, 0, kWarps - 1, err);
         double v = ((el + vw) + hb) + sl;
 #pragma unroll
@@ -1123,7 +1328,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
     __syncthreads();
     torsion_all(m, s);
     full_rebuild(m, s);
-    evaluate_block<F32>(set.f, m, s, err);
+    evaluate_block<F32, ROWS, SASA>(set.f, m, s, err);
     __syncthreads();
     {
       double sum[5];
@@ -1198,7 +1403,8 @@ size_t sweep_smem_bytes(const DMolSet& set) {
 }
 
 size_t stage_bytes_of(const DMol& d, bool lists) {
-  return stage_size(d.natoms, d.nvar, d.nsib, d.nlevels, d.nfree, d.nchunks, d.n14, d.nheavy, lists);
+  return stage_size(d.natoms, d.nvar, d.nsib, d.nlevels, d.nfree, d.nchunks, d.n14, d.nheavy,
+                    d.rows != 0, lists);
 }
 
 cudaError_t launch_seed(uint32_t* mt, const int* seeds, int nslots, cudaStream_t st) {
@@ -1220,47 +1426,75 @@ cudaError_t launch_random_start(const DMolSet& set, const DChains& ch, const int
 // Raise a kernel's dynamic shared-memory limit once per size, so that the
 // launches captured into CUDA graphs make no attribute calls.
 static cudaError_t prep_smem(const void* fn, size_t bytes) {
-  static const void* fns[8] = {nullptr};
-  static size_t done[8] = {0};
+  constexpr int kSlots = 32;
+  static const void* fns[kSlots] = {nullptr};
+  static size_t done[kSlots] = {0};
   int k = 0;
-  while (k < 8 && fns[k] && fns[k] != fn) ++k;
-  if (k < 8 && fns[k] == fn && done[k] >= bytes) return cudaSuccess;
+  while (k < kSlots && fns[k] && fns[k] != fn) ++k;
+  if (k < kSlots && fns[k] == fn && done[k] >= bytes) return cudaSuccess;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  if (e == cudaSuccess && k < 8) {
+  if (e == cudaSuccess && k < kSlots) {
     fns[k] = fn;
     done[k] = bytes;
   }
   return e;
 }
 
+template <bool F32, bool ROWS, bool SASA>
+static cudaError_t launch_energy_t(const DMolSet& set, const DChains& ch, int first, int count,
+                                   size_t sm, cudaStream_t st) {
+  cudaError_t e = prep_smem((const void*)k_energy<F32, ROWS, SASA>, sm);
+  if (e != cudaSuccess || count <= 0) return e;
+  k_energy<F32, ROWS, SASA><<<count, kThreads, sm, st>>>(set, ch, first);
+  return cudaGetLastError();
+}
+
+template <bool F32, bool ROWS, bool SASA>
+static cudaError_t launch_sweep_t(const DMolSet& set, const DChains& ch, const DWeight& w,
+                                  int first, int count, int nsweeps, int flags, double check_tol,
+                                  size_t sm, cudaStream_t st) {
+  cudaError_t e = prep_smem((const void*)k_sweep<F32, ROWS, SASA>, sm);
+  if (e != cudaSuccess || count <= 0) return e;
+  k_sweep<F32, ROWS, SASA><<<count, kThreads, sm, st>>>(set, ch, w, first, nsweeps, flags,
+                                                        check_tol);
+  return cudaGetLastError();
+}
+
+static int variant(const DMolSet& set, bool fp32) {
+  return (fp32 ? 4 : 0) | (set.any_rows ? 2 : 0) | (set.f.itysol > 0 ? 1 : 0);
+}
+
 cudaError_t launch_energy(const DMolSet& set, const DChains& ch, int first, int count, bool fp32,
                           cudaStream_t st) {
-  size_t sm = sweep_smem_bytes(set);
-  if (fp32) {
-    cudaError_t e = prep_smem((const void*)k_energy<true>, sm);
-    if (e != cudaSuccess || count <= 0) return e;
-    k_energy<true><<<count, kThreads, sm, st>>>(set, ch, first);
-  } else {
-    cudaError_t e = prep_smem((const void*)k_energy<false>, sm);
-    if (e != cudaSuccess || count <= 0) return e;
-    k_energy<false><<<count, kThreads, sm, st>>>(set, ch, first);
+  const size_t sm = sweep_smem_bytes(set);
+  switch (variant(set, fp32)) {
+    case 0: return launch_energy_t<false, false, false>(set, ch, first, count, sm, st);
+    case 1: return launch_energy_t<false, false, true>(set, ch, first, count, sm, st);
+    case 2: return launch_energy_t<false, true, false>(set, ch, first, count, sm, st);
+    case 3: return launch_energy_t<false, true, true>(set, ch, first, count, sm, st);
+    case 4: return launch_energy_t<true, false, false>(set, ch, first, count, sm, st);
+    case 5: return launch_energy_t<true, false, true>(set, ch, first, count, sm, st);
+    case 6: return launch_energy_t<true, true, false>(set, ch, first, count, sm, st);
+    default: return launch_energy_t<true, true, true>(set, ch, first, count, sm, st);
   }
-  return cudaGetLastError();
 }
 
 cudaError_t launch_sweep(const DMolSet& set, const DChains& ch, const DWeight& w, int first,
                          int count, int nsweeps, int flags, double check_tol, cudaStream_t st) {
-  size_t sm = sweep_smem_bytes(set);
-  if (flags & kFlagFP32) {
-    cudaError_t e = prep_smem((const void*)k_sweep<true>, sm);
-    if (e != cudaSuccess || count <= 0) return e;
-    k_sweep<true><<<count, kThreads, sm, st>>>(set, ch, w, first, nsweeps, flags, check_tol);
-  } else {
-    cudaError_t e = prep_smem((const void*)k_sweep<false>, sm);
-    if (e != cudaSuccess || count <= 0) return e;
-    k_sweep<false><<<count, kThreads, sm, st>>>(set, ch, w, first, nsweeps, flags, check_tol);
+  const size_t sm = sweep_smem_bytes(set);
+#define SMMP_SWEEP(a, b, c) \
+  launch_sweep_t<a, b, c>(set, ch, w, first, count, nsweeps, flags, check_tol, sm, st)
+  switch (variant(set, (flags & kFlagFP32) != 0)) {
+    case 0: return SMMP_SWEEP(false, false, false);
+    case 1: return SMMP_SWEEP(false, false, true);
+    case 2: return SMMP_SWEEP(false, true, false);
+    case 3: return SMMP_SWEEP(false, true, true);
+    case 4: return SMMP_SWEEP(true, false, false);
+    case 5: return SMMP_SWEEP(true, false, true);
+    case 6: return SMMP_SWEEP(true, true, false);
+    default: return SMMP_SWEEP(true, true, true);
   }
-  return cudaGetLastError();
+#undef SMMP_SWEEP
 }
 
 cudaError_t launch_exchange(const DChains& ch, int* temp_chain, const double* betas, int n,

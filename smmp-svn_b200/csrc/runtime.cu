@@ -90,6 +90,20 @@ DeviceSet::DeviceSet(const std::vector<std::shared_ptr<Molecule>>& mols) {
     const MolTopo& t = mp->topo;
     if (mp->ff.itysol != ff.itysol || mp->ff.epsd != ff.epsd)
       throw std::runtime_error("DeviceSet: molecules of one ensemble must share the force field");
+    if (ff.itysol > 0 && ff.npnt > 128)
+      throw std::runtime_error("DeviceSet: the SASA kernel takes at most 128 sphere points");
+    if (ff.itysol > 0 && !t.heavy.empty()) {
+      // The SASA kernel tests surface points in FP32 with a 1e-4 margin; that
+      // bounds the FP32 error while neighbour offsets stay below 3 radii,
+      // i.e. while no radius exceeds twice another.
+      double lo = 1e300, hi = 0.0;
+      for (int k : t.heavy) {
+        lo = std::min(lo, t.rvdw[k]);
+        hi = std::max(hi, t.rvdw[k]);
+      }
+      if (hi > 2.0 * lo)
+        throw std::runtime_error("DeviceSet: SASA radii differ by more than a factor of 2");
+    }
     DMol d{};
     d.natoms = t.natoms;
     d.nvar = t.nvar;
@@ -136,9 +150,10 @@ DeviceSet::DeviceSet(const std::vector<std::shared_ptr<Molecule>>& mols) {
       d.near_mask = upload(nm);
       d.near14 = upload(n14);
     }
-    d.tiles = upload(t.tiles);
-    d.tile_off = upload(t.tile_off);
-    d.ntiles = (int)t.tiles.size();
+    // Row-form pair sums pay off from about a hundred atoms on; smaller
+    // molecules keep the chunk lists (measured: Met-enkephalin, 75 atoms,
+    // is faster with lists; Ace-Ala40-NMe, 412 atoms, with rows).
+    d.rows = (t.rows_ok && t.natoms >= 128) ? 1 : 0;
     dm.push_back(d);
     max_atoms = std::max(max_atoms, t.natoms);
     max_vars = std::max(max_vars, t.nvar);
@@ -151,6 +166,8 @@ DeviceSet::DeviceSet(const std::vector<std::shared_ptr<Molecule>>& mols) {
   set_.max_vars = max_vars;
   set_.ff = dff;
   set_.f = FFScalars{ff.conv, ff.plt, ff.slp, ff.epsd, ff.itysol, ff.npnt};
+  set_.any_rows = 0;
+  for (const DMol& d : dm) set_.any_rows |= d.rows;
   // stage the pair lists too when the largest molecule's copy fits
   const size_t budget = 200 * 1024;
   size_t with_lists = 0, without = 0;

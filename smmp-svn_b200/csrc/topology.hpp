@@ -70,14 +70,13 @@ struct MolTopo {
   std::vector<uint32_t> chunks;        // i | j0<<14 | (len-1)<<28
   std::vector<uint32_t> pairs14;       // i | j<<14
   long long npairs = 0;                // pair terms per full evaluation
-  // The same pair set as a dense upper triangle: for atom i, bit k of
-  // near_mask[i] / near14[i] marks pair (i, i+1+k) as a normal / 1-4 pair;
-  // every pair more than kNearWindow apart is a normal pair (checked).  The
-  // triangle is cut into 32x32 tiles (tiles[t] = bi | bj<<16, bi <= bj);
-  // tile_off[t] is the first work item of tile t, one item per j column.
+  // The same pair set by rows: for atom i, bit k of near_mask[i] / near14[i]
+  // marks pair (i, i+1+k) as a normal / 1-4 pair.  rows_ok is set when every
+  // pair more than kNearWindow apart is a normal pair and no pair is listed
+  // twice (checked), so row i is the two masked 32-atom windows after i and
+  // then every later atom.
   std::vector<uint64_t> near_mask, near14;
-  std::vector<uint32_t> tiles;
-  std::vector<int> tile_off;
+  bool rows_ok = false;
   // solvation
   std::vector<int> heavy;              // atoms with rvdw > 0
   int nres = 0;
