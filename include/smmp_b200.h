@@ -196,6 +196,34 @@ int smmp_ens_draw(smmp_ens_t* e, int slot, int n, double* out);
 int smmp_ens_checkpoint(smmp_ens_t* e, void* buf, uint64_t* bytes);
 int smmp_ens_restore(smmp_ens_t* e, const void* buf, uint64_t bytes);
 
+/* ---------------------------------------------------------------- surrogate
+ * Learned energy surrogate (no counterpart in the reference): an MLP on the
+ * sin/cos of the nang free dihedrals, 3 hidden layers of 256 with SiLU, BF16
+ * weights and FP32 accumulation, trained on the GPU by the library's own
+ * tensor-core forward/backward kernels with Adam.  Angles are [n*nang]
+ * radians (FP64, row-major), energies kcal/mol. */
+typedef struct smmp_sur smmp_sur_t;
+smmp_sur_t* smmp_sur_create(int nang, uint64_t seed);
+void smmp_sur_free(smmp_sur_t* s);
+/* nin = 2*nang inputs, padded to nin_pad; nparams FP32 parameters in the
+ * order W1[nin_pad][256] b1 W2[256][256] b2 W3[256][256] b3 w4[256] b4. */
+int smmp_sur_sizes(smmp_sur_t* s, int* nin, int* nin_pad, int64_t* nparams);
+/* Training set; energies above clip are clipped, targets normalised by the
+ * set's mean and standard deviation (kept as {mu, sigma}). */
+int smmp_sur_set_data(smmp_sur_t* s, const double* ang, const double* energy, int n, double clip);
+/* epochs of minibatch Adam; *loss = mean squared error of the last epoch in
+ * normalised units. */
+int smmp_sur_train(smmp_sur_t* s, int epochs, int batch, double lr, uint64_t shuffle_seed,
+                   double* loss);
+int smmp_sur_predict(smmp_sur_t* s, const double* ang, int n, double* energy_out);
+/* Gradient of the batch's mean squared error (normalised units) with respect
+ * to every parameter, without an update. */
+int smmp_sur_gradients(smmp_sur_t* s, const double* ang, const double* energy, int n,
+                       float* grad_out, double* loss);
+/* Parameters and normalisation norm[2] = {mu, sigma}. */
+int smmp_sur_get_params(smmp_sur_t* s, float* params, float* norm);
+int smmp_sur_set_params(smmp_sur_t* s, const float* params, const float* norm);
+
 #ifdef __cplusplus
 }
 #endif

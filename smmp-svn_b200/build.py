@@ -24,7 +24,7 @@ NVFLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
 # host assembly code keeps the reference's separately rounded FP64 arithmetic
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I" + SRC, "-I" + INCLUDE]
 
-CUDA_SOURCES = ["kernels.cu", "runtime.cu", "capi.cu"]
+CUDA_SOURCES = ["kernels.cu", "runtime.cu", "capi.cu", "surrogate.cu"]
 CXX_SOURCES = ["assembly_setup.cpp", "assembly_build.cpp", "topology.cpp"]
 
 

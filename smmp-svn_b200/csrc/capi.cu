@@ -10,6 +10,7 @@
 
 #include "../../include/smmp_b200.h"
 #include "runtime.hpp"
+#include "surrogate.hpp"
 
 using namespace smmpb200;
 
@@ -845,6 +846,92 @@ int smmp_ens_restore(smmp_ens_t* e, const void* buf, uint64_t bytes) {
       en.pt_set_state(tc, (int)h.iswitch, ptmt, ptb);
     }
     (void)eo;
+  });
+}
+
+}  // extern "C"
+
+// ============================================================================ surrogate
+
+struct smmp_sur {
+  std::unique_ptr<Surrogate> s;
+};
+
+extern "C" {
+
+smmp_sur_t* smmp_sur_create(int nang, uint64_t seed) {
+  smmp_sur_t* out = nullptr;
+  int rc = guard([&] {
+    need(nang > 0, "smmp_sur_create: nang must be positive");
+    auto h = std::make_unique<smmp_sur>();
+    h->s.reset(new Surrogate(nang, seed));
+    out = h.release();
+  });
+  return rc == SMMP_OK ? out : nullptr;
+}
+
+void smmp_sur_free(smmp_sur_t* s) { delete s; }
+
+int smmp_sur_sizes(smmp_sur_t* s, int* nin, int* nin_pad, int64_t* nparams) {
+  return guard([&] {
+    need(s != nullptr, "null surrogate");
+    if (nin) *nin = s->s->layout().nin;
+    if (nin_pad) *nin_pad = s->s->layout().nin_pad;
+    if (nparams) *nparams = (int64_t)s->s->layout().n;
+  });
+}
+
+int smmp_sur_set_data(smmp_sur_t* s, const double* ang, const double* energy, int n, double clip) {
+  return guard([&] {
+    need(s && ang && energy && n > 0, "smmp_sur_set_data: bad arguments");
+    s->s->set_data(ang, energy, n, clip);
+  });
+}
+
+int smmp_sur_train(smmp_sur_t* s, int epochs, int batch, double lr, uint64_t shuffle_seed,
+                   double* loss) {
+  return guard([&] {
+    need(s != nullptr, "null surrogate");
+    double l = s->s->train(epochs, batch, lr, shuffle_seed);
+    if (loss) *loss = l;
+  });
+}
+
+int smmp_sur_predict(smmp_sur_t* s, const double* ang, int n, double* energy_out) {
+  return guard([&] {
+    need(s && ang && energy_out && n >= 0, "smmp_sur_predict: bad arguments");
+    if (n > 0) s->s->predict(ang, n, energy_out);
+  });
+}
+
+int smmp_sur_gradients(smmp_sur_t* s, const double* ang, const double* energy, int n,
+                       float* grad_out, double* loss) {
+  return guard([&] {
+    need(s && ang && energy && grad_out && n > 0, "smmp_sur_gradients: bad arguments");
+    double l = s->s->gradients(ang, energy, n, grad_out);
+    if (loss) *loss = l;
+  });
+}
+
+int smmp_sur_get_params(smmp_sur_t* s, float* params, float* norm) {
+  return guard([&] {
+    need(s != nullptr, "null surrogate");
+    if (params) s->s->get_params(params);
+    if (norm) {
+      norm[0] = s->s->mu();
+      norm[1] = s->s->sigma();
+    }
+  });
+}
+
+int smmp_sur_set_params(smmp_sur_t* s, const float* params, const float* norm) {
+  return guard([&] {
+    need(s != nullptr, "null surrogate");
+    if (params) s->s->set_params(params);
+    if (norm) {
+      need(norm[1] > 0.f, "smmp_sur_set_params: sigma must be positive");
+      s->s->set_norm(norm[0], norm[1]);
+    }
   });
 }
 

@@ -82,6 +82,16 @@ _SIGS = {
     "smmp_ens_draw": (c_int, [c_void_p, c_int, c_int, P(c_double)]),
     "smmp_ens_checkpoint": (c_int, [c_void_p, c_void_p, P(ctypes.c_uint64)]),
     "smmp_ens_restore": (c_int, [c_void_p, c_void_p, ctypes.c_uint64]),
+    "smmp_sur_create": (c_void_p, [c_int, ctypes.c_uint64]),
+    "smmp_sur_free": (None, [c_void_p]),
+    "smmp_sur_sizes": (c_int, [c_void_p, P(c_int), P(c_int), P(ctypes.c_int64)]),
+    "smmp_sur_set_data": (c_int, [c_void_p, P(c_double), P(c_double), c_int, c_double]),
+    "smmp_sur_train": (c_int, [c_void_p, c_int, c_int, c_double, ctypes.c_uint64, P(c_double)]),
+    "smmp_sur_predict": (c_int, [c_void_p, P(c_double), c_int, P(c_double)]),
+    "smmp_sur_gradients": (c_int, [c_void_p, P(c_double), P(c_double), c_int,
+                                   P(ctypes.c_float), P(c_double)]),
+    "smmp_sur_get_params": (c_int, [c_void_p, P(ctypes.c_float), P(ctypes.c_float)]),
+    "smmp_sur_set_params": (c_int, [c_void_p, P(ctypes.c_float), P(ctypes.c_float)]),
 }
 
 EXPORTED = sorted(_SIGS)
