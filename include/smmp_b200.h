@@ -220,6 +220,20 @@ int smmp_sur_predict(smmp_sur_t* s, const double* ang, int n, double* energy_out
  * to every parameter, without an update. */
 int smmp_sur_gradients(smmp_sur_t* s, const double* ang, const double* energy, int n,
                        float* grad_out, double* loss);
+/* The forward pass of smmp_sur_predict for callers that cannot allocate
+ * device memory when they need a prediction (a framework's caching allocator
+ * owns the memory budget, or allocation is forbidden in a real-time loop).
+ * No counterpart in the reference.  It allocates nothing: ang_dev
+ * ([n*nang] FP32 radians) and energy_dev ([n] FP64) are device pointers the
+ * caller owns, and the intermediate activations live in one fixed 16 MiB
+ * device array that every GPU loading the library holds until exit.  n above
+ * the rows that fit (3,563 for 24 dihedrals, 2,757 for 365) is
+ * rejected with SMMP_ERR_ARG.  The first call on a device looks up the
+ * array's device address; make it before any stream capture.  Calls share
+ * the array: calls that overlap on the GPU race. stream: a cudaStream_t or
+ * NULL (the default stream). */
+int smmp_sur_predict_noalloc(smmp_sur_t* s, const float* ang_dev, int n, double* energy_dev,
+                             void* stream);
 /* Parameters and normalisation norm[2] = {mu, sigma}. */
 int smmp_sur_get_params(smmp_sur_t* s, float* params, float* norm);
 int smmp_sur_set_params(smmp_sur_t* s, const float* params, const float* norm);

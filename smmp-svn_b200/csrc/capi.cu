@@ -924,6 +924,14 @@ int smmp_sur_get_params(smmp_sur_t* s, float* params, float* norm) {
   });
 }
 
+int smmp_sur_predict_noalloc(smmp_sur_t* s, const float* ang_dev, int n, double* energy_dev,
+                             void* stream) {
+  return guard([&] {
+    need(s && ang_dev && energy_dev && n >= 0, "smmp_sur_predict_noalloc: bad arguments");
+    s->s->predict_noalloc(ang_dev, n, energy_dev, static_cast<cudaStream_t>(stream));
+  });
+}
+
 int smmp_sur_set_params(smmp_sur_t* s, const float* params, const float* norm) {
   return guard([&] {
     need(s != nullptr, "null surrogate");

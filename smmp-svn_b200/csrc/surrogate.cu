@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <numeric>
 #include <random>
 #include <stdexcept>
@@ -516,6 +517,119 @@ DSurrogate Surrogate::device_view() const {
   d.mu = mu_;
   d.sigma = sigma_;
   return d;
+}
+
+// ============================================================================ no-alloc forward
+//
+// Some callers cannot allocate device memory at the point where they need a
+// prediction: code that runs while a framework's caching allocator owns the
+// device memory budget, a real-time loop whose allocations are forbidden, or
+// a host thread that must not take the driver's allocation locks.  For them,
+// predict_noalloc runs the same forward kernels as predict() on
+// device-resident inputs and outputs, with its intermediate activations in
+// the fixed array below instead of cudaMalloc'd buffers.
+//
+// * The array is kNoAllocScratchBytes (16 MiB) and lives on every GPU that
+//   loads the library until the process exits.  A call needs per row
+//   2*nin_pad + 18*256 + 4 bytes (plus 256-byte alignment per sub-buffer);
+//   noalloc_max_rows() gives the limit and larger n is rejected.
+// * Host code cannot pass the array's name to a kernel: on the host it names
+//   a host-side stand-in, not device memory.  The device address is looked up
+//   with cudaGetSymbolAddress once per device, on the first call made while
+//   that device is current; make that first call before any stream capture.
+// * Nothing in the array must start at zero: every scratch byte a call reads
+//   was written earlier in the same call.  Every call shares the one array
+//   and it keeps the last call's contents, so calls that overlap on the GPU
+//   (concurrent streams, or concurrent host threads) race; serialise them.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+
+__global__ void k_denorm(int n, const float* __restrict__ y, float mu, float sigma,
+                         double* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = (double)mu + (double)sigma * (double)y[i];
+}
+
+size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+// Scratch layout of one call: X | Z1 Z2 Z3 | H1 H2 H3 | y, each 256-aligned.
+struct NoAllocLayout {
+  size_t x, z1, z2, z3, h1, h2, h3, y, total;
+  NoAllocLayout(int n, int nin_pad) {
+    const size_t H = kHidden;
+    x = 0;
+    z1 = align256(x + (size_t)n * nin_pad * sizeof(bf16));
+    z2 = align256(z1 + (size_t)n * H * sizeof(float));
+    z3 = align256(z2 + (size_t)n * H * sizeof(float));
+    h1 = align256(z3 + (size_t)n * H * sizeof(float));
+    h2 = align256(h1 + (size_t)n * H * sizeof(bf16));
+    h3 = align256(h2 + (size_t)n * H * sizeof(bf16));
+    y = align256(h3 + (size_t)n * H * sizeof(bf16));
+    total = y + (size_t)n * sizeof(float);
+  }
+};
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+unsigned char* g_noalloc_ptr[kMaxDevices] = {nullptr};
+
+// Device address of the scratch array on the current device (looked up once
+// per device).
+unsigned char* noalloc_scratch() {
+  int dev = 0;
+  check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+  if (dev < 0 || dev >= kMaxDevices) throw std::runtime_error("predict_noalloc: device index");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    check_cuda(cudaGetSymbolAddress(&p, g_noalloc_scratch),
+               "cudaGetSymbolAddress (no-alloc scratch)");
+    g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+  }
+  return g_noalloc_ptr[dev];
+}
+
+}  // namespace
+
+int Surrogate::noalloc_max_rows(int nin_pad) {
+  int lo = 0, hi = 1 << 22;
+  while (lo < hi) {   // largest n whose layout fits
+    const int mid = lo + (hi - lo + 1) / 2;
+    if (NoAllocLayout(mid, nin_pad).total <= kNoAllocScratchBytes)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+void Surrogate::predict_noalloc(const float* ang_dev, int n, double* energy_dev,
+                                cudaStream_t st) const {
+  if (n <= 0) return;
+  const int maxn = noalloc_max_rows(L_.nin_pad);
+  if (n > maxn)
+    throw std::invalid_argument("smmp_sur_predict_noalloc: " + std::to_string(n) +
+                                " rows exceed the fixed scratch (at most " +
+                                std::to_string(maxn) + " rows for this network)");
+  unsigned char* base = noalloc_scratch();
+  const NoAllocLayout lay(n, L_.nin_pad);
+  bf16* X = reinterpret_cast<bf16*>(base + lay.x);
+  float* Z1 = reinterpret_cast<float*>(base + lay.z1);
+  float* Z2 = reinterpret_cast<float*>(base + lay.z2);
+  float* Z3 = reinterpret_cast<float*>(base + lay.z3);
+  bf16* H1 = reinterpret_cast<bf16*>(base + lay.h1);
+  bf16* H2 = reinterpret_cast<bf16*>(base + lay.h2);
+  bf16* H3 = reinterpret_cast<bf16*>(base + lay.h3);
+  float* y = reinterpret_cast<float*>(base + lay.y);
+  const int H = kHidden, K1 = L_.nin_pad;
+  k_features<<<n, 128, 0, st>>>(ang_dev, nullptr, n, nang_, K1, X);
+  gemm<0, 0, kEpiHidden>(st, n, H, K1, X, K1, Wb_ + wb1_, H, P_ + L_.b1, nullptr, Z1, H1, H);
+  gemm<0, 0, kEpiHidden>(st, n, H, H, H1, H, Wb_ + wb2_, H, P_ + L_.b2, nullptr, Z2, H2, H);
+  gemm<0, 0, kEpiHidden>(st, n, H, H, H2, H, Wb_ + wb3_, H, P_ + L_.b3, nullptr, Z3, H3, H);
+  k_out_fwd<<<(n + 7) / 8, 256, 0, st>>>(n, H3, Wb_ + wb4_, P_ + L_.b4, y);
+  k_denorm<<<(n + 255) / 256, 256, 0, st>>>(n, y, mu_, sigma_, energy_dev);
+  check_cuda(cudaGetLastError(), "predict_noalloc launch");
 }
 
 }  // namespace smmpb200

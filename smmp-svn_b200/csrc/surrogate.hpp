@@ -14,6 +14,9 @@
 namespace smmpb200 {
 
 constexpr int kHidden = 256;
+// Size of the fixed scratch array of Surrogate::predict_noalloc (held by
+// every GPU that loads the library, until the process exits).
+constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;
 
 // Offsets (in floats) of the parameters in the flat FP32 vector, for an
 // input width nin_pad (a multiple of 16):
@@ -67,6 +70,11 @@ class Surrogate {
   float mu() const { return mu_; }
   float sigma() const { return sigma_; }
   DSurrogate device_view() const;
+  // Forward pass that allocates nothing (for callers that cannot allocate
+  // device memory): device-resident inputs and outputs, scratch in a fixed
+  // file-scope device array (kNoAllocScratchBytes).  See surrogate.cu.
+  void predict_noalloc(const float* ang_dev, int n, double* energy_dev, cudaStream_t st) const;
+  static int noalloc_max_rows(int nin_pad);
 
  private:
   void ensure_scratch(int batch);

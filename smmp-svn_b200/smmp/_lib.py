@@ -90,6 +90,7 @@ _SIGS = {
     "smmp_sur_predict": (c_int, [c_void_p, P(c_double), c_int, P(c_double)]),
     "smmp_sur_gradients": (c_int, [c_void_p, P(c_double), P(c_double), c_int,
                                    P(ctypes.c_float), P(c_double)]),
+    "smmp_sur_predict_noalloc": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
     "smmp_sur_get_params": (c_int, [c_void_p, P(ctypes.c_float), P(ctypes.c_float)]),
     "smmp_sur_set_params": (c_int, [c_void_p, P(ctypes.c_float), P(ctypes.c_float)]),
 }
