@@ -148,6 +148,9 @@ void smmp_mol_free(smmp_mol_t* m);
  * number of heavy (SASA) atoms, residues. */
 int smmp_mol_info(const smmp_mol_t* m, long long info[6]);
 
+/* 0-based indices (into the molecule's variables) of its free dihedrals, in
+ * idvr order (redvar.f); info[2] of them. */
+int smmp_mol_idvr(const smmp_mol_t* m, int* idvr);
 /* An ensemble of nchains chains; chain c is a copy of mols[chain_mol[c]].
  * betas[c] is its inverse temperature.  shared_stream=0: chain c draws from
  * its own MT19937 stream seeded seeds[c]; shared_stream=1: all chains share
@@ -234,6 +237,18 @@ int smmp_sur_gradients(smmp_sur_t* s, const double* ang, const double* energy, i
  * NULL (the default stream). */
 int smmp_sur_predict_noalloc(smmp_sur_t* s, const float* ang_dev, int n, double* energy_dev,
                              void* stream);
+/* Delayed acceptance (no counterpart in the reference): sweeps of the
+ * ensemble screen each proposal with the surrogate first (stage 1) and
+ * evaluate the exact energy only for proposals that pass; the second stage
+ * corrects with the exact energy, so the stationary distribution is that of
+ * the plain sweep.  A chain whose stage-2 acceptance falls below `floor`
+ * after min_stage1 stage-1 passes takes plain steps from its next sweep on.
+ * All chains must be one molecule whose free dihedrals the surrogate takes;
+ * the surrogate must outlive the ensemble's use of it.  s = NULL: plain
+ * sweeps again.  Stage counters restart at zero. */
+int smmp_ens_set_surrogate(smmp_ens_t* e, smmp_sur_t* s, double floor, int min_stage1);
+/* Per chain: proposals that passed stage 1, and that were then accepted. */
+int smmp_ens_da_stats(smmp_ens_t* e, uint64_t* stage1, uint64_t* stage2);
 /* Parameters and normalisation norm[2] = {mu, sigma}. */
 int smmp_sur_get_params(smmp_sur_t* s, float* params, float* norm);
 int smmp_sur_set_params(smmp_sur_t* s, const float* params, const float* norm);

@@ -588,6 +588,14 @@ int smmp_mol_info(const smmp_mol_t* m, long long info[6]) {
   });
 }
 
+int smmp_mol_idvr(const smmp_mol_t* m, int* idvr) {
+  return guard([&] {
+    need(m && idvr, "NULL argument");
+    const MolTopo& t = m->m->topo;
+    for (size_t k = 0; k < t.idvr.size(); ++k) idvr[k] = t.idvr[k];
+  });
+}
+
 smmp_ens_t* smmp_ens_create(smmp_mol_t* const* mols, int nmols, const int* chain_mol,
                             int nchains, const int* seeds, const double* betas,
                             int shared_stream, int flags) {
@@ -929,6 +937,30 @@ int smmp_sur_predict_noalloc(smmp_sur_t* s, const float* ang_dev, int n, double*
   return guard([&] {
     need(s && ang_dev && energy_dev && n >= 0, "smmp_sur_predict_noalloc: bad arguments");
     s->s->predict_noalloc(ang_dev, n, energy_dev, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int smmp_ens_set_surrogate(smmp_ens_t* e, smmp_sur_t* s, double floor, int min_stage1) {
+  return guard([&] {
+    need(e != nullptr, "NULL ensemble");
+    if (s) {
+      DSurrogate v = s->s->device_view();
+      e->e->set_surrogate(&v, (float)floor, min_stage1);
+    } else {
+      e->e->set_surrogate(nullptr, 0.f, 0);
+    }
+  });
+}
+
+int smmp_ens_da_stats(smmp_ens_t* e, uint64_t* stage1, uint64_t* stage2) {
+  return guard([&] {
+    need(e && stage1 && stage2, "NULL argument");
+    std::vector<unsigned long long> a, b;
+    e->e->da_stats(a, b);
+    for (size_t c = 0; c < a.size(); ++c) {
+      stage1[c] = a[c];
+      stage2[c] = b[c];
+    }
   });
 }
 

@@ -1,5 +1,6 @@
 // Device-side data structures shared by the kernels and the host runtime.
 #pragma once
+#include <cuda_bf16.h>
 #include <cstdint>
 
 namespace smmpb200 {
@@ -79,6 +80,7 @@ struct DMolSet {
   int stage_bytes;           // shared-memory pool for the staged topology
   int stage_lists;           // 1: the pair lists are staged too (they fit)
   int any_rows;              // 1: some molecule evaluates its pairs by rows
+  int da;                    // 1: shared memory for the surrogate's first stage
   const DForceField* ff;     // device
   FFScalars f;
 };
@@ -94,6 +96,21 @@ struct DWeight {
 };
 
 // Mutable state of a set of chains (replicas).
+// Device view of a trained energy surrogate (an MLP on the sin/cos of the
+// free dihedrals, 3 hidden layers of 256, SiLU), BF16 weights.
+struct DSurrogate {
+  const __nv_bfloat16* w1;   // [nin_pad][256]
+  const __nv_bfloat16* w2;   // [256][256]
+  const __nv_bfloat16* w3;   // [256][256]
+  const __nv_bfloat16* w4;   // [256]
+  const float* b1;
+  const float* b2;
+  const float* b3;
+  const float* b4;
+  int nin, nin_pad;          // nin = 2 * free dihedrals
+  float mu, sigma;           // energy = mu + sigma * output
+};
+
 struct DChains {
   int nchains;
   const int* mol_of_chain;
@@ -111,6 +128,12 @@ struct DChains {
   unsigned long long* nprop;
   int* err;              // first error of each chain (0 = none)
   double* coords;        // optional [chain * 3 * tstride] coordinates after the call
+  // delayed acceptance (surrogate first stage), on when sur.w1 != nullptr
+  DSurrogate sur;
+  float da_floor;        // a chain whose stage-2 acceptance falls below this ...
+  int da_min;            // ... after this many stage-1 acceptances takes plain steps
+  unsigned long long* da_n1;   // [chain] proposals that passed stage 1
+  unsigned long long* da_n2;   // [chain] proposals accepted at stage 2
 };
 
 enum SweepFlags : int {

@@ -181,14 +181,17 @@ struct Smem {
   int* nbj;              // and their atom index (for the exact FP64 re-test)
   int* sq;               // SASA neighbour candidates per warp (kSasaQueue)
   Scalars* sc;
+  float* daf;            // surrogate: features (sin/cos, BF16-rounded) of the state
+  float* dap;            // surrogate: partial sums [4][256]
+  float* dah;            // surrogate: hidden activations [2][256]
   DMol* mol;
   char* pool;            // staged topology (see stage_mol)
 };
 
 __host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~size_t(15); }
 
-__host__ __device__ inline size_t smem_layout(int n, int v, int npnt, bool sasa, Smem* s,
-                                              char* base) {
+__host__ __device__ inline size_t smem_layout(int n, int v, int npnt, bool sasa, bool da,
+                                              Smem* s, char* base) {
   size_t off = 0;
   auto take = [&](size_t bytes) -> char* {
     char* p = base ? base + off : nullptr;
@@ -232,6 +235,9 @@ __host__ __device__ inline size_t smem_layout(int n, int v, int npnt, bool sasa,
   t.nbf = (float4*)take(sasa ? 16 * kWarps * kMaxNeighbours : 16);
   t.nbj = (int*)take(sasa ? 4 * kWarps * kMaxNeighbours : 4);
   t.sq = (int*)take(sasa ? 4 * kWarps * kSasaQueue : 4);
+  t.daf = (float*)take(da ? 4 * 2 * (size_t)(v > 0 ? v : 1) : 4);
+  t.dap = (float*)take(da ? 4 * 4 * 256 : 4);
+  t.dah = (float*)take(da ? 4 * 2 * 256 : 4);
   t.sc = (Scalars*)take(sizeof(Scalars));
   t.mol = (DMol*)take(sizeof(DMol));
   t.pool = take(0);
@@ -242,7 +248,7 @@ __host__ __device__ inline size_t smem_layout(int n, int v, int npnt, bool sasa,
 __device__ Smem carve(const DMolSet& set, bool sasa) {
   extern __shared__ __align__(16) char smem_raw[];
   Smem s;
-  smem_layout(set.max_atoms, set.max_vars, set.f.npnt, sasa, &s, smem_raw);
+  smem_layout(set.max_atoms, set.max_vars, set.f.npnt, sasa, set.da != 0, &s, smem_raw);
   return s;
 }
 
@@ -1354,6 +1360,304 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
   store_chain(ch, m, c, s);
 }
 
+// ============================================================================ delayed acceptance
+// Two-stage Metropolis step (delayed acceptance) with the energy surrogate as
+// the first stage.  For a proposal y from state x (same proposal as the plain
+// sweep, metropolis.f:42-66):
+//   stage 1: d1 = W(s(y)) - W(s(x)), pass with min(1, exp(-d1));
+//   stage 2 (only when stage 1 passes): the exact energy E(y);
+//            d2 = [W(E(y)) - W(E(x))] - d1, accept with min(1, exp(-d2)).
+// W is the sampling weight (beta*E canonically) and s the surrogate, a fixed
+// function of the state, so the chain keeps the exact stationary
+// distribution.  A chain whose stage-2 acceptance falls below the floor (after
+// da_min stage-1 passes) takes plain steps (stage 1 skipped) from its next
+// sweep on.  Uniforms come from the chain's own MT19937 stream as in the plain
+// sweep; the extra stage-1 draws make the stream's use differ from it.
+
+__device__ __forceinline__ float bf16_round(float v) {
+  return __bfloat162float(__float2bfloat16(v));
+}
+__device__ __forceinline__ float silu_f(float z) { return z / (1.f + expf(-z)); }
+
+// Features of the current state: sin/cos of every free dihedral, rounded to
+// BF16 as the training kernels round them.
+__device__ void sur_features(const DMol& m, Smem& s) {
+  for (int k = threadIdx.x; k < m.nfree; k += blockDim.x) {
+    float sn, cs;
+    sincosf((float)s.vlvr[m.idvr[k]], &sn, &cs);
+    s.daf[2 * k] = bf16_round(sn);
+    s.daf[2 * k + 1] = bf16_round(cs);
+  }
+}
+
+// One dense layer of 256 outputs for the whole block: out = act(b + x W),
+// W [K][256] BF16 row-major.  Thread t takes outputs 2*(t%128), +1 over the
+// K-slice t/128 (K split four ways); the slices are added in a fixed order,
+// so the result is a deterministic function of the input.  `kx`/`vx`: input
+// entries 2*kx, 2*kx+1 read as vx[0], vx[1] instead (kx < 0: none).
+template <bool SILU>
+__device__ void sur_layer(const __nv_bfloat16* __restrict__ W, const float* __restrict__ b,
+                          const float* x, int K, int kx, const float* vx, float* part,
+                          float* out) {
+  const int t = threadIdx.x, j2 = t & 127, ks = t >> 7;
+  float a0 = 0.f, a1 = 0.f;
+#pragma unroll 8
+  for (int k = ks; k < K; k += 4) {
+    const float xv = (k >> 1) == kx ? vx[k & 1] : x[k];
+    const __nv_bfloat162 w = reinterpret_cast<const __nv_bfloat162*>(W + (size_t)k * 256)[j2];
+    a0 = fmaf(xv, __low2float(w), a0);
+    a1 = fmaf(xv, __high2float(w), a1);
+  }
+  part[ks * 256 + 2 * j2] = a0;
+  part[ks * 256 + 2 * j2 + 1] = a1;
+  __syncthreads();
+  if (t < 256) {
+    const float z = b[t] + ((part[t] + part[256 + t]) + (part[512 + t] + part[768 + t]));
+    out[t] = SILU ? bf16_round(silu_f(z)) : z;
+  }
+  __syncthreads();
+}
+
+// Surrogate energy (kcal/mol) of the current features with free dihedral kx
+// replaced by (sin, cos) = vx; the same value in every thread.  Needs 512
+// threads.
+__device__ float sur_eval(const DSurrogate& S, Smem& s, int kx, const float* vx) {
+  float* h0 = s.dah;
+  float* h1 = s.dah + 256;
+  sur_layer<true>(S.w1, S.b1, s.daf, S.nin, kx, vx, s.dap, h0);
+  sur_layer<true>(S.w2, S.b2, h0, 256, -1, vx, s.dap, h1);
+  sur_layer<true>(S.w3, S.b3, h1, 256, -1, vx, s.dap, h0);
+  const int t = threadIdx.x;
+  float v = t < 256 ? h0[t] * __bfloat162float(S.w4[t]) : 0.f;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((t & 31) == 0 && t < 256) s.dap[t >> 5] = v;
+  __syncthreads();
+  float y = S.b4[0];
+#pragma unroll
+  for (int w = 0; w < 8; ++w) y += s.dap[w];
+  __syncthreads();
+  return S.mu + S.sigma * y;
+}
+
+// Metropolis test of exp(-d) against queue position k (as the plain sweep).
+__device__ __forceinline__ int mh_accept(const Smem& s, uint32_t k, double d) {
+  const double rd = qbuf(s.mt)[k & (kQueue - 1)], lrd = s.lq[k & (kQueue - 1)];
+  d = fmin(d, 100.0);
+  const double margin = -d - lrd;
+  if (margin > 1e-10) return 1;
+  if (margin < -1e-10) return 0;
+  return exp(-d) >= rd ? 1 : 0;
+}
+
+template <bool F32, bool ROWS, bool SASA>
+__global__ void __launch_bounds__(kThreads, 1) k_sweep_da(DMolSet set, DChains ch, DWeight w,
+                                                          int first, int nsweeps, int flags,
+                                                          double check_tol) {
+  const int c = first + blockIdx.x;
+  const bool rndord = (flags & kFlagRndOrd) != 0;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  Smem s = carve(set, SASA);
+  Scalars& sc = *s.sc;
+  const DMol& m = stage_mol(set, ch, c, s);
+  load_static(*set.ff, m, s, SASA);
+  load_chain(ch, m, c, s);
+  const double beta = ch.beta[c];
+  int* err = &ch.err[c];
+  const DSurrogate& S = ch.sur;
+  unsigned long long nacc = 0, nprop = 0, n1 = ch.da_n1[c], n2 = ch.da_n2[c];
+  const unsigned long long n1_0 = n1, n2_0 = n2;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t h = s.mt[kQHead], t = s.mt[kQTail];
+    const double* q = qbuf(s.mt);
+    for (uint32_t k = h + lane; k < t; k += 32) {
+      double v = q[k & (kQueue - 1)];
+      s.lq[k & (kQueue - 1)] = v > 0.0 ? log(v) : -INFINITY;
+    }
+    __syncwarp();
+    while (s.mt[kQTail] - s.mt[kQHead] < 24) rng_refill_warp(s.mt, s.lq);
+  }
+  __syncthreads();
+  uint32_t head = s.mt[kQHead];
+  double eol = 0.0, etor = 0.0;
+
+  for (int sw = 0; sw < nsweeps; ++sw) {
+    const bool plain = n1 >= (unsigned long long)ch.da_min &&
+                       (double)n2 < (double)ch.da_floor * (double)n1;
+    // ---- energy() and surrogate of the sweep's starting state
+    setvar_all(m, s);
+    __syncthreads();
+    torsion_all(m, s);
+    full_rebuild(m, s);
+    evaluate_block<F32, ROWS, SASA>(set.f, m, s, err);
+    __syncthreads();
+    {
+      double sum[5];
+      all_sums(s, sum);
+      eol = total_of(sum);
+      etor = sum[3];
+    }
+    sur_features(m, s);
+    __syncthreads();
+    float s_cur = plain ? 0.f : sur_eval(S, s, -1, nullptr);
+
+    for (int p = 0; p < m.nfree; ++p) {
+      if (warp == 0) {
+        const bool low = __shfl_sync(0xffffffffu, (s.mt[kQTail] - head) < 24u ? 1 : 0, 0) != 0;
+        if (low) rng_refill_warp(s.mt, s.lq);
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        make_proposal(m, s, p, head, rndord, sc.cur);
+        s.vlvr[sc.cur.jv] = sc.cur.vnew;
+      }
+      __syncthreads();
+      const Proposal cur = sc.cur;
+      head += cur.used;
+      ++nprop;
+      // ---- stage 1: surrogate
+      double d1 = 0.0;
+      float s_new = s_cur;
+      if (!plain) {
+        float vx[2];
+        float sn, cs;
+        sincosf((float)cur.vnew, &sn, &cs);
+        vx[0] = bf16_round(sn);
+        vx[1] = bf16_round(cs);
+        s_new = sur_eval(S, s, cur.ivar, vx);
+        d1 = __dsub_rn(weight(w, beta, (double)s_new), weight(w, beta, (double)s_cur));
+        int pass = 1;
+        if (d1 > 0.0) {
+          pass = mh_accept(s, head, d1);
+          head += 1;
+        }
+        if (!pass) {   // rejected without the exact energy
+          __syncthreads();
+          if (threadIdx.x == 0) s.vlvr[cur.jv] = cur.vold;
+          __syncthreads();
+          continue;
+        }
+        ++n1;
+      }
+      // ---- stage 2: exact energy of the proposal
+      const int lo = m.var_lo[cur.jv], hi = m.var_hi[cur.jv];
+      const bool flip = lo <= m.i3 && m.i3 <= hi;
+      const int span = hi - lo + 1;
+      const int nmoved = flip ? m.natoms - span : span;
+      {
+        const double sth = flip ? -cur.sth : cur.sth;
+        double px = s.x[cur.b], py = s.y[cur.b], pz = s.z[cur.b];
+        double kx = px - s.x[cur.a], ky = py - s.y[cur.a], kz = pz - s.z[cur.a];
+        double inv = rsqrt(kx * kx + ky * ky + kz * kz);
+        kx *= inv;
+        ky *= inv;
+        kz *= inv;
+        __syncthreads();   // every thread has read the axis
+        for (int t = threadIdx.x; t < nmoved; t += blockDim.x) {
+          const int k = moved_atom(t, lo, span, flip);
+          if (flip && (k == cur.a || k == cur.b)) continue;
+          double vx = s.x[k] - px, vy = s.y[k] - py, vz = s.z[k] - pz;
+          s.bx[k] = s.x[k];
+          s.by[k] = s.y[k];
+          s.bz[k] = s.z[k];
+          double kd = kx * vx + ky * vy + kz * vz;
+          double cx = ky * vz - kz * vy, cy = kz * vx - kx * vz, cz = kx * vy - ky * vx;
+          double f = kd * (1.0 - cur.cth);
+          s.x[k] = px + vx * cur.cth + cx * sth + kx * f;
+          s.y[k] = py + vy * cur.cth + cy * sth + ky * f;
+          s.z[k] = pz + vz * cur.cth + cz * sth + kz * f;
+          if (F32) f32_copy(s, k);
+        }
+      }
+      __syncthreads();
+      {
+        double el = 0.0, vw = 0.0, hb = 0.0, sl = 0.0;
+        if (ROWS && m.rows)
+          pair_rows<F32, true>(set.f, m, s, kWarps, el, vw, hb);
+        else
+          pair_energy<F32, false>(set.f, m, s, threadIdx.x, blockDim.x, el, vw, hb);
+        if (SASA) sl = sasa_energy(set.f, m, s, 0, kWarps, err);
+        double v = ((el + vw) + hb) + sl;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) s.red[warp * 8] = v;
+      }
+      __syncthreads();
+      double epair = 0.0;
+      for (int k = 0; k < kWarps; ++k) epair += s.red[k * 8];
+      const double etor_new = (etor - cur.eold) + cur.enew;
+      const double enw = epair + etor_new;
+      const double d2 =
+          __dsub_rn(__dsub_rn(weight(w, beta, enw), weight(w, beta, eol)), d1);
+      int up = 1;
+      if (d2 > 0.0) {
+        up = mh_accept(s, head, d2);
+        head += 1;
+      }
+      __syncthreads();   // every thread has read s.red and the queue
+      if (up) {
+        eol = enw;
+        etor = etor_new;
+        s_cur = s_new;
+        ++nacc;
+        if (!plain) ++n2;
+        if (threadIdx.x == 0) {
+          s.et[cur.jv] = cur.enew;
+          float sn, cs;
+          sincosf((float)cur.vnew, &sn, &cs);
+          s.daf[2 * cur.ivar] = bf16_round(sn);
+          s.daf[2 * cur.ivar + 1] = bf16_round(cs);
+        }
+      } else {
+        for (int t = threadIdx.x; t < nmoved; t += blockDim.x) {
+          const int k = moved_atom(t, lo, span, flip);
+          if (flip && (k == cur.a || k == cur.b)) continue;
+          s.x[k] = s.bx[k];
+          s.y[k] = s.by[k];
+          s.z[k] = s.bz[k];
+          if (F32) f32_copy(s, k);
+        }
+        if (threadIdx.x == 0) s.vlvr[cur.jv] = cur.vold;
+      }
+      if (!isfinite(enw) && threadIdx.x == 0) set_err(err, kErrNonFinite);
+      __syncthreads();
+      // the dihedral state follows the variables (the setvar of energy())
+      setvar_all(m, s);
+      __syncthreads();
+    }
+    // ---- closing energy() and consistency check (metropolis.f:172-179)
+    setvar_all(m, s);
+    __syncthreads();
+    torsion_all(m, s);
+    full_rebuild(m, s);
+    evaluate_block<F32, ROWS, SASA>(set.f, m, s, err);
+    __syncthreads();
+    {
+      double sum[5];
+      all_sums(s, sum);
+      const double enew = total_of(sum);
+      if (threadIdx.x == 0) {
+        if (!(flags & kFlagNoCheck) && fabs(eol - enew) > check_tol && eol < 100000.0)
+          set_err(err, kErrConsistency);
+        write_terms(ch, c, sum);
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    ch.eol[c] = eol;
+    ch.nacc[c] += nacc;
+    ch.nprop[c] += nprop;
+    ch.da_n1[c] = n1;
+    ch.da_n2[c] = n2;
+    s.mt[kQHead] = head;
+  }
+  (void)n1_0;
+  (void)n2_0;
+  __syncthreads();
+  store_chain(ch, m, c, s);
+}
+
 // Replica exchange (partem_s.f:210-232): alternate even/odd neighbour pairs,
 // replica num_rep pairs with 1 when `wrap` is set.  temp_chain[k] is the chain
 // at temperature label k (ipoi); betas[k] the inverse temperature of label k.
@@ -1398,7 +1702,8 @@ __global__ void k_exchange(DChains ch, int* temp_chain, const double* betas, int
 // ============================================================================ host wrappers
 
 size_t sweep_smem_bytes(const DMolSet& set) {
-  return smem_layout(set.max_atoms, set.max_vars, set.f.npnt, set.f.itysol > 0, nullptr, nullptr) +
+  return smem_layout(set.max_atoms, set.max_vars, set.f.npnt, set.f.itysol > 0, set.da != 0,
+                     nullptr, nullptr) +
          (size_t)set.stage_bytes;
 }
 
@@ -1453,6 +1758,13 @@ template <bool F32, bool ROWS, bool SASA>
 static cudaError_t launch_sweep_t(const DMolSet& set, const DChains& ch, const DWeight& w,
                                   int first, int count, int nsweeps, int flags, double check_tol,
                                   size_t sm, cudaStream_t st) {
+  if (ch.sur.w1 != nullptr) {   // delayed acceptance with the surrogate
+    cudaError_t e = prep_smem((const void*)k_sweep_da<F32, ROWS, SASA>, sm);
+    if (e != cudaSuccess || count <= 0) return e;
+    k_sweep_da<F32, ROWS, SASA><<<count, kThreads, sm, st>>>(set, ch, w, first, nsweeps, flags,
+                                                             check_tol);
+    return cudaGetLastError();
+  }
   cudaError_t e = prep_smem((const void*)k_sweep<F32, ROWS, SASA>, sm);
   if (e != cudaSuccess || count <= 0) return e;
   k_sweep<F32, ROWS, SASA><<<count, kThreads, sm, st>>>(set, ch, w, first, nsweeps, flags,

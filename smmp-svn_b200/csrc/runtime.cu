@@ -168,13 +168,24 @@ DeviceSet::DeviceSet(const std::vector<std::shared_ptr<Molecule>>& mols) {
   set_.f = FFScalars{ff.conv, ff.plt, ff.slp, ff.epsd, ff.itysol, ff.npnt};
   set_.any_rows = 0;
   for (const DMol& d : dm) set_.any_rows |= d.rows;
+  set_.da = 0;
+  with_lists_ = without_ = 0;
+  for (const DMol& d : dm) {
+    with_lists_ = std::max(with_lists_, stage_bytes_of(d, true));
+    without_ = std::max(without_, stage_bytes_of(d, false));
+  }
+  size_staging();
+}
+
+void DeviceSet::set_da(bool on) {
+  set_.da = on ? 1 : 0;
+  size_staging();
+}
+
+void DeviceSet::size_staging() {
+  const size_t with_lists = with_lists_, without = without_;
   // stage the pair lists too when the largest molecule's copy fits
   const size_t budget = 200 * 1024;
-  size_t with_lists = 0, without = 0;
-  for (const DMol& d : dm) {
-    with_lists = std::max(with_lists, stage_bytes_of(d, true));
-    without = std::max(without, stage_bytes_of(d, false));
-  }
   set_.stage_lists = 1;
   set_.stage_bytes = (int)with_lists;
   if (sweep_smem_bytes(set_) > budget) {
@@ -240,6 +251,13 @@ Ensemble::Ensemble(std::vector<std::shared_ptr<Molecule>> mols, std::vector<int>
   ch_.nprop = dalloc<unsigned long long>(allocs_, n_);
   ch_.err = dalloc<int>(allocs_, n_);
   ch_.coords = nullptr;
+  ch_.sur = DSurrogate{};
+  ch_.da_floor = 0.2f;
+  ch_.da_min = 64;
+  ch_.da_n1 = dalloc<unsigned long long>(allocs_, n_);
+  ch_.da_n2 = dalloc<unsigned long long>(allocs_, n_);
+  check_cuda(cudaMemset(ch_.da_n1, 0, n_ * sizeof(unsigned long long)), "memset");
+  check_cuda(cudaMemset(ch_.da_n2, 0, n_ * sizeof(unsigned long long)), "memset");
   check_cuda(cudaMemset(ch_.nacc, 0, n_ * sizeof(unsigned long long)), "memset");
   check_cuda(cudaMemset(ch_.nprop, 0, n_ * sizeof(unsigned long long)), "memset");
   check_cuda(cudaMemset(ch_.err, 0, n_ * sizeof(int)), "memset");
@@ -271,6 +289,36 @@ Ensemble::~Ensemble() {
   for (void* p : allocs_) cudaFree(p);
   if (coords_buf_) cudaFree(coords_buf_);
   if (own_stream_) cudaStreamDestroy(own_stream_);
+}
+
+void Ensemble::set_surrogate(const DSurrogate* view, float floor, int min_stage1) {
+  check_cuda(cudaStreamSynchronize(stream_), "set_surrogate sync");
+  if (view) {
+    if (view->w1 == nullptr) throw std::invalid_argument("set_surrogate: empty surrogate");
+    for (int c = 0; c < n_; ++c)
+      if (2 * molecule_of(c).topo.nfree != view->nin)
+        throw std::invalid_argument("set_surrogate: the surrogate's input width does not match "
+                                    "every chain's free dihedrals");
+    if (floor < 0.f || floor > 1.f || min_stage1 < 0)
+      throw std::invalid_argument("set_surrogate: floor in [0,1], min_stage1 >= 0");
+    ch_.sur = *view;
+    ch_.da_floor = floor;
+    ch_.da_min = min_stage1;
+  } else {
+    ch_.sur = DSurrogate{};
+  }
+  dev_->set_da(view != nullptr);
+  check_cuda(cudaMemset(ch_.da_n1, 0, n_ * sizeof(unsigned long long)), "memset");
+  check_cuda(cudaMemset(ch_.da_n2, 0, n_ * sizeof(unsigned long long)), "memset");
+  if (graph_) cudaGraphExecDestroy(graph_);   // kernel arguments changed
+  graph_ = nullptr;
+  graph_len_ = 0;
+}
+
+void Ensemble::da_stats(std::vector<unsigned long long>& n1,
+                        std::vector<unsigned long long>& n2) const {
+  d2h(n1, ch_.da_n1, n_);
+  d2h(n2, ch_.da_n2, n_);
 }
 
 void Ensemble::set_stream(cudaStream_t s) {

@@ -40,8 +40,12 @@ class DeviceSet {
   DeviceSet(const DeviceSet&) = delete;
   DeviceSet& operator=(const DeviceSet&) = delete;
   const DMolSet& set() const { return set_; }
+  // reserve shared memory for the surrogate's first stage (re-sizes staging)
+  void set_da(bool on);
 
  private:
+  void size_staging();
+  size_t with_lists_ = 0, without_ = 0;
   template <class T>
   const T* upload(const std::vector<T>& v);
   std::vector<void*> allocs_;
@@ -72,6 +76,12 @@ class Ensemble {
 
   int nchains() const { return n_; }
   void set_stream(cudaStream_t s);   // nullptr: own stream
+  // Delayed acceptance with a trained surrogate as the first stage (nullptr:
+  // plain Metropolis).  A chain whose stage-2 acceptance falls below `floor`
+  // after min_stage1 stage-1 passes takes plain steps.  The surrogate's
+  // device memory must outlive its use here.
+  void set_surrogate(const DSurrogate* view, float floor, int min_stage1);
+  void da_stats(std::vector<unsigned long long>& n1, std::vector<unsigned long long>& n2) const;
   cudaStream_t stream() const { return stream_; }
   const DChains& chains() const { return ch_; }
   const DMolSet& set() const { return dev_->set(); }

@@ -11,6 +11,8 @@
 #include <cstdint>
 #include <vector>
 
+#include "device.cuh"
+
 namespace smmpb200 {
 
 constexpr int kHidden = 256;
@@ -25,20 +27,6 @@ struct MlpLayout {
   int nin = 0, nin_pad = 0;
   size_t w1 = 0, b1 = 0, w2 = 0, b2 = 0, w3 = 0, b3 = 0, w4 = 0, b4 = 0, n = 0;
   explicit MlpLayout(int nin_ = 0);
-};
-
-// Device-side view of a trained surrogate for the sweep kernel.
-struct DSurrogate {
-  const __nv_bfloat16* w1;   // [nin_pad][H]
-  const __nv_bfloat16* w2;   // [H][H]
-  const __nv_bfloat16* w3;   // [H][H]
-  const __nv_bfloat16* w4;   // [H]
-  const float* b1;
-  const float* b2;
-  const float* b3;
-  const float* b4;
-  int nin, nin_pad;          // nin = 2 * free dihedrals
-  float mu, sigma;           // energy = mu + sigma * output
 };
 
 class Surrogate {

@@ -59,6 +59,7 @@ _SIGS = {
     "smmp_mol_build": (c_void_p, [c_char_p, P(Config), c_char_p, c_char_p, c_char_p, c_char_p]),
     "smmp_mol_free": (None, [c_void_p]),
     "smmp_mol_info": (c_int, [c_void_p, P(ctypes.c_longlong)]),
+    "smmp_mol_idvr": (c_int, [c_void_p, P(c_int)]),
     "smmp_ens_create": (c_void_p, [P(c_void_p), c_int, P(c_int), c_int, P(c_int), P(c_double),
                                    c_int, c_int]),
     "smmp_ens_free": (None, [c_void_p]),
@@ -91,6 +92,8 @@ _SIGS = {
     "smmp_sur_gradients": (c_int, [c_void_p, P(c_double), P(c_double), c_int,
                                    P(ctypes.c_float), P(c_double)]),
     "smmp_sur_predict_noalloc": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
+    "smmp_ens_set_surrogate": (c_int, [c_void_p, c_void_p, c_double, c_int]),
+    "smmp_ens_da_stats": (c_int, [c_void_p, P(ctypes.c_uint64), P(ctypes.c_uint64)]),
     "smmp_sur_get_params": (c_int, [c_void_p, P(ctypes.c_float), P(ctypes.c_float)]),
     "smmp_sur_set_params": (c_int, [c_void_p, P(ctypes.c_float), P(ctypes.c_float)]),
 }

@@ -49,6 +49,9 @@ class Molecule:
         check(lib.smmp_mol_info(self._h, info))
         self.natoms, self.nvar, self.nvr, self.npairs, self.nheavy, self.nres = list(info)
         self.itysol = itysol
+        idvr = np.zeros(max(self.nvr, 1), dtype=np.int32)
+        check(lib.smmp_mol_idvr(self._h, idvr.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+        self.idvr = idvr[:self.nvr]          # 0-based variable index of each free dihedral
 
     def __del__(self):
         if getattr(self, "_h", None):
@@ -183,6 +186,23 @@ class Ensemble:
         out = np.zeros(n)
         check(lib.smmp_ens_draw(self._h, int(slot), int(n), out.ctypes.data_as(_D)))
         return out
+
+    def set_surrogate(self, surrogate, floor=0.2, min_stage1=64):
+        """Delayed acceptance with a trained smmp.surrogate.Surrogate as the
+        first stage (None: plain sweeps).  Chains whose stage-2 acceptance
+        falls below `floor` after min_stage1 stage-1 passes take plain
+        steps."""
+        self._surrogate = surrogate          # keep its device memory alive
+        check(lib.smmp_ens_set_surrogate(self._h, surrogate._h if surrogate else None,
+                                         float(floor), int(min_stage1)))
+
+    def da_stats(self):
+        """(stage-1 passes, stage-2 accepts) per chain."""
+        a = np.zeros(self.nchains, dtype=np.uint64)
+        b = np.zeros(self.nchains, dtype=np.uint64)
+        check(lib.smmp_ens_da_stats(self._h, a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
+                                    b.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))))
+        return a, b
 
     def checkpoint(self):
         n = ctypes.c_uint64(0)

@@ -93,3 +93,18 @@ class Surrogate:
             out[name] = (slice(off, off + n), shape)
             off += n
         return out
+
+
+def collect_samples(ens, molecule, nsweeps, pt=True):
+    """Run nsweeps sweeps (parallel tempering when pt) of an ensemble of one
+    molecule and return its states after every sweep: (angles [n, nvr] of the
+    free dihedrals, energies [n])."""
+    ang, en = [], []
+    for _ in range(int(nsweeps)):
+        if pt:
+            ens.pt_sweeps(1, graph_chunk=1)
+        else:
+            ens.sweeps(1)
+        ang.append(ens.vlvr()[:, molecule.idvr].copy())
+        en.append(ens.energies().copy())
+    return np.concatenate(ang), np.concatenate(en)
