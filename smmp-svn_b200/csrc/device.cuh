@@ -103,6 +103,9 @@ struct DSurrogate {
   const __nv_bfloat16* w2;   // [256][256]
   const __nv_bfloat16* w3;   // [256][256]
   const __nv_bfloat16* w4;   // [256]
+  const __nv_bfloat16* w1t;  // [256][nin_pad]  (transposed copies: K contiguous)
+  const __nv_bfloat16* w2t;  // [256][256]
+  const __nv_bfloat16* w3t;  // [256][256]
   const float* b1;
   const float* b2;
   const float* b3;

@@ -182,8 +182,11 @@ struct Smem {
   int* sq;               // SASA neighbour candidates per warp (kSasaQueue)
   Scalars* sc;
   float* daf;            // surrogate: features (sin/cos, BF16-rounded) of the state
-  float* dap;            // surrogate: partial sums [4][256]
-  float* dah;            // surrogate: hidden activations [2][256]
+  __nv_bfloat16* dfe;    // surrogate: feature rows of a batch [16][kDaStride(nin_pad)]
+  __nv_bfloat16* dh0;    // surrogate: hidden activations [16][264]
+  __nv_bfloat16* dh1;
+  float* dsv;            // surrogate energies of the batch's rows [16]
+  Proposal* dprop;       // the batch's proposals [16]
   DMol* mol;
   char* pool;            // staged topology (see stage_mol)
 };
@@ -235,9 +238,13 @@ __host__ __device__ inline size_t smem_layout(int n, int v, int npnt, bool sasa,
   t.nbf = (float4*)take(sasa ? 16 * kWarps * kMaxNeighbours : 16);
   t.nbj = (int*)take(sasa ? 4 * kWarps * kMaxNeighbours : 4);
   t.sq = (int*)take(sasa ? 4 * kWarps * kSasaQueue : 4);
+  const size_t fpad = ((size_t)2 * (v > 0 ? v : 1) + 15) / 16 * 16 + 8;   // row stride
   t.daf = (float*)take(da ? 4 * 2 * (size_t)(v > 0 ? v : 1) : 4);
-  t.dap = (float*)take(da ? 4 * 4 * 256 : 4);
-  t.dah = (float*)take(da ? 4 * 2 * 256 : 4);
+  t.dfe = (__nv_bfloat16*)take(da ? 2 * 16 * fpad : 16);
+  t.dh0 = (__nv_bfloat16*)take(da ? 2 * 16 * 264 : 16);
+  t.dh1 = (__nv_bfloat16*)take(da ? 2 * 16 * 264 : 16);
+  t.dsv = (float*)take(da ? 4 * 16 : 16);
+  t.dprop = (Proposal*)take(da ? sizeof(Proposal) * 16 : 16);
   t.sc = (Scalars*)take(sizeof(Scalars));
   t.mol = (DMol*)take(sizeof(DMol));
   t.pool = take(0);
@@ -1390,53 +1397,82 @@ __device__ void sur_features(const DMol& m, Smem& s) {
   }
 }
 
-// One dense layer of 256 outputs for the whole block: out = act(b + x W),
-// W [K][256] BF16 row-major.  Thread t takes outputs 2*(t%128), +1 over the
-// K-slice t/128 (K split four ways); the slices are added in a fixed order,
-// so the result is a deterministic function of the input.  `kx`/`vx`: input
-// entries 2*kx, 2*kx+1 read as vx[0], vx[1] instead (kx < 0: none).
-template <bool SILU>
-__device__ void sur_layer(const __nv_bfloat16* __restrict__ W, const float* __restrict__ b,
-                          const float* x, int K, int kx, const float* vx, float* part,
-                          float* out) {
-  const int t = threadIdx.x, j2 = t & 127, ks = t >> 7;
-  float a0 = 0.f, a1 = 0.f;
-#pragma unroll 8
-  for (int k = ks; k < K; k += 4) {
-    const float xv = (k >> 1) == kx ? vx[k & 1] : x[k];
-    const __nv_bfloat162 w = reinterpret_cast<const __nv_bfloat162*>(W + (size_t)k * 256)[j2];
-    a0 = fmaf(xv, __low2float(w), a0);
-    a1 = fmaf(xv, __high2float(w), a1);
+__device__ __forceinline__ uint32_t lds32(const __nv_bfloat16* p) {
+  return *reinterpret_cast<const uint32_t*>(p);
+}
+__device__ __forceinline__ uint32_t ldg32(const __nv_bfloat16* p) {
+  return __ldg(reinterpret_cast<const unsigned int*>(p));
+}
+__device__ __forceinline__ void mma_bf16_16816(float* c, const uint32_t* a, const uint32_t* b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// One dense layer for the 16 rows of a batch on the tensor cores:
+// out[r][n] = bf16(silu(b[n] + sum_k A[r][k] Wt[n][k])), A [16][K] BF16 in
+// shared memory (row stride lda), Wt [256][K] BF16 (the transposed weights,
+// K contiguous, read from L2).  Warp w computes columns 16w..16w+15 (two
+// m16n8k16 tiles).  Every row is computed by the same instructions, so a
+// row's result does not depend on the other rows.
+__device__ void mlp_layer16(const __nv_bfloat16* __restrict__ Wt, const float* __restrict__ b,
+                            const __nv_bfloat16* A, int lda, int K, __nv_bfloat16* out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+  const int n0 = warp * 16;
+  const __nv_bfloat16* w0 = Wt + (size_t)(n0 + g) * K + 2 * t;
+  const __nv_bfloat16* w1 = Wt + (size_t)(n0 + 8 + g) * K + 2 * t;
+  float c0[4] = {0.f, 0.f, 0.f, 0.f}, c1[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 4
+  for (int kk = 0; kk < K; kk += 16) {
+    const uint32_t b0[2] = {ldg32(w0 + kk), ldg32(w0 + kk + 8)};
+    const uint32_t b1[2] = {ldg32(w1 + kk), ldg32(w1 + kk + 8)};
+    const uint32_t a[4] = {lds32(A + g * lda + kk + 2 * t), lds32(A + (g + 8) * lda + kk + 2 * t),
+                           lds32(A + g * lda + kk + 2 * t + 8),
+                           lds32(A + (g + 8) * lda + kk + 2 * t + 8)};
+    mma_bf16_16816(c0, a, b0);
+    mma_bf16_16816(c1, a, b1);
   }
-  part[ks * 256 + 2 * j2] = a0;
-  part[ks * 256 + 2 * j2 + 1] = a1;
-  __syncthreads();
-  if (t < 256) {
-    const float z = b[t] + ((part[t] + part[256 + t]) + (part[512 + t] + part[768 + t]));
-    out[t] = SILU ? bf16_round(silu_f(z)) : z;
-  }
+#pragma unroll
+  for (int h = 0; h < 2; ++h)
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int r = g + 8 * h;
+      const int n = n0 + 2 * t + q;
+      out[r * 264 + n] = __float2bfloat16(silu_f(c0[2 * h + q] + b[n]));
+      out[r * 264 + n + 8] = __float2bfloat16(silu_f(c1[2 * h + q] + b[n + 8]));
+    }
   __syncthreads();
 }
 
-// Surrogate energy (kcal/mol) of the current features with free dihedral kx
-// replaced by (sin, cos) = vx; the same value in every thread.  Needs 512
-// threads.
-__device__ float sur_eval(const DSurrogate& S, Smem& s, int kx, const float* vx) {
-  float* h0 = s.dah;
-  float* h1 = s.dah + 256;
-  sur_layer<true>(S.w1, S.b1, s.daf, S.nin, kx, vx, s.dap, h0);
-  sur_layer<true>(S.w2, S.b2, h0, 256, -1, vx, s.dap, h1);
-  sur_layer<true>(S.w3, S.b3, h1, 256, -1, vx, s.dap, h0);
-  const int t = threadIdx.x;
-  float v = t < 256 ? h0[t] * __bfloat162float(S.w4[t]) : 0.f;
+// Surrogate energies (kcal/mol) of the 16 feature rows in s.dfe, into
+// s.dsv.  Needs 16 warps.
+__device__ void sur_batch(const DSurrogate& S, Smem& s) {
+  const int lda1 = S.nin_pad + 8;
+  mlp_layer16(S.w1t, S.b1, s.dfe, lda1, S.nin_pad, s.dh0);
+  mlp_layer16(S.w2t, S.b2, s.dh0, 264, 256, s.dh1);
+  mlp_layer16(S.w3t, S.b3, s.dh1, 264, 256, s.dh0);
+  const int lane = threadIdx.x & 31, r = threadIdx.x >> 5;
+  float v = 0.f;
+  for (int n = lane; n < 256; n += 32)
+    v += __bfloat162float(s.dh0[r * 264 + n]) * __bfloat162float(S.w4[n]);
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  if ((t & 31) == 0 && t < 256) s.dap[t >> 5] = v;
+  if (lane == 0) s.dsv[r] = S.mu + S.sigma * (v + S.b4[0]);
   __syncthreads();
-  float y = S.b4[0];
-#pragma unroll
-  for (int w = 0; w < 8; ++w) y += s.dap[w];
-  __syncthreads();
-  return S.mu + S.sigma * y;
+}
+
+// Feature row r of the batch: the state's features with free dihedral kx
+// set to angle a (kx < 0: the state itself); padding columns zero.
+__device__ void sur_row(const DSurrogate& S, Smem& s, int r, int kx, double a) {
+  const int lda1 = S.nin_pad + 8;
+  float sn = 0.f, cs = 0.f;
+  if (kx >= 0) sincosf((float)a, &sn, &cs);
+  for (int c = threadIdx.x & 31; c < S.nin_pad; c += 32) {
+    float v = c < S.nin ? s.daf[c] : 0.f;
+    if ((c >> 1) == kx) v = (c & 1) ? bf16_round(cs) : bf16_round(sn);
+    s.dfe[r * lda1 + c] = __float2bfloat16(v);
+  }
 }
 
 // Metropolis test of exp(-d) against queue position k (as the plain sweep).
@@ -1457,7 +1493,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep_da(DMolSet set, DChains c
   const bool rndord = (flags & kFlagRndOrd) != 0;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   Smem s = carve(set, SASA);
-  Scalars& sc = *s.sc;
   const DMol& m = stage_mol(set, ch, c, s);
   load_static(*set.ff, m, s, SASA);
   load_chain(ch, m, c, s);
@@ -1482,8 +1517,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep_da(DMolSet set, DChains c
   double eol = 0.0, etor = 0.0;
 
   for (int sw = 0; sw < nsweeps; ++sw) {
+    // stage-2 acceptance n2 / max(n1, 1) below the floor, once n1 >= da_min
     const bool plain = n1 >= (unsigned long long)ch.da_min &&
-                       (double)n2 < (double)ch.da_floor * (double)n1;
+                       (double)n2 < (double)ch.da_floor * (double)(n1 > 0 ? n1 : 1);
     // ---- energy() and surrogate of the sweep's starting state
     setvar_all(m, s);
     __syncthreads();
@@ -1499,131 +1535,162 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep_da(DMolSet set, DChains c
     }
     sur_features(m, s);
     __syncthreads();
-    float s_cur = plain ? 0.f : sur_eval(S, s, -1, nullptr);
-
-    for (int p = 0; p < m.nfree; ++p) {
+    float s_cur = 0.f;
+    if (!plain) {   // the state's own surrogate energy: row 0 of a batch
+      if (warp == 0) sur_row(S, s, 0, -1, 0.0);
+      __syncthreads();
+      sur_batch(S, s);
+      s_cur = s.dsv[0];
+    }
+    // Proposals are drawn in batches of up to 16 (variables p, p+1, ... in
+    // turn; each one from the current state) and screened together on the
+    // tensor cores.  They are then decided in order; an accepted move changes
+    // the state, so the batch ends there and the next one starts after it.
+    // Drawn proposals that a batch's end leaves unused are dropped (their
+    // uniforms are independent of everything else).
+    int p = 0;
+    while (p < m.nfree) {
+      const int per = rndord ? 2 : 1;              // uniforms per proposal
+      // the 64-entry queue is refilled 32 at a time below 32 entries: a
+      // batch takes at most 30 of them and leaves two for its first decisions
+      const int nb = plain ? 1 : min(min(16, 30 / per), m.nfree - p);
       if (warp == 0) {
-        const bool low = __shfl_sync(0xffffffffu, (s.mt[kQTail] - head) < 24u ? 1 : 0, 0) != 0;
-        if (low) rng_refill_warp(s.mt, s.lq);
+        while (true) {   // room for the batch's proposals and two decisions
+          const bool low =
+              __shfl_sync(0xffffffffu, (s.mt[kQTail] - head) < (uint32_t)(nb * per + 2) ? 1 : 0, 0) != 0;
+          if (!low) break;
+          rng_refill_warp(s.mt, s.lq);
+        }
+        if (lane < nb) make_proposal(m, s, p + lane, head + lane * per, rndord, s.dprop[lane]);
       }
       __syncthreads();
-      if (threadIdx.x == 0) {
-        make_proposal(m, s, p, head, rndord, sc.cur);
-        s.vlvr[sc.cur.jv] = sc.cur.vnew;
-      }
-      __syncthreads();
-      const Proposal cur = sc.cur;
-      head += cur.used;
-      ++nprop;
-      // ---- stage 1: surrogate
-      double d1 = 0.0;
-      float s_new = s_cur;
+      head += nb * per;
       if (!plain) {
-        float vx[2];
-        float sn, cs;
-        sincosf((float)cur.vnew, &sn, &cs);
-        vx[0] = bf16_round(sn);
-        vx[1] = bf16_round(cs);
-        s_new = sur_eval(S, s, cur.ivar, vx);
-        d1 = __dsub_rn(weight(w, beta, (double)s_new), weight(w, beta, (double)s_cur));
-        int pass = 1;
-        if (d1 > 0.0) {
-          pass = mh_accept(s, head, d1);
+        for (int r = warp; r < 16; r += kWarps) {
+          if (r < nb)
+            sur_row(S, s, r, s.dprop[r].ivar, s.dprop[r].vnew);
+          else
+            sur_row(S, s, r, -1, 0.0);
+        }
+        __syncthreads();
+        sur_batch(S, s);
+      }
+      int next = p + nb;
+      for (int j = 0; j < nb; ++j) {
+        if (warp == 0) {   // at most two decisions per proposal
+          const bool low = __shfl_sync(0xffffffffu, (s.mt[kQTail] - head) < 2u ? 1 : 0, 0) != 0;
+          if (low) rng_refill_warp(s.mt, s.lq);
+        }
+        __syncthreads();
+        const Proposal cur = s.dprop[j];
+        ++nprop;
+        // ---- stage 1: surrogate
+        double d1 = 0.0;
+        float s_new = s_cur;
+        if (!plain) {
+          s_new = s.dsv[j];
+          d1 = __dsub_rn(weight(w, beta, (double)s_new), weight(w, beta, (double)s_cur));
+          int pass = 1;
+          if (d1 > 0.0) {
+            pass = mh_accept(s, head, d1);
+            head += 1;
+          }
+          if (!pass) continue;   // rejected without the exact energy
+          ++n1;
+        }
+        // ---- stage 2: exact energy of the proposal
+        __syncthreads();
+        if (threadIdx.x == 0) s.vlvr[cur.jv] = cur.vnew;
+        const int lo = m.var_lo[cur.jv], hi = m.var_hi[cur.jv];
+        const bool flip = lo <= m.i3 && m.i3 <= hi;
+        const int span = hi - lo + 1;
+        const int nmoved = flip ? m.natoms - span : span;
+        {
+          const double sth = flip ? -cur.sth : cur.sth;
+          double px = s.x[cur.b], py = s.y[cur.b], pz = s.z[cur.b];
+          double kx = px - s.x[cur.a], ky = py - s.y[cur.a], kz = pz - s.z[cur.a];
+          double inv = rsqrt(kx * kx + ky * ky + kz * kz);
+          kx *= inv;
+          ky *= inv;
+          kz *= inv;
+          __syncthreads();   // every thread has read the axis
+          for (int t = threadIdx.x; t < nmoved; t += blockDim.x) {
+            const int k = moved_atom(t, lo, span, flip);
+            if (flip && (k == cur.a || k == cur.b)) continue;
+            double vx = s.x[k] - px, vy = s.y[k] - py, vz = s.z[k] - pz;
+            s.bx[k] = s.x[k];
+            s.by[k] = s.y[k];
+            s.bz[k] = s.z[k];
+            double kd = kx * vx + ky * vy + kz * vz;
+            double cx = ky * vz - kz * vy, cy = kz * vx - kx * vz, cz = kx * vy - ky * vx;
+            double f = kd * (1.0 - cur.cth);
+            s.x[k] = px + vx * cur.cth + cx * sth + kx * f;
+            s.y[k] = py + vy * cur.cth + cy * sth + ky * f;
+            s.z[k] = pz + vz * cur.cth + cz * sth + kz * f;
+            if (F32) f32_copy(s, k);
+          }
+        }
+        __syncthreads();
+        {
+          double el = 0.0, vw = 0.0, hb = 0.0, sl = 0.0;
+          if (ROWS && m.rows)
+            pair_rows<F32, true>(set.f, m, s, kWarps, el, vw, hb);
+          else
+            pair_energy<F32, false>(set.f, m, s, threadIdx.x, blockDim.x, el, vw, hb);
+          if (SASA) sl = sasa_energy(set.f, m, s, 0, kWarps, err);
+          double v = ((el + vw) + hb) + sl;
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+          if (lane == 0) s.red[warp * 8] = v;
+        }
+        __syncthreads();
+        double epair = 0.0;
+        for (int k = 0; k < kWarps; ++k) epair += s.red[k * 8];
+        const double etor_new = (etor - cur.eold) + cur.enew;
+        const double enw = epair + etor_new;
+        const double d2 =
+            __dsub_rn(__dsub_rn(weight(w, beta, enw), weight(w, beta, eol)), d1);
+        int up = 1;
+        if (d2 > 0.0) {
+          up = mh_accept(s, head, d2);
           head += 1;
         }
-        if (!pass) {   // rejected without the exact energy
-          __syncthreads();
+        __syncthreads();   // every thread has read s.red and the queue
+        if (up) {
+          eol = enw;
+          etor = etor_new;
+          s_cur = s_new;
+          ++nacc;
+          if (!plain) ++n2;
+          if (threadIdx.x == 0) {
+            s.et[cur.jv] = cur.enew;
+            float sn, cs;
+            sincosf((float)cur.vnew, &sn, &cs);
+            s.daf[2 * cur.ivar] = bf16_round(sn);
+            s.daf[2 * cur.ivar + 1] = bf16_round(cs);
+          }
+        } else {
+          for (int t = threadIdx.x; t < nmoved; t += blockDim.x) {
+            const int k = moved_atom(t, lo, span, flip);
+            if (flip && (k == cur.a || k == cur.b)) continue;
+            s.x[k] = s.bx[k];
+            s.y[k] = s.by[k];
+            s.z[k] = s.bz[k];
+            if (F32) f32_copy(s, k);
+          }
           if (threadIdx.x == 0) s.vlvr[cur.jv] = cur.vold;
-          __syncthreads();
-          continue;
         }
-        ++n1;
-      }
-      // ---- stage 2: exact energy of the proposal
-      const int lo = m.var_lo[cur.jv], hi = m.var_hi[cur.jv];
-      const bool flip = lo <= m.i3 && m.i3 <= hi;
-      const int span = hi - lo + 1;
-      const int nmoved = flip ? m.natoms - span : span;
-      {
-        const double sth = flip ? -cur.sth : cur.sth;
-        double px = s.x[cur.b], py = s.y[cur.b], pz = s.z[cur.b];
-        double kx = px - s.x[cur.a], ky = py - s.y[cur.a], kz = pz - s.z[cur.a];
-        double inv = rsqrt(kx * kx + ky * ky + kz * kz);
-        kx *= inv;
-        ky *= inv;
-        kz *= inv;
-        __syncthreads();   // every thread has read the axis
-        for (int t = threadIdx.x; t < nmoved; t += blockDim.x) {
-          const int k = moved_atom(t, lo, span, flip);
-          if (flip && (k == cur.a || k == cur.b)) continue;
-          double vx = s.x[k] - px, vy = s.y[k] - py, vz = s.z[k] - pz;
-          s.bx[k] = s.x[k];
-          s.by[k] = s.y[k];
-          s.bz[k] = s.z[k];
-          double kd = kx * vx + ky * vy + kz * vz;
-          double cx = ky * vz - kz * vy, cy = kz * vx - kx * vz, cz = kx * vy - ky * vx;
-          double f = kd * (1.0 - cur.cth);
-          s.x[k] = px + vx * cur.cth + cx * sth + kx * f;
-          s.y[k] = py + vy * cur.cth + cy * sth + ky * f;
-          s.z[k] = pz + vz * cur.cth + cz * sth + kz * f;
-          if (F32) f32_copy(s, k);
+        if (!isfinite(enw) && threadIdx.x == 0) set_err(err, kErrNonFinite);
+        __syncthreads();
+        // the dihedral state follows the variables (the setvar of energy())
+        setvar_all(m, s);
+        __syncthreads();
+        if (up) {   // the state changed: the batch's later proposals are stale
+          next = p + j + 1;
+          break;
         }
       }
-      __syncthreads();
-      {
-        double el = 0.0, vw = 0.0, hb = 0.0, sl = 0.0;
-        if (ROWS && m.rows)
-          pair_rows<F32, true>(set.f, m, s, kWarps, el, vw, hb);
-        else
-          pair_energy<F32, false>(set.f, m, s, threadIdx.x, blockDim.x, el, vw, hb);
-        if (SASA) sl = sasa_energy(set.f, m, s, 0, kWarps, err);
-        double v = ((el + vw) + hb) + sl;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0) s.red[warp * 8] = v;
-      }
-      __syncthreads();
-      double epair = 0.0;
-      for (int k = 0; k < kWarps; ++k) epair += s.red[k * 8];
-      const double etor_new = (etor - cur.eold) + cur.enew;
-      const double enw = epair + etor_new;
-      const double d2 =
-          __dsub_rn(__dsub_rn(weight(w, beta, enw), weight(w, beta, eol)), d1);
-      int up = 1;
-      if (d2 > 0.0) {
-        up = mh_accept(s, head, d2);
-        head += 1;
-      }
-      __syncthreads();   // every thread has read s.red and the queue
-      if (up) {
-        eol = enw;
-        etor = etor_new;
-        s_cur = s_new;
-        ++nacc;
-        if (!plain) ++n2;
-        if (threadIdx.x == 0) {
-          s.et[cur.jv] = cur.enew;
-          float sn, cs;
-          sincosf((float)cur.vnew, &sn, &cs);
-          s.daf[2 * cur.ivar] = bf16_round(sn);
-          s.daf[2 * cur.ivar + 1] = bf16_round(cs);
-        }
-      } else {
-        for (int t = threadIdx.x; t < nmoved; t += blockDim.x) {
-          const int k = moved_atom(t, lo, span, flip);
-          if (flip && (k == cur.a || k == cur.b)) continue;
-          s.x[k] = s.bx[k];
-          s.y[k] = s.by[k];
-          s.z[k] = s.bz[k];
-          if (F32) f32_copy(s, k);
-        }
-        if (threadIdx.x == 0) s.vlvr[cur.jv] = cur.vold;
-      }
-      if (!isfinite(enw) && threadIdx.x == 0) set_err(err, kErrNonFinite);
-      __syncthreads();
-      // the dihedral state follows the variables (the setvar of energy())
-      setvar_all(m, s);
-      __syncthreads();
+      p = next;
     }
     // ---- closing energy() and consistency check (metropolis.f:172-179)
     setvar_all(m, s);

@@ -248,6 +248,13 @@ __global__ void k_adam(size_t n, float* __restrict__ P, const float* __restrict_
   }
 }
 
+// dst[n][k] = bf16(src[k][n]) for a [K][256] FP32 matrix.
+__global__ void k_transpose_bf16(int K, const float* __restrict__ src, bf16* __restrict__ dst) {
+  const int n = blockIdx.x, k0 = threadIdx.x;
+  for (int k = k0; k < K; k += blockDim.x)
+    dst[(size_t)n * K + k] = __float2bfloat16(src[(size_t)k * kHidden + n]);
+}
+
 __global__ void k_to_bf16(size_t n, const float* __restrict__ src, bf16* __restrict__ dst) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)
@@ -313,7 +320,7 @@ Surrogate::Surrogate(int nang, uint64_t seed) : nang_(nang), L_(2 * nang) {
 }
 
 Surrogate::~Surrogate() {
-  for (void* q : {(void*)P_, (void*)G_, (void*)M_, (void*)V_, (void*)Wb_, (void*)loss_,
+  for (void* q : {(void*)P_, (void*)G_, (void*)M_, (void*)V_, (void*)Wb_, (void*)Wt_, (void*)loss_,
                   (void*)ang_, (void*)tgt_, (void*)X_, (void*)H1_, (void*)H2_, (void*)H3_,
                   (void*)dA_, (void*)dB_, (void*)Z1_, (void*)Z2_, (void*)Z3_, (void*)y_,
                   (void*)dy_, (void*)tbuf_, (void*)abuf_, (void*)idx_})
@@ -502,8 +509,21 @@ void Surrogate::set_params(const float* in) {
   sync();
 }
 
-DSurrogate Surrogate::device_view() const {
+DSurrogate Surrogate::device_view() {
+  const int H = kHidden;
+  if (!Wt_) Wt_ = dmalloc<bf16>((size_t)L_.nin_pad * H + 2 * (size_t)H * H);
+  bf16* w1t = Wt_;
+  bf16* w2t = w1t + (size_t)L_.nin_pad * H;
+  bf16* w3t = w2t + (size_t)H * H;
+  k_transpose_bf16<<<H, 256, 0, stream_>>>(L_.nin_pad, P_ + L_.w1, w1t);
+  k_transpose_bf16<<<H, 256, 0, stream_>>>(H, P_ + L_.w2, w2t);
+  k_transpose_bf16<<<H, 256, 0, stream_>>>(H, P_ + L_.w3, w3t);
+  check_cuda(cudaGetLastError(), "surrogate transpose");
+  sync();
   DSurrogate d;
+  d.w1t = w1t;
+  d.w2t = w2t;
+  d.w3t = w3t;
   d.w1 = Wb_ + wb1_;
   d.w2 = Wb_ + wb2_;
   d.w3 = Wb_ + wb3_;

@@ -57,7 +57,8 @@ class Surrogate {
   void set_norm(float mu, float sigma) { mu_ = mu, sigma_ = sigma; }
   float mu() const { return mu_; }
   float sigma() const { return sigma_; }
-  DSurrogate device_view() const;
+  // Device view for the sweep kernels (builds the transposed weight copies).
+  DSurrogate device_view();
   // Forward pass that allocates nothing (for callers that cannot allocate
   // device memory): device-resident inputs and outputs, scratch in a fixed
   // file-scope device array (kNoAllocScratchBytes).  See surrogate.cu.
@@ -80,6 +81,7 @@ class Surrogate {
   // parameters: FP32 master, Adam moments, gradients, BF16 copies of weights
   float *P_ = nullptr, *G_ = nullptr, *M_ = nullptr, *V_ = nullptr;
   __nv_bfloat16* Wb_ = nullptr;   // W1 | W2 | W3 | w4
+  __nv_bfloat16* Wt_ = nullptr;   // W1^T | W2^T | W3^T ([256][K] each)
   size_t wb1_ = 0, wb2_ = 0, wb3_ = 0, wb4_ = 0, nwb_ = 0;
   long long step_ = 0;
   // training set
