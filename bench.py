@@ -428,6 +428,9 @@ def run_ours(args, rank, world):
                      "bytes_per_launch": bytes_per_launch},
         "clocks": clk.summary(),
     }
+    if wl.name == "pt_enkefa64" and not args.no_surrogate:
+        line["plain_single_replica"] = single_replica(mols[0], spp, stream)
+        line["surrogate"] = surrogate_leg(ens, mols[0], betas, spp, stream, flush)
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(wl, files)
     if world > 1:
@@ -435,6 +438,112 @@ def run_ours(args, rank, world):
         torch.distributed.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def single_replica(mol, spp, stream):
+    """The plain method on one replica (one chain, same kernel): the GPU
+    baseline the batched throughput is compared with."""
+    import torch
+    from smmp.ensemble import Ensemble
+    one = Ensemble([mol], [0], [31433], [1.0 / (300.0 * GAS)], fp32=True)
+    one.set_stream(stream.cuda_stream)
+    one.random_start()
+    one.sweeps(20)
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    n = 400
+    t0.record(stream)
+    for _ in range(n // spp):
+        one.sweeps(spp)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    return {"value": n / (t0.elapsed_time(t1) / 1000.0), "unit": "sweeps/s",
+            "config": "1 chain, 300 K, same kernel, %d sweeps per launch" % spp}
+
+
+def surrogate_leg(ens, mol, betas, spp, stream, flush):
+    """Train the energy surrogate on the run's own PT states and time the
+    delayed-acceptance sweeps (surrogate first stage, exact second stage).
+    Training time is reported separately, as the metric asks."""
+    import numpy as np
+    import torch
+    from smmp.ensemble import Ensemble
+    from smmp.surrogate import Surrogate, collect_samples
+    nch = len(betas)
+    t0 = time.time()
+    ang, e = collect_samples(ens, mol, 500)                  # 32,000 states
+    t_collect = time.time() - t0
+    # FP64 labels from the GPU's FP64 energy kernel (parity-tested against the
+    # FP64 oracle to 1e-10); the sampler's own energies are FP32-pair sums
+    lab = Ensemble([mol], [0] * len(e), [1] * len(e), [1.0] * len(e))
+    V = np.zeros((len(e), lab.vstride))
+    V[:] = ens.vlvr()[0]
+    V[:, mol.idvr] = ang
+    lab.set_vlvr(V)
+    e64 = lab.energy()
+    del lab
+    rng = np.random.default_rng(0)
+    order = rng.permutation(len(e))
+    nt = len(e) // 10
+    test, train = order[:nt], order[nt:]
+    clip = float(np.percentile(e64, 99))
+    sur = Surrogate(mol.nvr, seed=2)
+    sur.set_data(ang[train], e64[train], clip=clip)
+    epochs, batch = 40, 512
+    torch.cuda.synchronize()
+    t0 = time.time()
+    sur.train(epochs, batch=batch, lr=1e-3)
+    t_train = time.time() - t0
+    pred = sur.predict(ang[test])
+    keep = e64[test] < clip
+    rmse = float(np.sqrt(np.mean((pred[keep] - e64[test][keep]) ** 2)))
+    flops = 3 * 2 * (2 * mol.nvr * 256 + 2 * 256 * 256 + 256) * (len(train) // batch) * batch * epochs
+    peak = 1590.0
+    if os.path.exists(PEAKS):
+        try:
+            peak = float(json.load(open(PEAKS))["bf16_tflops"])
+        except Exception:
+            pass
+    out = {"train_states": int(len(train)), "collect_s": t_collect, "train_s": t_train,
+           "epochs": epochs, "batch": batch,
+           "heldout_rmse_kcal": rmse, "heldout_energy_std_kcal": float(e64[test][keep].std()),
+           "labels": "FP64 GPU energies (parity-tested to 1e-10 against the FP64 oracle)",
+           "train_roofline": {"bound": "tensor", "achieved": flops / t_train / 1e12, "peak": peak,
+                              "unit": "TFLOP/s", "frac": flops / t_train / 1e12 / peak}}
+    # delayed-acceptance PT sweeps on the same replicas, timed like the plain arm
+    res = {}
+    for mode in ("plain", "delayed"):
+        ens.set_surrogate(sur if mode == "delayed" else None, floor=0.2, min_stage1=64)
+        ens.pt_sweeps(spp, graph_chunk=spp)
+        a0, p0 = ens.acceptance()
+        s0 = ens.da_stats()
+        k = 20
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ms = 0.0
+        for _ in range(k):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                ev0.record(stream)
+            ens.pt_sweeps(spp, graph_chunk=spp)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            ms += ev0.elapsed_time(ev1)
+        a, p = ens.acceptance()
+        s1 = ens.da_stats()
+        accepted = float((a - a0).sum())
+        exact = float((s1[0] - s0[0]).sum()) if mode == "delayed" else float((p - p0).sum())
+        res[mode] = {"value": nch * spp * k / (ms / 1000.0), "unit": "sweeps/s",
+                     "acceptance": accepted / float((p - p0).sum()),
+                     "exact_evaluations_per_accepted_move": exact / max(accepted, 1.0)}
+        if mode == "delayed":
+            res[mode]["stage1_pass"] = float((s1[0] - s0[0]).sum()) / float((p - p0).sum())
+            res[mode]["stage2_acceptance"] = float((s1[1] - s0[1]).sum()) / max(
+                float((s1[0] - s0[0]).sum()), 1.0)
+    ens.set_surrogate(None)
+    out["pt_plain"] = res["plain"]
+    out["pt_delayed_acceptance"] = res["delayed"]
+    return out
 
 
 def run_reference(args, rank, world):
@@ -485,6 +594,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="pt_enkefa64", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-surrogate", action="store_true",
+                    help="skip the surrogate training / delayed-acceptance leg")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", 0))
