@@ -952,6 +952,19 @@ int smmp_ens_set_surrogate(smmp_ens_t* e, smmp_sur_t* s, double floor, int min_s
   });
 }
 
+int smmp_ens_autotune(smmp_ens_t* e, int* choice, double* ms) {
+  return guard([&] {
+    need(e != nullptr, "NULL ensemble");
+    double t[2];
+    int c = e->e->autotune(e->flags & (kFlagFP32 | kFlagRndOrd), t);
+    if (choice) *choice = c;
+    if (ms) {
+      ms[0] = t[0];
+      ms[1] = t[1];
+    }
+  });
+}
+
 int smmp_ens_da_stats(smmp_ens_t* e, uint64_t* stage1, uint64_t* stage2) {
   return guard([&] {
     need(e && stage1 && stage2, "NULL argument");

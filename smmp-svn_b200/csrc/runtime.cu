@@ -150,16 +150,19 @@ DeviceSet::DeviceSet(const std::vector<std::shared_ptr<Molecule>>& mols) {
       d.near_mask = upload(nm);
       d.near14 = upload(n14);
     }
-    // Row-form pair sums pay off from about a hundred atoms on; smaller
-    // molecules keep the chunk lists (measured: Met-enkephalin, 75 atoms,
-    // is faster with lists; Ace-Ala40-NMe, 412 atoms, with rows).
+    // Default pair-work form before any autotuning: rows from about a
+    // hundred atoms on (measured: Met-enkephalin, 75 atoms, is faster with
+    // the chunk lists; Ace-Ala40-NMe, 412 atoms, with rows).
     d.rows = (t.rows_ok && t.natoms >= 128) ? 1 : 0;
+    rows_ok_.push_back(t.rows_ok ? 1 : 0);
     dm.push_back(d);
     max_atoms = std::max(max_atoms, t.natoms);
     max_vars = std::max(max_vars, t.nvar);
   }
   DMol* dmols = dalloc<DMol>(allocs_, dm.size());
   h2d(dmols, dm);
+  dmols_ = dmols;
+  dm_ = dm;
   set_.mols = dmols;
   set_.nmols = (int)dm.size();
   set_.max_atoms = max_atoms;
@@ -171,6 +174,28 @@ DeviceSet::DeviceSet(const std::vector<std::shared_ptr<Molecule>>& mols) {
   set_.da = 0;
   with_lists_ = without_ = 0;
   for (const DMol& d : dm) {
+    with_lists_ = std::max(with_lists_, stage_bytes_of(d, true));
+    without_ = std::max(without_, stage_bytes_of(d, false));
+  }
+  size_staging();
+}
+
+int DeviceSet::any_rows_possible() const {
+  int any = 0;
+  for (int r : rows_ok_) any |= r;
+  return any;
+}
+
+void DeviceSet::set_rows(int mode) {
+  for (size_t k = 0; k < dm_.size(); ++k) {
+    const bool big = dm_[k].natoms >= 128;
+    dm_[k].rows = rows_ok_[k] && (mode == 1 || (mode < 0 && big)) ? 1 : 0;
+  }
+  h2d(dmols_, dm_);
+  set_.any_rows = 0;
+  for (const DMol& d : dm_) set_.any_rows |= d.rows;
+  with_lists_ = without_ = 0;
+  for (const DMol& d : dm_) {
     with_lists_ = std::max(with_lists_, stage_bytes_of(d, true));
     without_ = std::max(without_, stage_bytes_of(d, false));
   }
@@ -313,6 +338,77 @@ void Ensemble::set_surrogate(const DSurrogate* view, float floor, int min_stage1
   if (graph_) cudaGraphExecDestroy(graph_);   // kernel arguments changed
   graph_ = nullptr;
   graph_len_ = 0;
+}
+
+// Autotuner: time one sweep of every chain with each pair-work form (chunk
+// lists; 32-partner row passes) from the same saved state, keep the faster,
+// and put the state back.  The timed sweeps leave no trace.
+int Ensemble::autotune(int flags, double* ms_out) {
+  if (!dev_->any_rows_possible()) {
+    if (ms_out) ms_out[0] = ms_out[1] = 0.0;
+    return 0;
+  }
+  check_cuda(cudaStreamSynchronize(stream_), "autotune sync");
+  const size_t nv = (size_t)n_ * ch_.vstride, nt = (size_t)ntoat_ * ch_.tstride,
+               nm = (size_t)nmt_ * kMTWords;
+  std::vector<double> v, t, e, tr;
+  std::vector<uint32_t> mt;
+  std::vector<unsigned long long> a, p, d1, d2;
+  std::vector<int> er;
+  d2h(v, ch_.vlvr, nv);
+  d2h(t, ch_.toat, nt);
+  d2h(mt, ch_.mt, nm);
+  d2h(e, ch_.eol, n_);
+  d2h(tr, ch_.terms, (size_t)n_ * 6);
+  d2h(a, ch_.nacc, n_);
+  d2h(p, ch_.nprop, n_);
+  d2h(d1, ch_.da_n1, n_);
+  d2h(d2, ch_.da_n2, n_);
+  d2h(er, ch_.err, n_);
+  auto restore = [&] {
+    h2d(ch_.vlvr, v);
+    h2d(ch_.toat, t);
+    h2d(ch_.mt, mt);
+    h2d(ch_.eol, e);
+    h2d(ch_.terms, tr);
+    h2d(ch_.nacc, a);
+    h2d(ch_.nprop, p);
+    h2d(ch_.da_n1, d1);
+    h2d(ch_.da_n2, d2);
+    h2d(ch_.err, er);
+  };
+  DWeight w{kWeightCanon, 0, 0, 1.0, nullptr, nullptr};
+  cudaEvent_t e0, e1;
+  check_cuda(cudaEventCreate(&e0), "event");
+  check_cuda(cudaEventCreate(&e1), "event");
+  double ms[2] = {0.0, 0.0};
+  for (int mode = 0; mode < 2; ++mode) {
+    dev_->set_rows(mode);
+    restore();
+    launch_sweep_range(0, n_, 1, flags | kFlagNoCheck, w);   // warm-up
+    check_cuda(cudaStreamSynchronize(stream_), "autotune sync");
+    restore();
+    check_cuda(cudaEventRecord(e0, stream_), "event");
+    launch_sweep_range(0, n_, 1, flags | kFlagNoCheck, w);
+    check_cuda(cudaEventRecord(e1, stream_), "event");
+    check_cuda(cudaEventSynchronize(e1), "event sync");
+    float f = 0.f;
+    check_cuda(cudaEventElapsedTime(&f, e0, e1), "event time");
+    ms[mode] = f;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  const int best = ms[1] < ms[0] ? 1 : 0;
+  dev_->set_rows(best);
+  restore();
+  if (graph_) cudaGraphExecDestroy(graph_);   // kernel arguments changed
+  graph_ = nullptr;
+  graph_len_ = 0;
+  if (ms_out) {
+    ms_out[0] = ms[0];
+    ms_out[1] = ms[1];
+  }
+  return best;
 }
 
 void Ensemble::da_stats(std::vector<unsigned long long>& n1,

@@ -42,10 +42,17 @@ class DeviceSet {
   const DMolSet& set() const { return set_; }
   // reserve shared memory for the surrogate's first stage (re-sizes staging)
   void set_da(bool on);
+  // pair-work form of the molecules that allow rows: 0 chunk lists, 1 rows,
+  // -1 the size-based default
+  void set_rows(int mode);
+  int any_rows_possible() const;
 
  private:
   void size_staging();
   size_t with_lists_ = 0, without_ = 0;
+  std::vector<DMol> dm_;
+  std::vector<int> rows_ok_;
+  DMol* dmols_ = nullptr;
   template <class T>
   const T* upload(const std::vector<T>& v);
   std::vector<void*> allocs_;
@@ -82,6 +89,10 @@ class Ensemble {
   // device memory must outlive its use here.
   void set_surrogate(const DSurrogate* view, float floor, int min_stage1);
   void da_stats(std::vector<unsigned long long>& n1, std::vector<unsigned long long>& n2) const;
+  // Autotuner: times one sweep of all chains with each pair-work form (chunk
+  // lists / row passes) from the same saved state, keeps the faster and
+  // restores the state.  Returns 1 when rows won; ms_out[2] the two times.
+  int autotune(int flags, double* ms_out);
   cudaStream_t stream() const { return stream_; }
   const DChains& chains() const { return ch_; }
   const DMolSet& set() const { return dev_->set(); }

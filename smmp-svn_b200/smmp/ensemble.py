@@ -196,6 +196,15 @@ class Ensemble:
         check(lib.smmp_ens_set_surrogate(self._h, surrogate._h if surrogate else None,
                                          float(floor), int(min_stage1)))
 
+    def autotune(self):
+        """Pick the faster pair-work decomposition (chunk lists or row
+        passes) by timing one sweep of each from the same saved state; the
+        state is restored.  Returns (rows_won, (ms_lists, ms_rows))."""
+        choice = ctypes.c_int()
+        ms = (ctypes.c_double * 2)()
+        check(lib.smmp_ens_autotune(self._h, ctypes.byref(choice), ms))
+        return bool(choice.value), (ms[0], ms[1])
+
     def da_stats(self):
         """(stage-1 passes, stage-2 accepts) per chain."""
         a = np.zeros(self.nchains, dtype=np.uint64)

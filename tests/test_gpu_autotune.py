@@ -1,0 +1,50 @@
+"""The autotuner: it times both pair-work decompositions from a saved state,
+keeps the faster, and leaves the ensemble's state (variables, energies,
+random streams, counters) exactly as it found it."""
+import numpy as np
+import pytest
+
+from conftest import DATA, Oracle, seqfile
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("n", [6, 40])
+def test_autotune_leaves_no_trace_and_keeps_parity(tmp_path, n):
+    from smmp.ensemble import Ensemble, Molecule, beta_of
+    from smmp.sequences import polyala
+    f = seqfile(tmp_path, polyala(n), "ala%d" % n)
+    mol = Molecule(f, libdir=DATA)
+    b = beta_of(300.0)
+    ens = Ensemble([mol], [0] * 16, [40 + c for c in range(16)], [b] * 16, fp32=True)
+    twin = Ensemble([mol], [0] * 16, [40 + c for c in range(16)], [b] * 16, fp32=True)
+    for e in (ens, twin):
+        e.random_start()
+        e.sweeps(5)
+    v0, e0 = ens.vlvr(), ens.energies()
+    a0, p0 = ens.acceptance()
+    rows, (ms_lists, ms_rows) = ens.autotune()
+    assert np.array_equal(ens.vlvr(), v0) and np.array_equal(ens.energies(), e0)
+    a1, p1 = ens.acceptance()
+    assert np.array_equal(a0, a1) and np.array_equal(p0, p1)
+    assert ms_lists > 0 and ms_rows > 0
+    assert rows == (ms_rows < ms_lists)
+    # the random streams were restored: the next draws equal the twin's
+    assert np.array_equal(ens.draw(3, 50), twin.draw(3, 50))
+    ens.sweeps(5)
+    assert not ens.errors().any()
+    o = Oracle(f)
+    V = ens.vlvr()
+    E = ens.energies()
+    for c in (0, 7, 15):
+        o.set_vlvr(V[c, :o.ntlvr])
+        e, _ = o.energy()
+        assert abs(E[c] - e) <= max(1e-2, 1e-7 * abs(e))
+
+
+def test_autotune_without_row_form_is_a_no_op():
+    from smmp.ensemble import Ensemble, Molecule, beta_of
+    mol = Molecule(DATA + "enkefa.seq", DATA + "enkefa.var", libdir=DATA)
+    ens = Ensemble([mol], [0] * 4, [1, 2, 3, 4], [beta_of(300.0)] * 4, fp32=True)
+    rows, ms = ens.autotune()
+    assert rows in (False, True)
