@@ -1728,42 +1728,62 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep_da(DMolSet set, DChains c
 // Replica exchange (partem_s.f:210-232): alternate even/odd neighbour pairs,
 // replica num_rep pairs with 1 when `wrap` is set.  temp_chain[k] is the chain
 // at temperature label k (ipoi); betas[k] the inverse temperature of label k.
-__global__ void k_exchange(DChains ch, int* temp_chain, const double* betas, int n,
-                           uint32_t* mt, int* iswitch, int wrap, unsigned long long* stats) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// One warp: the pairs of one parity step are disjoint, so lane k decides the
+// k-th pair with the k-th uniform of the exchange stream (the order in which
+// the reference's loop draws them); the stream slot is worked on in shared
+// memory and written back.
+__global__ void __launch_bounds__(32) k_exchange(DChains ch, int* temp_chain, const double* betas,
+                                                 int n, uint32_t* mt, int* iswitch, int wrap,
+                                                 unsigned long long* stats) {
+  __shared__ uint32_t slot[kMTWords];
+  __shared__ double lq[kQueue];
+  const int lane = threadIdx.x;
+  if (blockIdx.x != 0) return;
   if (n > 1) {
-    int num_rep1, nu;
-    if (*iswitch == 1) {
-      num_rep1 = n - 1;
-      nu = 1;
-      *iswitch = 2;
-    } else {
-      num_rep1 = n;
-      nu = 2;
-      *iswitch = 1;
-    }
-    for (int i = nu; i <= num_rep1; i += 2) {
-      int j = i + 1;
-      if (i == n) {
-        if (!wrap) continue;
-        j = 1;
+    for (int k = lane; k < kMTWords; k += 32) slot[k] = mt[k];
+    __syncwarp();
+    const int sw = *iswitch;
+    const int num_rep1 = sw == 1 ? n - 1 : n, nu = sw == 1 ? 1 : 2;
+    // pairs i = nu, nu+2, ..., num_rep1 (1-based); i == n is the wrap pair
+    int npairs = 0;
+    for (int i = nu; i <= num_rep1; i += 2)
+      if (i != n || wrap) ++npairs;
+    uint32_t head = slot[kQHead];
+    for (int base = 0; base < npairs; base += 32) {
+      const int cnt = min(32, npairs - base);
+      while ((int)(slot[kQTail] - head) < cnt) rng_refill_warp(slot, lq);   // < 32 before: fits
+      __syncwarp();
+      if (lane < cnt) {
+        const int i = nu + 2 * (base + lane);   // the wrap pair, if any, is the last
+        int j = i + 1;
+        if (i == n) j = 1;
+        const int in = temp_chain[i - 1], jn = temp_chain[j - 1];
+        const double bi = betas[i - 1], bj = betas[j - 1];
+        const double ein = ch.eol[in], ejn = ch.eol[jn];
+        double delta = __dsub_rn(-__dmul_rn(bi, ejn), __dmul_rn(bj, ein));
+        delta = __dadd_rn(delta, __dmul_rn(bi, ein));
+        delta = __dadd_rn(delta, __dmul_rn(bj, ejn));
+        const double ra = qbuf(slot)[(head + lane) & (kQueue - 1)];
+        stats[2 * (i - 1)] += 1;
+        if (ra <= exp(delta)) {
+          temp_chain[i - 1] = jn;
+          temp_chain[j - 1] = in;
+          stats[2 * (i - 1) + 1] += 1;
+        }
       }
-      int in = temp_chain[i - 1], jn = temp_chain[j - 1];
-      double bi = betas[i - 1], bj = betas[j - 1];
-      double ein = ch.eol[in], ejn = ch.eol[jn];
-      double delta = __dsub_rn(-__dmul_rn(bi, ejn), __dmul_rn(bj, ein));
-      delta = __dadd_rn(delta, __dmul_rn(bi, ein));
-      delta = __dadd_rn(delta, __dmul_rn(bj, ejn));
-      double ra = stream_next(mt);
-      stats[2 * (i - 1)] += 1;
-      if (ra <= exp(delta)) {
-        temp_chain[i - 1] = jn;
-        temp_chain[j - 1] = in;
-        stats[2 * (i - 1) + 1] += 1;
-      }
+      head += cnt;
+      __syncwarp();
     }
+    if (lane == 0) {
+      slot[kQHead] = head;
+      *iswitch = sw == 1 ? 2 : 1;
+    }
+    __syncwarp();
+    for (int k = lane; k < kMTWords; k += 32) mt[k] = slot[k];
+    __threadfence_block();
+    __syncwarp();
   }
-  for (int k = 0; k < n; ++k) ch.beta[temp_chain[k]] = betas[k];
+  for (int k = lane; k < n; k += 32) ch.beta[temp_chain[k]] = betas[k];
 }
 
 // ============================================================================ host wrappers
@@ -1879,7 +1899,7 @@ cudaError_t launch_sweep(const DMolSet& set, const DChains& ch, const DWeight& w
 cudaError_t launch_exchange(const DChains& ch, int* temp_chain, const double* betas, int n,
                             uint32_t* mt, int* iswitch, int wrap, unsigned long long* stats,
                             cudaStream_t st) {
-  k_exchange<<<1, 1, 0, st>>>(ch, temp_chain, betas, n, mt, iswitch, wrap, stats);
+  k_exchange<<<1, 32, 0, st>>>(ch, temp_chain, betas, n, mt, iswitch, wrap, stats);
   return cudaGetLastError();
 }
 
