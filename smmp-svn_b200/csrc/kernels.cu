@@ -158,6 +158,7 @@ struct Scalars {
   Proposal cur;
   Proposal spec[2];      // next proposal if this one draws 1 (spec[0]) or 2 (spec[1]) numbers
   int refill;
+  int hlo, hhi;          // heavy-atom indices of the proposal's subtree range
 };
 
 struct Smem {
@@ -180,6 +181,8 @@ struct Smem {
   float4* nbf;           // SASA neighbours per warp: (dx, dy, dz, rb2) in FP32
   int* nbj;              // and their atom index (for the exact FP64 re-test)
   int* sq;               // SASA neighbour candidates per warp (kSasaQueue)
+  double* sae;           // SASA: each heavy atom's term in the current state
+  double* san;           // SASA: each heavy atom's term for the proposal
   Scalars* sc;
   float* daf;            // surrogate: features (sin/cos, BF16-rounded) of the state
   __nv_bfloat16* dfe;    // surrogate: feature rows of a batch [16][kDaStride(nin_pad)]
@@ -238,6 +241,8 @@ __host__ __device__ inline size_t smem_layout(int n, int v, int npnt, bool sasa,
   t.nbf = (float4*)take(sasa ? 16 * kWarps * kMaxNeighbours : 16);
   t.nbj = (int*)take(sasa ? 4 * kWarps * kMaxNeighbours : 4);
   t.sq = (int*)take(sasa ? 4 * kWarps * kSasaQueue : 4);
+  t.sae = (double*)take(sasa ? 8 * (size_t)(n > 0 ? n : 1) : 8);
+  t.san = (double*)take(sasa ? 8 * (size_t)(n > 0 ? n : 1) : 8);
   const size_t fpad = ((size_t)2 * (v > 0 ? v : 1) + 15) / 16 * 16 + 8;   // row stride
   t.daf = (float*)take(da ? 4 * 2 * (size_t)(v > 0 ? v : 1) : 4);
   t.dfe = (__nv_bfloat16*)take(da ? 2 * 16 * fpad : 16);
@@ -828,8 +833,25 @@ __device__ __forceinline__ bool sasa_buried(double s0, double s1, double s2, dou
 
 constexpr float kSasaMargin = 1e-4f;
 
+// Incremental SASA of a proposal.  Only the proposal's moved atoms change
+// position; a heavy atom that did not move and has no moved heavy atom among
+// its neighbour candidates before or after the move (pre-test on the new and
+// the backed-up positions) keeps its neighbours and their positions, hence
+// its exposed-point count: its term is taken from `cache` instead of being
+// recounted.  Terms are written to `out` (per heavy atom) when it is set.
+struct SasaInc {
+  const double* cache;   // nullptr: count every atom
+  double* out;
+  int lo, span, a, b;
+  bool flip;
+  int hlo, hhi;          // heavy-atom indices with atom index in [lo, lo + span)
+  __device__ __forceinline__ bool moved(int j) const {
+    return flip ? ((j < lo || j >= lo + span) && j != a && j != b) : (j >= lo && j < lo + span);
+  }
+};
+
 __device__ double sasa_energy(const FFScalars& ff, const DMol& m, Smem& s, int w0, int nw,
-                              int* err) {
+                              int* err, const SasaInc& inc = SasaInc{nullptr, nullptr, 0, 0, 0, 0, false, 0, 0}) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   float4* nbf = s.nbf + (size_t)warp * kMaxNeighbours;
   int* nbj = s.nbj + (size_t)warp * kMaxNeighbours;
@@ -855,6 +877,31 @@ __device__ double sasa_energy(const FFScalars& ff, const DMol& m, Smem& s, int w
       }
       nn += __popc(mask);
     };
+    if (inc.cache != nullptr && !inc.moved(i)) {
+      // is a moved heavy atom a neighbour candidate, before or after the move?
+      bool touched = false;
+      const int inner = inc.hhi - inc.hlo;
+      const int nmv = inc.flip ? m.nheavy - inner : inner;
+      for (int t = lane; t < nmv; t += 32) {
+        const int hj = inc.flip ? (t < inc.hlo ? t : t + inner) : inc.hlo + t;
+        const int j = m.heavy[hj];
+        if (inc.flip && (j == inc.a || j == inc.b)) continue;
+        const double lim = trad + m.rvdw[j];
+        const double l2 = lim * lim * 1.0000001 + 1e-12;
+        const double ex = xi - s.x[j], ey = yi - s.y[j], ez = zi - s.z[j];
+        const double ox = xi - s.bx[j], oy = yi - s.by[j], oz = zi - s.bz[j];
+        touched = touched || ex * ex + ey * ey + ez * ez <= l2 || ox * ox + oy * oy + oz * oz <= l2;
+      }
+      if (!__any_sync(0xffffffffu, touched)) {   // unchanged: the cached term
+        if (lane == 0) {
+          const double tv = inc.cache[h];
+          eysl += tv;
+          if (inc.out) inc.out[h] = tv;
+        }
+        __syncwarp();
+        continue;
+      }
+    }
     for (int base = 0; base < m.nheavy; base += 32) {
       const int hj = base + lane;
       const int j = hj < m.nheavy ? m.heavy[hj] : i;
@@ -937,7 +984,9 @@ __device__ double sasa_energy(const FFScalars& ff, const DMol& m, Smem& s, int w
     if (lane == 0) {
       double sdr = __ddiv_rn(__dmul_rn(__dmul_rn(4.0 * kPi, trad), trad), (double)npnt);
       double area = __dmul_rn(sdr, (double)cnt);
-      eysl += __dmul_rn(area, m.sigma[i]);
+      const double t = __dmul_rn(area, m.sigma[i]);
+      eysl += t;
+      if (inc.out) inc.out[h] = t;
     }
     __syncwarp();
   }
@@ -986,7 +1035,7 @@ __device__ void evaluate_block(const FFScalars& ff, const DMol& m, Smem& s, int*
   double el = 0.0, vw = 0.0, hb = 0.0, sl = 0.0, vr = 0.0;
   pair_energy<F32, ROWS>(ff, m, s, threadIdx.x, blockDim.x, el, vw, hb);
   for (int v = threadIdx.x; v < m.nvar; v += blockDim.x) vr += s.et[v];
-  if (SASA) sl = sasa_energy(ff, m, s, 0, kWarps, err);
+  if (SASA) sl = sasa_energy(ff, m, s, 0, kWarps, err, SasaInc{nullptr, s.sae, 0, 0, 0, 0, false, 0, 0});
   warp_partials(s, el, vw, hb, vr, sl);
 }
 
@@ -1229,6 +1278,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       const bool flip = lo <= m.i3 && m.i3 <= hi;
       const int span = hi - lo + 1;
       const int nmoved = flip ? m.natoms - span : span;
+      if (SASA && threadIdx.x == 0) {   // heavy-atom index range of [lo, hi]
+        int l = 0, r = m.nheavy;
+        while (l < r) {
+          const int mid = (l + r) >> 1;
+          if (m.heavy[mid] < lo) l = mid + 1; else r = mid;
+        }
+        sc.hlo = l;
+        r = m.nheavy;
+        while (l < r) {
+          const int mid = (l + r) >> 1;
+          if (m.heavy[mid] <= hi) l = mid + 1; else r = mid;
+        }
+        sc.hhi = l;
+      }
       // ---- phase A: rotate the subtree of cur.jv about its bond (+theta)
       {
         const double sth = flip ? -cur.sth : cur.sth;
@@ -1263,7 +1326,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
           pair_rows<F32, true>(set.f, m, s, kWarps - 1, el, vw, hb);
         else
           pair_energy<F32, false>(set.f, m, s, threadIdx.x, nthr_pairs, el, vw, hb);
-        if (sasa) sl = sasa_energy(set.f, m, s, 0, kWarps - 1, err);
+        if (sasa)
+          sl = sasa_energy(set.f, m, s, 0, kWarps - 1, err,
+                           SasaInc{s.sae, s.san, lo, span, cur.a, cur.b, flip, sc.hlo, sc.hhi});
         double v = ((el + vw) + hb) + sl;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -1303,6 +1368,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       if (up) {
         eol = enw;
         etor = etor_new;
+        if (sasa)   // the proposal's SASA terms become the state's
+          for (int h = threadIdx.x; h < m.nheavy; h += blockDim.x) s.sae[h] = s.san[h];
       } else {
         for (int t = threadIdx.x; t < nmoved; t += blockDim.x) {
           const int k = moved_atom(t, lo, span, flip);
