@@ -729,6 +729,54 @@ __device__ void pair_rows(const FFScalars& ff, const DMol& m, const Smem& s, int
   }
 }
 
+// Energy of the pairs that cross the partition {lo..hi} | rest (the pairs
+// whose distance a rotation of either side changes), this thread's share, for
+// warps [0, nw): rows i < lo take partners lo..hi, rows i in lo..hi take
+// partners beyond hi (row form: the first 64 partners of a row are masked).
+// A proposal's energy change is this sum after the rotation minus the same
+// sum before it, computed by the same threads over the same pairs.
+template <bool F32>
+__device__ double cross_rows(const FFScalars& ff, const DMol& m, const Smem& s, int nw, int lo,
+                             int hi) {
+  const int lane = threadIdx.x & 31, n = m.natoms;
+  double e64[3] = {0.0, 0.0, 0.0};
+  KSum ke;
+  const float convf = (float)ff.conv;
+  for (int i = (threadIdx.x >> 5); i <= hi && i < n - 1; i += nw) {
+    const int jb = i < lo ? lo : hi + 1;
+    const int je = i < lo ? hi : n - 1;
+    if (jb > je) continue;
+    const unsigned long long nm = m.near_mask[i], n14 = m.near14[i];
+    if (!F32 || ff.epsd) {
+      for (int j = jb + lane; j <= je; j += 32) {
+        const int d = j - i - 1;
+        bool use = true, is14 = false;
+        if (d < 64) {
+          use = (((nm | n14) >> d) & 1ull) != 0;
+          is14 = ((n14 >> d) & 1ull) != 0;
+        }
+        if (use) pair_term<false>(ff, s, i, j, is14, e64[0], e64[1], e64[2]);
+      }
+      continue;
+    }
+    const float4 pi = s.p4[i], li = s.l4[i];
+    const float qi = convf * pi.w;
+    const float4* trow = s.tab4 + __float_as_int(li.w) * kTypes;
+    for (int j0 = jb; j0 <= je; j0 += 32) {
+      const int j = j0 + lane, d = j - i - 1;
+      bool use = j <= je, is14 = false;
+      if (use && d < 64) {
+        use = (((nm | n14) >> d) & 1ull) != 0;
+        is14 = ((n14 >> d) & 1ull) != 0;
+      }
+      float t[3];
+      row_term<true>(ff, s, i, use ? j : jb, use, is14, pi, li, qi, trow, e64, t);
+      ke.add(t[0] + t[1]);
+    }
+  }
+  return ((ke.value() + e64[0]) + e64[1]) + e64[2];
+}
+
 // Pair sums of the threads [0, nthr): by rows when the molecule has the row
 // form (kernels built with ROWS), else vdW chunks (8 partners each) and 1-4
 // pairs from the mklist lists.
@@ -1239,6 +1287,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
   __syncthreads();
   uint32_t head = s.mt[kQHead];   // identical in every thread from here on
   double eol = ch.eol[c], enew = 0.0, etor = 0.0;
+  double ep = 0.0;   // pair energy of the state (row-form molecules: updated by differences)
   bool fresh = false;
 
   for (int sw = 0; sw < nsweeps; ++sw) {
@@ -1259,6 +1308,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       all_sums(s, sum);
       enew = total_of(sum);
       etor = sum[3];
+      ep = (sum[0] + sum[1]) + sum[2];
     }
     eol = enew;
     if (m.nfree > 0 && threadIdx.x == 0) {
@@ -1292,6 +1342,34 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
         }
         sc.hhi = l;
       }
+      // ---- phase A0 (row-form molecules): energy of the pairs across the
+      // rotating bond before the move; after it, phase B computes the same
+      // sum again and the pair energy changes by the difference
+      // (FP32 pair terms only: in FP64 mode every proposal is summed in full,
+      // so that eol carries no accumulated rounding into the reference's
+      // 1e-6 consistency check)
+      const bool incr = ROWS && F32 && m.rows && !set.f.epsd;
+      double xold = 0.0;
+      if (incr && p > 0 && (p & 31) == 0) {
+        // FP32 differences drift: every 32 proposals the pair energy of the
+        // state is summed afresh (same coordinates), which also resets eol
+        double el = 0.0, vw = 0.0, hb = 0.0;
+        pair_rows<F32, true>(set.f, m, s, kWarps, el, vw, hb);
+        double v = el;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) s.red[warp * 8 + 2] = v;
+        __syncthreads();
+        double fresh_ep = 0.0;
+        for (int k = 0; k < kWarps; ++k) fresh_ep += s.red[k * 8 + 2];
+        eol = (eol - ep) + fresh_ep;
+        ep = fresh_ep;
+        __syncthreads();
+      }
+      if (incr) {
+        if (warp != spec_warp) xold = cross_rows<F32>(set.f, m, s, kWarps - 1, lo, hi);
+        __syncthreads();
+      }
       // ---- phase A: rotate the subtree of cur.jv about its bond (+theta)
       {
         const double sth = flip ? -cur.sth : cur.sth;
@@ -1322,17 +1400,25 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       // setvar call on the dihedral state and prepares proposal p+1
       if (warp != spec_warp) {
         double el = 0.0, vw = 0.0, hb = 0.0, sl = 0.0;
-        if (ROWS && m.rows)
+        if (incr)
+          el = cross_rows<F32>(set.f, m, s, kWarps - 1, lo, hi) - xold;   // the change
+        else if (ROWS && m.rows)
           pair_rows<F32, true>(set.f, m, s, kWarps - 1, el, vw, hb);
         else
           pair_energy<F32, false>(set.f, m, s, threadIdx.x, nthr_pairs, el, vw, hb);
         if (sasa)
           sl = sasa_energy(set.f, m, s, 0, kWarps - 1, err,
                            SasaInc{s.sae, s.san, lo, span, cur.a, cur.b, flip, sc.hlo, sc.hhi});
-        double v = ((el + vw) + hb) + sl;
+        double v = (el + vw) + hb;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0) s.red[warp * 8] = v;
+        for (int o = 16; o > 0; o >>= 1) {
+          v += __shfl_xor_sync(0xffffffffu, v, o);
+          sl += __shfl_xor_sync(0xffffffffu, sl, o);
+        }
+        if (lane == 0) {
+          s.red[warp * 8] = v;
+          s.red[warp * 8 + 1] = sl;
+        }
       } else {
         setvar_warp(m, s);
         __syncwarp();
@@ -1342,8 +1428,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       }
       __syncthreads();
       // ---- phase C: every warp sums and decides (metropolis.f:72-87)
-      double epair = 0.0;
-      for (int k = 0; k < kWarps - 1; ++k) epair += s.red[k * 8];
+      double dpair = 0.0, esl = 0.0;
+      for (int k = 0; k < kWarps - 1; ++k) {
+        dpair += s.red[k * 8];
+        esl += s.red[k * 8 + 1];
+      }
+      // pair energy of the proposal: the state's plus the change (row form),
+      // or the full sum
+      const double epair = (incr ? ep + dpair : dpair) + esl;
       // every value read here was written before the last barrier
       const double etor_new = (etor - cur.eold) + cur.enew;
       const double enw = epair + etor_new;
@@ -1368,6 +1460,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       if (up) {
         eol = enw;
         etor = etor_new;
+        if (incr) ep += dpair;
         if (sasa)   // the proposal's SASA terms become the state's
           for (int h = threadIdx.x; h < m.nheavy; h += blockDim.x) s.sae[h] = s.san[h];
       } else {
@@ -1415,6 +1508,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       all_sums(s, sum);
       enew = total_of(sum);
       etor = sum[3];
+      ep = (sum[0] + sum[1]) + sum[2];   // the next sweep starts from this evaluation
       if (threadIdx.x == 0) {
         if (!(flags & kFlagNoCheck) && fabs(eol - enew) > check_tol && eol < 100000.0)
           set_err(err, kErrConsistency);
