@@ -1311,6 +1311,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       ep = (sum[0] + sum[1]) + sum[2];
     }
     eol = enew;
+    const bool relaxed = fabs(eol) < 1e4;
     if (m.nfree > 0 && threadIdx.x == 0) {
       make_proposal(m, s, 0, head, rndord, sc.cur);
       s.vlvr[sc.cur.jv] = sc.cur.vnew;
@@ -1348,11 +1349,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       // (FP32 pair terms only: in FP64 mode every proposal is summed in full,
       // so that eol carries no accumulated rounding into the reference's
       // 1e-6 consistency check)
-      const bool incr = ROWS && F32 && m.rows && !set.f.epsd;
+      // The FP32 differences carry the rounding of the terms they touch, so
+      // they are used only for relaxed states (|E| < 1e4 kcal/mol at the
+      // sweep's start: no clash terms) and the state's pair energy is summed
+      // afresh every 16 proposals (same coordinates; eol follows).
+      const bool incr = ROWS && F32 && m.rows && !set.f.epsd && relaxed;
       double xold = 0.0;
-      if (incr && p > 0 && (p & 31) == 0) {
-        // FP32 differences drift: every 32 proposals the pair energy of the
-        // state is summed afresh (same coordinates), which also resets eol
+      if (incr && p > 0 && (p & 15) == 0) {
         double el = 0.0, vw = 0.0, hb = 0.0;
         pair_rows<F32, true>(set.f, m, s, kWarps, el, vw, hb);
         double v = el;
