@@ -356,6 +356,9 @@ def run_ours(args, rank, world):
             ends[k].record(stream)
         barrier()
     ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    # batched PT runs each step as one cooperative launch of spp (sweep,
+    # exchange) rounds when every chain is resident at once
+    fused = bool(wl.pt and ens.pt_fused_last())
     # ---- roofline: the sweep kernel alone, one launch per sweep, event-timed
     n_roof = 50 if wl.name == "pt_enkefa64" else 8
     rs = [torch.cuda.Event(enable_timing=True) for _ in range(n_roof)]
@@ -396,8 +399,13 @@ def run_ours(args, rank, world):
     # roofline: algorithmic HBM bytes per launch of the sweep kernel
     # (16 B coordinates per atom + 8 B per dihedral + 8 B energy, per
     # evaluation; one evaluation per free dihedral per sweep; every chain)
-    bytes_per_launch = sum(mols[m].nvr * (16 * mols[m].natoms + 8 * mols[m].nvr + 8) for m in cm)
-    achieved = bytes_per_launch / (sweep_kernel_ms / 1000.0) / 1e9
+    bytes_per_sweep = sum(mols[m].nvr * (16 * mols[m].natoms + 8 * mols[m].nvr + 8) for m in cm)
+    if fused:   # the timed step is that one launch (and an 8-byte memset)
+        roof_kernel, roof_ms, bytes_per_launch = "k_sweep<true> (fused PT)", ms / args.steps, \
+            bytes_per_sweep * spp
+    else:
+        roof_kernel, roof_ms, bytes_per_launch = "k_sweep<true>", sweep_kernel_ms, bytes_per_sweep
+    achieved = bytes_per_launch / (roof_ms / 1000.0) / 1e9
     peak, peak_src = 6650.0, "fallback"
     if os.path.exists(PEAKS):
         try:
@@ -409,7 +417,8 @@ def run_ours(args, rank, world):
     tf = os.path.join(ROOT, "profiles", "k_sweep_traffic.json")
     if wl.name == "pt_enkefa64" and os.path.exists(tf):
         try:
-            traffic = json.load(open(tf)).get("bytes_per_launch")
+            traffic = json.load(open(tf)).get("fused_bytes_per_launch" if fused
+                                              else "bytes_per_launch")
         except Exception:
             traffic = None
     line = {
@@ -424,12 +433,13 @@ def run_ours(args, rank, world):
         "e2e": {"value": e2e_value, "unit": "sweeps/s",
                 "h2d_bytes_per_step": int(vl.nbytes),
                 "d2h_bytes_per_step": int(vl.nbytes + 8 * nch)},
-        "gpu_launches": args.steps * (spp * 2 if wl.pt else 1),
+        "gpu_launches": args.steps * (1 if fused or not wl.pt else spp * 2),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "peak_source": peak_src, "kernel": "k_sweep<true>",
-                     "kernel_ms_per_launch": sweep_kernel_ms,
-                     "bytes_per_launch": bytes_per_launch},
+                     "peak_source": peak_src, "kernel": roof_kernel,
+                     "kernel_ms_per_launch": roof_ms,
+                     "bytes_per_launch": bytes_per_launch,
+                     "single_sweep_launch_ms": sweep_kernel_ms},
         "clocks": clk.summary(),
     }
     if wl.name == "pt_enkefa64" and not args.no_surrogate:

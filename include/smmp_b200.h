@@ -181,6 +181,13 @@ int smmp_ens_set_pt(smmp_ens_t* e, const double* betas, int wrap, int exchange_s
  * chains one at a time in label order (the partem_s.f schedule); serial=0
  * runs all chains at once, captured in CUDA graphs of graph_chunk sweeps. */
 int smmp_ens_pt_sweeps(smmp_ens_t* e, int nsweeps, int serial, int graph_chunk);
+/* Batched runs (serial=0) go as one cooperative launch when every chain can
+ * be resident at once (on by default): each sweep ends at a grid barrier, one
+ * warp exchanges, a second barrier hands out the new temperatures.  A barrier
+ * wait longer than timeout_s seconds ends the run with error code 4.  Results
+ * are bit-identical to the graph path.  No counterpart in the reference. */
+int smmp_ens_set_pt_fused(smmp_ens_t* e, int on, double timeout_s);
+int smmp_ens_pt_fused_last(smmp_ens_t* e, int* fused);   /* 1: last run was fused */
 int smmp_ens_pt_map(smmp_ens_t* e, int* temp_chain);   /* ipoi, 0-based chains */
 int smmp_ens_sizes(smmp_ens_t* e, int* nchains, int* vstride, int* tstride);
 int smmp_ens_get_energies(smmp_ens_t* e, double* eol);          /* [nchains] */

@@ -683,6 +683,21 @@ int smmp_ens_pt_sweeps(smmp_ens_t* e, int nsweeps, int serial, int graph_chunk) 
   });
 }
 
+int smmp_ens_set_pt_fused(smmp_ens_t* e, int on, double timeout_s) {
+  return guard([&] {
+    need(e != nullptr, "NULL argument");
+    need(timeout_s > 0.0, "timeout must be positive");
+    e->e->set_pt_fused(on != 0, timeout_s);
+  });
+}
+
+int smmp_ens_pt_fused_last(smmp_ens_t* e, int* fused) {
+  return guard([&] {
+    need(e != nullptr && fused != nullptr, "NULL argument");
+    *fused = e->e->pt_fused_last() ? 1 : 0;
+  });
+}
+
 int smmp_ens_pt_map(smmp_ens_t* e, int* temp_chain) {
   return guard([&] {
     need(e && temp_chain && e->e->has_pt(), "bad arguments");

@@ -139,6 +139,24 @@ struct DChains {
   unsigned long long* da_n2;   // [chain] proposals accepted at stage 2
 };
 
+// Parallel tempering fused into one cooperative sweep launch: after every
+// sweep all blocks meet at a grid barrier, block 0 runs the exchange step
+// (partem_s.f:210-232) and every chain takes up its new inverse temperature.
+// on == 0 for ordinary launches.
+struct DPTFused {
+  int on;
+  int n;                       // temperature labels (= chains of the launch)
+  int wrap;
+  int* temp_chain;             // [n] chain at each label
+  const double* betas;         // [n] inverse temperature of each label
+  uint32_t* mt;                // exchange stream slot (kMTWords)
+  double* lq;                  // [kQueue] scratch of the exchange stream's refills
+  int* iswitch;
+  unsigned long long* stats;   // [2n]
+  unsigned* bar;               // [2] grid barrier: arrivals, generation
+  unsigned long long timeout_ns;   // a barrier wait longer than this sets kErrTimeout
+};
+
 enum SweepFlags : int {
   kFlagRndOrd = 1,        // random variable order (rndord)
   kFlagFP32 = 2,          // FP32 pair terms with FP64 guard and accumulation

@@ -159,6 +159,7 @@ struct Scalars {
   Proposal spec[2];      // next proposal if this one draws 1 (spec[0]) or 2 (spec[1]) numbers
   int refill;
   int hlo, hhi;          // heavy-atom indices of the proposal's subtree range
+  int gsync;             // result of the last grid barrier
 };
 
 struct Smem {
@@ -1238,26 +1239,127 @@ __global__ void __launch_bounds__(kThreads, 1) k_energy(DMolSet set, DChains ch,
   store_chain(ch, m, c, s);
 }
 
-// nsweeps Metropolis sweeps (metropolis.f:13-184) of chains
-// [first, first+gridDim.x).  Per sweep the reference calls energy() nvr+2
-// times; here the start of a sweep and the closing consistency check do a full
-// setvar+rebuild+evaluation, and each proposal updates the dihedral state with
-// the same setvar arithmetic, rotates the moving subtree in place and
-// evaluates every pair of the lists.  The start of sweep k+1 reuses the
-// coordinates and energy of the check that closed sweep k (same variables),
-// after the setvar call the reference makes there.
+// Replica exchange (partem_s.f:210-232): alternate even/odd neighbour pairs,
+// replica num_rep pairs with 1 when `wrap` is set.  temp_chain[k] is the chain
+// at temperature label k (ipoi); betas[k] the inverse temperature of label k.
+// One warp: the pairs of one parity step are disjoint, so lane k decides the
+// k-th pair with the k-th uniform of the exchange stream (the order in which
+// the reference's loop draws them).  `slot` is the exchange stream's slot
+// (shared or global memory, used by this warp only); `lq` receives the logs
+// the refill computes.  Energies are read past L1: in the fused sweep other
+// blocks wrote them.
+__device__ void exchange_core(const DChains& ch, int* temp_chain, const double* betas, int n,
+                              uint32_t* slot, double* lq, int* iswitch, int wrap,
+                              unsigned long long* stats) {
+  const int lane = threadIdx.x & 31;
+  if (n > 1) {
+    const int sw = *iswitch;
+    const int num_rep1 = sw == 1 ? n - 1 : n, nu = sw == 1 ? 1 : 2;
+    // pairs i = nu, nu+2, ..., num_rep1 (1-based); i == n is the wrap pair
+    int npairs = 0;
+    for (int i = nu; i <= num_rep1; i += 2)
+      if (i != n || wrap) ++npairs;
+    uint32_t head = slot[kQHead];
+    for (int base = 0; base < npairs; base += 32) {
+      const int cnt = min(32, npairs - base);
+      while ((int)(slot[kQTail] - head) < cnt) rng_refill_warp(slot, lq);   // < 32 before: fits
+      __syncwarp();
+      if (lane < cnt) {
+        const int i = nu + 2 * (base + lane);   // the wrap pair, if any, is the last
+        int j = i + 1;
+        if (i == n) j = 1;
+        const int in = temp_chain[i - 1], jn = temp_chain[j - 1];
+        const double bi = betas[i - 1], bj = betas[j - 1];
+        const double ein = __ldcg(&ch.eol[in]), ejn = __ldcg(&ch.eol[jn]);
+        double delta = __dsub_rn(-__dmul_rn(bi, ejn), __dmul_rn(bj, ein));
+        delta = __dadd_rn(delta, __dmul_rn(bi, ein));
+        delta = __dadd_rn(delta, __dmul_rn(bj, ejn));
+        const double ra = qbuf(slot)[(head + lane) & (kQueue - 1)];
+        stats[2 * (i - 1)] += 1;
+        if (ra <= exp(delta)) {
+          temp_chain[i - 1] = jn;
+          temp_chain[j - 1] = in;
+          stats[2 * (i - 1) + 1] += 1;
+        }
+      }
+      head += cnt;
+      __syncwarp();
+    }
+    if (lane == 0) {
+      slot[kQHead] = head;
+      *iswitch = sw == 1 ? 2 : 1;
+    }
+  }
+  __threadfence_block();
+  __syncwarp();
+  for (int k = lane; k < n; k += 32) ch.beta[temp_chain[k]] = betas[k];
+  __threadfence();
+  __syncwarp();
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Barrier of all blocks of a cooperative launch (every block resident), with
+// a bounded wait: after timeout_ns a block gives up, records kErrTimeout and
+// returns false, and the caller ends its sweeps.  bar[0] counts arrivals,
+// bar[1] is the generation.  Returns the same value in every thread.
+__device__ bool grid_barrier(unsigned* bar, unsigned long long timeout_ns, int* err, int* flag) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    __threadfence();
+    volatile unsigned* gen = bar + 1;
+    const unsigned g = *gen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(bar, 1u) + 1u;
+    if (arrived == gridDim.x) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      const unsigned long long t0 = global_ns();
+      while (*gen == g) {
+        if (global_ns() - t0 > timeout_ns) {
+          ok = 0;
+          if (*err == 0) *err = kErrTimeout;
+          break;
+        }
+        __nanosleep(256);
+      }
+    }
+    __threadfence();
+    *flag = ok;
+  }
+  __syncthreads();
+  return *flag != 0;
+}
+
 // Atom t of the set a proposal moves: the subtree [lo, lo+span) or, when
 // `flip`, every other atom.
 __device__ __forceinline__ int moved_atom(int t, int lo, int span, bool flip) {
   return flip ? (t < lo ? t : t + span) : lo + t;
 }
 
+// nsweeps Metropolis sweeps (metropolis.f:13-184) of chains
+// [first, first+gridDim.x).  Per sweep the reference calls energy() nvr+2
+// times; here the start of every sweep does a full setvar+rebuild+evaluation,
+// each proposal updates the dihedral state with the same setvar arithmetic,
+// rotates the moving subtree in place and evaluates every pair of the lists,
+// and the closing consistency check of the launch's last sweep does a full
+// evaluation (earlier sweeps are checked against the next opening one).
+// With pt.on every sweep is followed by a replica exchange of all chains of
+// the (cooperative) launch.
 // Kernels are built per (F32, ROWS, SASA): a launch whose molecules have no
 // row form, or that runs without solvation, carries none of that code (and
 // none of its registers).
 template <bool F32, bool ROWS, bool SASA>
 __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, DWeight w, int first,
-                                                       int nsweeps, int flags, double check_tol) {
+                                                       int nsweeps, int flags, double check_tol,
+                                                       DPTFused pt) {
   const int c = first + blockIdx.x;
   const bool sasa = SASA;
   const bool rndord = (flags & kFlagRndOrd) != 0;
@@ -1269,7 +1371,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
   const DMol& m = stage_mol(set, ch, c, s);
   load_static(*set.ff, m, s, sasa);
   load_chain(ch, m, c, s);
-  const double beta = ch.beta[c];
+  double beta = ch.beta[c];
   int* err = &ch.err[c];
   unsigned long long nacc = 0, nprop = 0;
   __syncthreads();
@@ -1288,28 +1390,37 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
   uint32_t head = s.mt[kQHead];   // identical in every thread from here on
   double eol = ch.eol[c], enew = 0.0, etor = 0.0;
   double ep = 0.0;   // pair energy of the state (row-form molecules: updated by differences)
-  bool fresh = false;
+  // The closing energy() of a sweep that another sweep of this launch
+  // follows is not evaluated on its own: that sweep's opening energy() (one
+  // more setvar on the same variables, then the rebuild) stands in for it in
+  // the consistency check.  energy() calls setvar every time (energy.f:47)
+  // and setvar is not idempotent to the last bit, so it is the opening
+  // evaluation that the trajectory must start from.
+  bool check_pending = false;
 
   for (int sw = 0; sw < nsweeps; ++sw) {
     if (flags & kFlagExtraSetvar) {   // partem_s.f:194-198: setvar(i, vlvr) first
       setvar_all(m, s);
       __syncthreads();
-      fresh = false;
     }
     // ---- eol = energy() (metropolis.f:35)
     setvar_all(m, s);
     __syncthreads();
-    if (!fresh) {
-      torsion_all(m, s);
-      full_rebuild(m, s);
-      evaluate_block<F32, ROWS, SASA>(set.f, m, s, err);
-      __syncthreads();
+    torsion_all(m, s);
+    full_rebuild(m, s);
+    evaluate_block<F32, ROWS, SASA>(set.f, m, s, err);
+    __syncthreads();
+    {
       double sum[5];
       all_sums(s, sum);
       enew = total_of(sum);
       etor = sum[3];
       ep = (sum[0] + sum[1]) + sum[2];
     }
+    if (check_pending && threadIdx.x == 0 && !(flags & kFlagNoCheck) &&
+        fabs(eol - enew) > check_tol && eol < 100000.0)
+      set_err(err, kErrConsistency);
+    check_pending = false;
     eol = enew;
     const bool relaxed = fabs(eol) < 1e4;
     if (m.nfree > 0 && threadIdx.x == 0) {
@@ -1502,24 +1613,34 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
     }
     setvar_all(m, s);
     __syncthreads();
-    torsion_all(m, s);
-    full_rebuild(m, s);
-    evaluate_block<F32, ROWS, SASA>(set.f, m, s, err);
-    __syncthreads();
-    {
+    if (sw + 1 == nsweeps) {
+      torsion_all(m, s);
+      full_rebuild(m, s);
+      evaluate_block<F32, ROWS, SASA>(set.f, m, s, err);
+      __syncthreads();
       double sum[5];
       all_sums(s, sum);
       enew = total_of(sum);
-      etor = sum[3];
-      ep = (sum[0] + sum[1]) + sum[2];   // the next sweep starts from this evaluation
       if (threadIdx.x == 0) {
         if (!(flags & kFlagNoCheck) && fabs(eol - enew) > check_tol && eol < 100000.0)
           set_err(err, kErrConsistency);
         write_terms(ch, c, sum);
       }
+      __syncthreads();
+    } else {
+      check_pending = true;
     }
-    __syncthreads();
-    fresh = true;
+    if (pt.on) {
+      // fused parallel tempering: every chain's energy is in place, block 0's
+      // first warp exchanges, then every chain takes up its new temperature
+      if (threadIdx.x == 0) ch.eol[c] = eol;
+      if (!grid_barrier(pt.bar, pt.timeout_ns, err, &sc.gsync)) break;
+      if (blockIdx.x == 0 && warp == 0)
+        exchange_core(ch, pt.temp_chain, pt.betas, pt.n, pt.mt, pt.lq, pt.iswitch, pt.wrap,
+                      pt.stats);
+      if (!grid_barrier(pt.bar, pt.timeout_ns, err, &sc.gsync)) break;
+      beta = __ldcg(&ch.beta[c]);
+    }
   }
   if (threadIdx.x == 0) {
     ch.eol[c] = eol;
@@ -1679,6 +1800,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep_da(DMolSet set, DChains c
   __syncthreads();
   uint32_t head = s.mt[kQHead];
   double eol = 0.0, etor = 0.0;
+  bool check_pending = false;   // as in k_sweep: the next opening energy() checks
 
   for (int sw = 0; sw < nsweeps; ++sw) {
     // stage-2 acceptance n2 / max(n1, 1) below the floor, once n1 >= da_min
@@ -1694,7 +1816,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep_da(DMolSet set, DChains c
     {
       double sum[5];
       all_sums(s, sum);
-      eol = total_of(sum);
+      const double enew = total_of(sum);
+      if (check_pending && threadIdx.x == 0 && !(flags & kFlagNoCheck) &&
+          fabs(eol - enew) > check_tol && eol < 100000.0)
+        set_err(err, kErrConsistency);
+      check_pending = false;
+      eol = enew;
       etor = sum[3];
     }
     sur_features(m, s);
@@ -1859,6 +1986,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep_da(DMolSet set, DChains c
     // ---- closing energy() and consistency check (metropolis.f:172-179)
     setvar_all(m, s);
     __syncthreads();
+    if (sw + 1 < nsweeps) {
+      check_pending = true;
+      continue;
+    }
     torsion_all(m, s);
     full_rebuild(m, s);
     evaluate_block<F32, ROWS, SASA>(set.f, m, s, err);
@@ -1889,13 +2020,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep_da(DMolSet set, DChains c
   store_chain(ch, m, c, s);
 }
 
-// Replica exchange (partem_s.f:210-232): alternate even/odd neighbour pairs,
-// replica num_rep pairs with 1 when `wrap` is set.  temp_chain[k] is the chain
-// at temperature label k (ipoi); betas[k] the inverse temperature of label k.
-// One warp: the pairs of one parity step are disjoint, so lane k decides the
-// k-th pair with the k-th uniform of the exchange stream (the order in which
-// the reference's loop draws them); the stream slot is worked on in shared
-// memory and written back.
+// Replica exchange step as a kernel: the stream slot is copied into shared
+// memory, worked on by exchange_core and written back.
 __global__ void __launch_bounds__(32) k_exchange(DChains ch, int* temp_chain, const double* betas,
                                                  int n, uint32_t* mt, int* iswitch, int wrap,
                                                  unsigned long long* stats) {
@@ -1903,51 +2029,11 @@ __global__ void __launch_bounds__(32) k_exchange(DChains ch, int* temp_chain, co
   __shared__ double lq[kQueue];
   const int lane = threadIdx.x;
   if (blockIdx.x != 0) return;
-  if (n > 1) {
-    for (int k = lane; k < kMTWords; k += 32) slot[k] = mt[k];
-    __syncwarp();
-    const int sw = *iswitch;
-    const int num_rep1 = sw == 1 ? n - 1 : n, nu = sw == 1 ? 1 : 2;
-    // pairs i = nu, nu+2, ..., num_rep1 (1-based); i == n is the wrap pair
-    int npairs = 0;
-    for (int i = nu; i <= num_rep1; i += 2)
-      if (i != n || wrap) ++npairs;
-    uint32_t head = slot[kQHead];
-    for (int base = 0; base < npairs; base += 32) {
-      const int cnt = min(32, npairs - base);
-      while ((int)(slot[kQTail] - head) < cnt) rng_refill_warp(slot, lq);   // < 32 before: fits
-      __syncwarp();
-      if (lane < cnt) {
-        const int i = nu + 2 * (base + lane);   // the wrap pair, if any, is the last
-        int j = i + 1;
-        if (i == n) j = 1;
-        const int in = temp_chain[i - 1], jn = temp_chain[j - 1];
-        const double bi = betas[i - 1], bj = betas[j - 1];
-        const double ein = ch.eol[in], ejn = ch.eol[jn];
-        double delta = __dsub_rn(-__dmul_rn(bi, ejn), __dmul_rn(bj, ein));
-        delta = __dadd_rn(delta, __dmul_rn(bi, ein));
-        delta = __dadd_rn(delta, __dmul_rn(bj, ejn));
-        const double ra = qbuf(slot)[(head + lane) & (kQueue - 1)];
-        stats[2 * (i - 1)] += 1;
-        if (ra <= exp(delta)) {
-          temp_chain[i - 1] = jn;
-          temp_chain[j - 1] = in;
-          stats[2 * (i - 1) + 1] += 1;
-        }
-      }
-      head += cnt;
-      __syncwarp();
-    }
-    if (lane == 0) {
-      slot[kQHead] = head;
-      *iswitch = sw == 1 ? 2 : 1;
-    }
-    __syncwarp();
-    for (int k = lane; k < kMTWords; k += 32) mt[k] = slot[k];
-    __threadfence_block();
-    __syncwarp();
-  }
-  for (int k = lane; k < n; k += 32) ch.beta[temp_chain[k]] = betas[k];
+  for (int k = lane; k < kMTWords; k += 32) slot[k] = mt[k];
+  __syncwarp();
+  exchange_core(ch, temp_chain, betas, n, slot, lq, iswitch, wrap, stats);
+  __syncwarp();
+  for (int k = lane; k < kMTWords; k += 32) mt[k] = slot[k];
 }
 
 // ============================================================================ host wrappers
@@ -2019,8 +2105,32 @@ static cudaError_t launch_sweep_t(const DMolSet& set, const DChains& ch, const D
   cudaError_t e = prep_smem((const void*)k_sweep<F32, ROWS, SASA>, sm);
   if (e != cudaSuccess || count <= 0) return e;
   k_sweep<F32, ROWS, SASA><<<count, kThreads, sm, st>>>(set, ch, w, first, nsweeps, flags,
-                                                        check_tol);
+                                                        check_tol, DPTFused{});
   return cudaGetLastError();
+}
+
+// One cooperative launch of nsweeps (sweep, exchange) rounds over chains
+// [0, count).  Returns cudaErrorCooperativeLaunchTooLarge when the chains
+// cannot all be resident at once, cudaErrorNotSupported when the device has
+// no cooperative launch; nothing is launched then.
+template <bool F32, bool ROWS, bool SASA>
+static cudaError_t launch_sweep_pt_t(DMolSet set, DChains ch, DWeight w, int count, int nsweeps,
+                                     int flags, double check_tol, DPTFused pt, size_t sm,
+                                     cudaStream_t st) {
+  const void* fn = (const void*)k_sweep<F32, ROWS, SASA>;
+  cudaError_t e = prep_smem(fn, sm);
+  if (e != cudaSuccess) return e;
+  int dev = 0, coop = 0, nsm = 0, per = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, kThreads, sm)) != cudaSuccess)
+    return e;
+  if (!coop) return cudaErrorNotSupported;
+  if ((long long)per * nsm < count) return cudaErrorCooperativeLaunchTooLarge;
+  int first = 0;
+  void* args[] = {&set, &ch, &w, &first, &nsweeps, &flags, &check_tol, &pt};
+  return cudaLaunchCooperativeKernel(fn, dim3(count), dim3(kThreads), args, sm, st);
 }
 
 static int variant(const DMolSet& set, bool fp32) {
@@ -2047,6 +2157,26 @@ cudaError_t launch_sweep(const DMolSet& set, const DChains& ch, const DWeight& w
   const size_t sm = sweep_smem_bytes(set);
 #define SMMP_SWEEP(a, b, c) \
   launch_sweep_t<a, b, c>(set, ch, w, first, count, nsweeps, flags, check_tol, sm, st)
+  switch (variant(set, (flags & kFlagFP32) != 0)) {
+    case 0: return SMMP_SWEEP(false, false, false);
+    case 1: return SMMP_SWEEP(false, false, true);
+    case 2: return SMMP_SWEEP(false, true, false);
+    case 3: return SMMP_SWEEP(false, true, true);
+    case 4: return SMMP_SWEEP(true, false, false);
+    case 5: return SMMP_SWEEP(true, false, true);
+    case 6: return SMMP_SWEEP(true, true, false);
+    default: return SMMP_SWEEP(true, true, true);
+  }
+#undef SMMP_SWEEP
+}
+
+cudaError_t launch_sweep_pt(const DMolSet& set, const DChains& ch, const DWeight& w, int count,
+                            int nsweeps, int flags, double check_tol, const DPTFused& pt,
+                            cudaStream_t st) {
+  if (ch.sur.w1 != nullptr || pt.n != count) return cudaErrorNotSupported;
+  const size_t sm = sweep_smem_bytes(set);
+#define SMMP_SWEEP(a, b, c) \
+  launch_sweep_pt_t<a, b, c>(set, ch, w, count, nsweeps, flags, check_tol, pt, sm, st)
   switch (variant(set, (flags & kFlagFP32) != 0)) {
     case 0: return SMMP_SWEEP(false, false, false);
     case 1: return SMMP_SWEEP(false, false, true);

@@ -20,6 +20,11 @@ cudaError_t launch_energy(const DMolSet& set, const DChains& ch, int first, int 
                           cudaStream_t st);
 cudaError_t launch_sweep(const DMolSet& set, const DChains& ch, const DWeight& w, int first,
                          int count, int nsweeps, int flags, double check_tol, cudaStream_t st);
+// Fused parallel tempering: nsweeps rounds of (one sweep of every chain, one
+// exchange) in one cooperative launch over chains [0, count).
+cudaError_t launch_sweep_pt(const DMolSet& set, const DChains& ch, const DWeight& w, int count,
+                            int nsweeps, int flags, double check_tol, const DPTFused& pt,
+                            cudaStream_t st);
 cudaError_t launch_exchange(const DChains& ch, int* temp_chain, const double* betas, int n,
                             uint32_t* mt, int* iswitch, int wrap, unsigned long long* stats,
                             cudaStream_t st);

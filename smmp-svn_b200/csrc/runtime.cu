@@ -20,8 +20,13 @@ namespace {
 template <class T>
 T* dalloc(std::vector<void*>& owner, size_t n) {
   void* p = nullptr;
-  check_cuda(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)), "cudaMalloc");
+  const size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+  check_cuda(cudaMalloc(&p, bytes), "cudaMalloc");
   owner.push_back(p);
+  // zeroed, so that the unused words of a stream slot (and with them a
+  // checkpoint) do not depend on what the memory held before
+  check_cuda(cudaMemset(p, 0, bytes), "cudaMemset");
+  check_cuda(cudaStreamSynchronize(nullptr), "cudaMemset sync");   // before any other stream
   return static_cast<T*>(p);
 }
 template <class T>
@@ -487,6 +492,8 @@ void Ensemble::set_pt(const std::vector<double>& betas, int wrap, int exchange_s
   pt_.mt = dalloc<uint32_t>(allocs_, kMTWords);
   pt_.iswitch = dalloc<int>(allocs_, 1);
   pt_.stats = dalloc<unsigned long long>(allocs_, 2 * n_);
+  pt_.lq = dalloc<double>(allocs_, kQueue);
+  pt_.bar = dalloc<unsigned>(allocs_, 2);
   std::vector<int> tc(n_);
   std::iota(tc.begin(), tc.end(), 0);
   h2d(pt_.temp_chain, tc);
@@ -506,9 +513,16 @@ void Ensemble::set_pt(const std::vector<double>& betas, int wrap, int exchange_s
   check_cuda(cudaStreamSynchronize(stream_), "set_pt sync");
 }
 
+void Ensemble::set_pt_fused(bool on, double timeout_s) {
+  if (!(timeout_s > 0.0)) throw std::runtime_error("set_pt_fused: timeout must be positive");
+  pt_.fused = on;
+  pt_.timeout_s = timeout_s;
+}
+
 void Ensemble::pt_sweeps(int nsweeps, int flags, bool serial, int graph_chunk) {
   if (pt_.n != n_) throw std::runtime_error("pt_sweeps: call set_pt first");
   DWeight w{kWeightCanon, 0, 0, 1.0, nullptr, nullptr};
+  pt_fused_last_ = false;
   if (serial) {
     std::vector<int> tc;
     for (int s = 0; s < nsweeps; ++s) {
@@ -522,6 +536,23 @@ void Ensemble::pt_sweeps(int nsweeps, int flags, bool serial, int graph_chunk) {
     return;
   }
   double tol = (flags & kFlagFP32) ? check_tol_fp32 : check_tol;
+  if (pt_.fused && nmt_ != 1 && nsweeps > 0) {
+    // every chain resident at once: sweeps and exchanges in one launch, the
+    // rounds separated by grid barriers
+    check_cuda(cudaMemsetAsync(pt_.bar, 0, 2 * sizeof(unsigned), stream_), "memset");
+    DPTFused f{1,          n_,        pt_.wrap,   pt_.temp_chain, pt_.betas,
+               pt_.mt,     pt_.lq,    pt_.iswitch, pt_.stats,     pt_.bar,
+               (unsigned long long)(pt_.timeout_s * 1e9)};
+    cudaError_t e = launch_sweep_pt(set(), ch_, w, n_, nsweeps, flags, tol, f, stream_);
+    if (e == cudaSuccess) {
+      pt_fused_last_ = true;
+      check_cuda(cudaStreamSynchronize(stream_), "pt sync");
+      return;
+    }
+    if (e != cudaErrorCooperativeLaunchTooLarge && e != cudaErrorNotSupported)
+      check_cuda(e, "fused pt launch");
+    (void)cudaGetLastError();   // not possible here: take the graph path
+  }
   auto enqueue = [&](int k) {
     for (int i = 0; i < k; ++i) {
       check_cuda(launch_sweep(set(), ch_, w, 0, n_, 1, flags, tol, stream_), "sweep");

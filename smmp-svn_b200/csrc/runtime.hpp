@@ -68,6 +68,10 @@ struct PTState {
   uint32_t* mt = nullptr;             // device stream slot (kMTWords) of the exchanges
   int* iswitch = nullptr;             // device
   unsigned long long* stats = nullptr;   // device [2n] attempts/accepts per pair
+  double* lq = nullptr;               // device [kQueue] refill scratch of the fused exchange
+  unsigned* bar = nullptr;            // device [2] grid barrier of the fused launch
+  bool fused = true;                  // batched runs: one cooperative launch when possible
+  double timeout_s = 30.0;            // bound on one grid-barrier wait
 };
 
 // An ensemble of chains; every chain is an independent copy of one molecule.
@@ -113,6 +117,10 @@ class Ensemble {
   void pt_stats(std::vector<unsigned long long>& s) const;
   // exchange state for checkpoints: map, parity switch, exchange stream
   bool has_pt() const { return pt_.n == n_; }
+  // Fused cooperative launch for batched parallel tempering (on by default);
+  // off, or when the chains cannot all be resident, runs take the graph path.
+  void set_pt_fused(bool on, double timeout_s);
+  bool pt_fused_last() const { return pt_fused_last_; }
   void pt_get_state(std::vector<int>& tc, int& iswitch, std::vector<uint32_t>& mt,
                     std::vector<double>& betas) const;
   void pt_set_state(const std::vector<int>& tc, int iswitch, const std::vector<uint32_t>& mt,
@@ -156,6 +164,7 @@ class Ensemble {
   PTState pt_;
   cudaGraphExec_t graph_ = nullptr;
   int graph_len_ = 0, graph_flags_ = -1;
+  bool pt_fused_last_ = false;   // the last batched pt_sweeps ran the fused launch
   double* coords_buf_ = nullptr;
 };
 

@@ -132,6 +132,17 @@ class Ensemble:
     def pt_sweeps(self, n, serial=False, graph_chunk=64):
         check(lib.smmp_ens_pt_sweeps(self._h, int(n), int(bool(serial)), int(graph_chunk)))
 
+    def set_pt_fused(self, on=True, timeout_s=30.0):
+        """Batched pt_sweeps as one cooperative launch (default) or as CUDA
+        graphs of separate sweep and exchange launches; both give the same
+        bits."""
+        check(lib.smmp_ens_set_pt_fused(self._h, int(bool(on)), float(timeout_s)))
+
+    def pt_fused_last(self):
+        v = ctypes.c_int(0)
+        check(lib.smmp_ens_pt_fused_last(self._h, ctypes.byref(v)))
+        return bool(v.value)
+
     def pt_map(self):
         out = np.zeros(self.nchains, dtype=np.int32)
         check(lib.smmp_ens_pt_map(self._h, out.ctypes.data_as(_I)))
