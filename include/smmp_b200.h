@@ -185,8 +185,10 @@ int smmp_ens_pt_sweeps(smmp_ens_t* e, int nsweeps, int serial, int graph_chunk);
  * be resident at once (on by default): each sweep ends at a grid barrier, one
  * warp exchanges, a second barrier hands out the new temperatures.  A barrier
  * wait longer than timeout_s seconds ends the run with error code 4.  Results
- * are bit-identical to the graph path.  No counterpart in the reference. */
-int smmp_ens_set_pt_fused(smmp_ens_t* e, int on, double timeout_s);
+ * are bit-identical to the graph path.  barrier_extra is 0 except in tests of
+ * that bounded wait: the barriers then wait for arrivals that never come.
+ * No counterpart in the reference. */
+int smmp_ens_set_pt_fused(smmp_ens_t* e, int on, double timeout_s, int barrier_extra);
 int smmp_ens_pt_fused_last(smmp_ens_t* e, int* fused);   /* 1: last run was fused */
 int smmp_ens_pt_map(smmp_ens_t* e, int* temp_chain);   /* ipoi, 0-based chains */
 int smmp_ens_sizes(smmp_ens_t* e, int* nchains, int* vstride, int* tstride);

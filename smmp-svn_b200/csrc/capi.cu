@@ -683,11 +683,11 @@ int smmp_ens_pt_sweeps(smmp_ens_t* e, int nsweeps, int serial, int graph_chunk) 
   });
 }
 
-int smmp_ens_set_pt_fused(smmp_ens_t* e, int on, double timeout_s) {
+int smmp_ens_set_pt_fused(smmp_ens_t* e, int on, double timeout_s, int barrier_extra) {
   return guard([&] {
     need(e != nullptr, "NULL argument");
-    need(timeout_s > 0.0, "timeout must be positive");
-    e->e->set_pt_fused(on != 0, timeout_s);
+    need(timeout_s > 0.0 && barrier_extra >= 0, "bad arguments");
+    e->e->set_pt_fused(on != 0, timeout_s, (unsigned)barrier_extra);
   });
 }
 

@@ -155,6 +155,8 @@ struct DPTFused {
   unsigned long long* stats;   // [2n]
   unsigned* bar;               // [2] grid barrier: arrivals, generation
   unsigned long long timeout_ns;   // a barrier wait longer than this sets kErrTimeout
+  unsigned extra;              // arrivals beyond the launch's blocks (0; >0 only in tests:
+                               // the barrier then never opens and every wait runs out)
 };
 
 enum SweepFlags : int {

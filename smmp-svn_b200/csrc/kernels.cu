@@ -1305,9 +1305,11 @@ __device__ __forceinline__ unsigned long long global_ns() {
 
 // Barrier of all blocks of a cooperative launch (every block resident), with
 // a bounded wait: after timeout_ns a block gives up, records kErrTimeout and
-// returns false, and the caller ends its sweeps.  bar[0] counts arrivals,
-// bar[1] is the generation.  Returns the same value in every thread.
-__device__ bool grid_barrier(unsigned* bar, unsigned long long timeout_ns, int* err, int* flag) {
+// returns false, and the caller ends its sweeps.  bar[0] counts arrivals
+// (the barrier opens at `expected`, the launch's block count), bar[1] is the
+// generation.  Returns the same value in every thread.
+__device__ bool grid_barrier(unsigned* bar, unsigned expected, unsigned long long timeout_ns,
+                             int* err, int* flag) {
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
@@ -1316,7 +1318,7 @@ __device__ bool grid_barrier(unsigned* bar, unsigned long long timeout_ns, int* 
     const unsigned g = *gen;
     __threadfence();
     const unsigned arrived = atomicAdd(bar, 1u) + 1u;
-    if (arrived == gridDim.x) {
+    if (arrived == expected) {
       atomicExch(bar, 0u);
       __threadfence();
       atomicAdd(bar + 1, 1u);
@@ -1634,11 +1636,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       // fused parallel tempering: every chain's energy is in place, block 0's
       // first warp exchanges, then every chain takes up its new temperature
       if (threadIdx.x == 0) ch.eol[c] = eol;
-      if (!grid_barrier(pt.bar, pt.timeout_ns, err, &sc.gsync)) break;
+      if (!grid_barrier(pt.bar, gridDim.x + pt.extra, pt.timeout_ns, err, &sc.gsync)) break;
       if (blockIdx.x == 0 && warp == 0)
         exchange_core(ch, pt.temp_chain, pt.betas, pt.n, pt.mt, pt.lq, pt.iswitch, pt.wrap,
                       pt.stats);
-      if (!grid_barrier(pt.bar, pt.timeout_ns, err, &sc.gsync)) break;
+      if (!grid_barrier(pt.bar, gridDim.x + pt.extra, pt.timeout_ns, err, &sc.gsync)) break;
       beta = __ldcg(&ch.beta[c]);
     }
   }

@@ -513,10 +513,11 @@ void Ensemble::set_pt(const std::vector<double>& betas, int wrap, int exchange_s
   check_cuda(cudaStreamSynchronize(stream_), "set_pt sync");
 }
 
-void Ensemble::set_pt_fused(bool on, double timeout_s) {
+void Ensemble::set_pt_fused(bool on, double timeout_s, unsigned barrier_extra) {
   if (!(timeout_s > 0.0)) throw std::runtime_error("set_pt_fused: timeout must be positive");
   pt_.fused = on;
   pt_.timeout_s = timeout_s;
+  pt_.barrier_extra = barrier_extra;
 }
 
 void Ensemble::pt_sweeps(int nsweeps, int flags, bool serial, int graph_chunk) {
@@ -542,7 +543,7 @@ void Ensemble::pt_sweeps(int nsweeps, int flags, bool serial, int graph_chunk) {
     check_cuda(cudaMemsetAsync(pt_.bar, 0, 2 * sizeof(unsigned), stream_), "memset");
     DPTFused f{1,          n_,        pt_.wrap,   pt_.temp_chain, pt_.betas,
                pt_.mt,     pt_.lq,    pt_.iswitch, pt_.stats,     pt_.bar,
-               (unsigned long long)(pt_.timeout_s * 1e9)};
+               (unsigned long long)(pt_.timeout_s * 1e9), pt_.barrier_extra};
     cudaError_t e = launch_sweep_pt(set(), ch_, w, n_, nsweeps, flags, tol, f, stream_);
     if (e == cudaSuccess) {
       pt_fused_last_ = true;

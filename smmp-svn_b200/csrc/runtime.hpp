@@ -72,6 +72,7 @@ struct PTState {
   unsigned* bar = nullptr;            // device [2] grid barrier of the fused launch
   bool fused = true;                  // batched runs: one cooperative launch when possible
   double timeout_s = 30.0;            // bound on one grid-barrier wait
+  unsigned barrier_extra = 0;         // tests only: arrivals that never come
 };
 
 // An ensemble of chains; every chain is an independent copy of one molecule.
@@ -119,7 +120,9 @@ class Ensemble {
   bool has_pt() const { return pt_.n == n_; }
   // Fused cooperative launch for batched parallel tempering (on by default);
   // off, or when the chains cannot all be resident, runs take the graph path.
-  void set_pt_fused(bool on, double timeout_s);
+  // barrier_extra > 0 (tests of the bounded wait) makes every barrier wait
+  // for arrivals that never come: every chain ends with kErrTimeout.
+  void set_pt_fused(bool on, double timeout_s, unsigned barrier_extra = 0);
   bool pt_fused_last() const { return pt_fused_last_; }
   void pt_get_state(std::vector<int>& tc, int& iswitch, std::vector<uint32_t>& mt,
                     std::vector<double>& betas) const;

@@ -70,7 +70,7 @@ _SIGS = {
     "smmp_ens_sweeps": (c_int, [c_void_p, c_int, P(Weight)]),
     "smmp_ens_set_pt": (c_int, [c_void_p, P(c_double), c_int, c_int]),
     "smmp_ens_pt_sweeps": (c_int, [c_void_p, c_int, c_int, c_int]),
-    "smmp_ens_set_pt_fused": (c_int, [c_void_p, c_int, c_double]),
+    "smmp_ens_set_pt_fused": (c_int, [c_void_p, c_int, c_double, c_int]),
     "smmp_ens_pt_fused_last": (c_int, [c_void_p, c_void_p]),
     "smmp_ens_pt_map": (c_int, [c_void_p, P(c_int)]),
     "smmp_ens_sizes": (c_int, [c_void_p, P(c_int), P(c_int), P(c_int)]),

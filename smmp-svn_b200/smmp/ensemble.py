@@ -132,11 +132,14 @@ class Ensemble:
     def pt_sweeps(self, n, serial=False, graph_chunk=64):
         check(lib.smmp_ens_pt_sweeps(self._h, int(n), int(bool(serial)), int(graph_chunk)))
 
-    def set_pt_fused(self, on=True, timeout_s=30.0):
+    def set_pt_fused(self, on=True, timeout_s=30.0, barrier_extra=0):
         """Batched pt_sweeps as one cooperative launch (default) or as CUDA
         graphs of separate sweep and exchange launches; both give the same
-        bits."""
-        check(lib.smmp_ens_set_pt_fused(self._h, int(bool(on)), float(timeout_s)))
+        bits.  A grid-barrier wait longer than timeout_s ends the run with
+        error code 4 on the chains that waited; barrier_extra > 0 (tests only)
+        makes the barriers wait for arrivals that never come."""
+        check(lib.smmp_ens_set_pt_fused(self._h, int(bool(on)), float(timeout_s),
+                                        int(barrier_extra)))
 
     def pt_fused_last(self):
         v = ctypes.c_int(0)

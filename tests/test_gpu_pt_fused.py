@@ -105,3 +105,23 @@ def test_more_chains_than_resident_blocks_take_the_graph_path():
         assert not ens.errors().any()
         out.append(ens.checkpoint())
     assert out[0] == out[1]
+
+
+def test_grid_barrier_wait_is_bounded():
+    """A barrier that never opens (it waits for one arrival more than the
+    launch has blocks): every chain gives up after the timeout with error
+    code 4, the call reports it, and the context stays usable."""
+    from smmp._lib import SmmpError
+    from smmp.ensemble import Ensemble
+    mol = _enkefa()
+    betas = _ladder(8)
+    ens = Ensemble([mol], [0] * 8, list(range(1, 9)), betas)
+    ens.random_start()
+    ens.set_pt(betas)
+    ens.set_pt_fused(True, timeout_s=0.05, barrier_extra=1)
+    with pytest.raises(SmmpError):
+        ens.pt_sweeps(3)
+    assert ens.pt_fused_last()
+    assert (ens.errors() == 4).all()
+    ok = _run([mol], [0] * 8, False, True, 2, [2], True)   # a new ensemble runs
+    assert not ok.errors().any()
