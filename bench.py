@@ -340,9 +340,9 @@ def run_ours(args, rank, world):
     for _ in range(args.warmup):
         step()
     # the autotuner picks the pair-work decomposition (state left unchanged)
-    rows, (ms_lists, ms_rows) = ens.autotune()
-    tuned = {"pair_work": "rows" if rows else "chunk lists",
-             "sweep_ms_lists": ms_lists, "sweep_ms_rows": ms_rows}
+    form, (ms_lists, ms_rows, ms_size) = ens.autotune()
+    tuned = {"pair_work": form, "sweep_ms_lists": ms_lists, "sweep_ms_rows": ms_rows,
+             "sweep_ms_rows_128plus": ms_size}
     # ---- device-timed region: K steps, each bracketed by events on the stream
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]

@@ -257,12 +257,13 @@ int smmp_sur_predict_noalloc(smmp_sur_t* s, const float* ang_dev, int n, double*
  * sweeps again.  Stage counters restart at zero. */
 int smmp_ens_set_surrogate(smmp_ens_t* e, smmp_sur_t* s, double floor, int min_stage1);
 /* Autotuner (no counterpart in the reference): times one sweep of every
- * chain with each pair-work decomposition the molecules allow (8-partner
- * chunks of the mklist lists; 32-partner passes over rows of the pair
- * triangle) from the same saved state, keeps the faster for later sweeps and
- * restores the state, so the call leaves no trace in the trajectory.
- * *choice = 1 when rows won; ms[2] = {lists, rows} in milliseconds (zeros
- * when no molecule allows rows). */
+ * chain with each pair-work decomposition the molecules allow (0: 8-partner
+ * chunks of the mklist lists; 1: 32-partner passes over rows of the pair
+ * triangle; 2: rows for molecules of 128 atoms or more, lists for the rest)
+ * from the same saved state, keeps the fastest for later sweeps and restores
+ * the state, so the call leaves no trace in the trajectory.  *choice = the
+ * winner; ms[3] = the three times in milliseconds (zeros when no molecule
+ * allows rows). */
 int smmp_ens_autotune(smmp_ens_t* e, int* choice, double* ms);
 /* Per chain: proposals that passed stage 1, and that were then accepted. */
 int smmp_ens_da_stats(smmp_ens_t* e, uint64_t* stage1, uint64_t* stage2);

@@ -970,12 +970,13 @@ int smmp_ens_set_surrogate(smmp_ens_t* e, smmp_sur_t* s, double floor, int min_s
 int smmp_ens_autotune(smmp_ens_t* e, int* choice, double* ms) {
   return guard([&] {
     need(e != nullptr, "NULL ensemble");
-    double t[2];
+    double t[3];
     int c = e->e->autotune(e->flags & (kFlagFP32 | kFlagRndOrd), t);
     if (choice) *choice = c;
     if (ms) {
       ms[0] = t[0];
       ms[1] = t[1];
+      ms[2] = t[2];
     }
   });
 }

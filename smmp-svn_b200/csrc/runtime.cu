@@ -345,12 +345,13 @@ void Ensemble::set_surrogate(const DSurrogate* view, float floor, int min_stage1
   graph_len_ = 0;
 }
 
-// Autotuner: time one sweep of every chain with each pair-work form (chunk
-// lists; 32-partner row passes) from the same saved state, keep the faster,
-// and put the state back.  The timed sweeps leave no trace.
+// Autotuner: time one sweep of every chain with each pair-work form (0:
+// chunk lists; 1: 32-partner row passes; 2: row passes for molecules of 128
+// atoms or more, lists for the rest) from the same saved state, keep the
+// fastest, and put the state back.  The timed sweeps leave no trace.
 int Ensemble::autotune(int flags, double* ms_out) {
   if (!dev_->any_rows_possible()) {
-    if (ms_out) ms_out[0] = ms_out[1] = 0.0;
+    if (ms_out) ms_out[0] = ms_out[1] = ms_out[2] = 0.0;
     return 0;
   }
   check_cuda(cudaStreamSynchronize(stream_), "autotune sync");
@@ -386,9 +387,10 @@ int Ensemble::autotune(int flags, double* ms_out) {
   cudaEvent_t e0, e1;
   check_cuda(cudaEventCreate(&e0), "event");
   check_cuda(cudaEventCreate(&e1), "event");
-  double ms[2] = {0.0, 0.0};
-  for (int mode = 0; mode < 2; ++mode) {
-    dev_->set_rows(mode);
+  double ms[3] = {0.0, 0.0, 0.0};
+  const int rows_mode[3] = {0, 1, -1};   // DeviceSet::set_rows argument of each form
+  for (int mode = 0; mode < 3; ++mode) {
+    dev_->set_rows(rows_mode[mode]);
     restore();
     launch_sweep_range(0, n_, 1, flags | kFlagNoCheck, w);   // warm-up
     check_cuda(cudaStreamSynchronize(stream_), "autotune sync");
@@ -403,8 +405,10 @@ int Ensemble::autotune(int flags, double* ms_out) {
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  const int best = ms[1] < ms[0] ? 1 : 0;
-  dev_->set_rows(best);
+  int best = 0;
+  for (int mode = 1; mode < 3; ++mode)
+    if (ms[mode] < ms[best]) best = mode;
+  dev_->set_rows(rows_mode[best]);
   restore();
   if (graph_) cudaGraphExecDestroy(graph_);   // kernel arguments changed
   graph_ = nullptr;
@@ -412,6 +416,7 @@ int Ensemble::autotune(int flags, double* ms_out) {
   if (ms_out) {
     ms_out[0] = ms[0];
     ms_out[1] = ms[1];
+    ms_out[2] = ms[2];
   }
   return best;
 }

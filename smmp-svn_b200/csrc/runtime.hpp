@@ -94,9 +94,10 @@ class Ensemble {
   // device memory must outlive its use here.
   void set_surrogate(const DSurrogate* view, float floor, int min_stage1);
   void da_stats(std::vector<unsigned long long>& n1, std::vector<unsigned long long>& n2) const;
-  // Autotuner: times one sweep of all chains with each pair-work form (chunk
-  // lists / row passes) from the same saved state, keeps the faster and
-  // restores the state.  Returns 1 when rows won; ms_out[2] the two times.
+  // Autotuner: times one sweep of all chains with each pair-work form (0 chunk
+  // lists, 1 row passes, 2 rows for molecules of 128+ atoms) from the same
+  // saved state, keeps the fastest and restores the state.  Returns the
+  // winner; ms_out[3] the three times.
   int autotune(int flags, double* ms_out);
   cudaStream_t stream() const { return stream_; }
   const DChains& chains() const { return ch_; }

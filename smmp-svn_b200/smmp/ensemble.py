@@ -210,14 +210,17 @@ class Ensemble:
         check(lib.smmp_ens_set_surrogate(self._h, surrogate._h if surrogate else None,
                                          float(floor), int(min_stage1)))
 
+    AUTOTUNE_FORMS = ("chunk lists", "rows", "rows for 128+ atoms")
+
     def autotune(self):
-        """Pick the faster pair-work decomposition (chunk lists or row
-        passes) by timing one sweep of each from the same saved state; the
-        state is restored.  Returns (rows_won, (ms_lists, ms_rows))."""
+        """Pick the fastest pair-work decomposition (chunk lists, row passes,
+        or row passes for molecules of 128 atoms or more) by timing one sweep
+        of each from the same saved state; the state is restored.  Returns
+        (form, (ms_lists, ms_rows, ms_by_size)), form one of AUTOTUNE_FORMS."""
         choice = ctypes.c_int()
-        ms = (ctypes.c_double * 2)()
+        ms = (ctypes.c_double * 3)()
         check(lib.smmp_ens_autotune(self._h, ctypes.byref(choice), ms))
-        return bool(choice.value), (ms[0], ms[1])
+        return self.AUTOTUNE_FORMS[choice.value], (ms[0], ms[1], ms[2])
 
     def da_stats(self):
         """(stage-1 passes, stage-2 accepts) per chain."""

@@ -1,6 +1,7 @@
-"""The autotuner: it times both pair-work decompositions from a saved state,
-keeps the faster, and leaves the ensemble's state (variables, energies,
-random streams, counters) exactly as it found it."""
+"""The autotuner: it times the pair-work decompositions (chunk lists, rows,
+rows for molecules of 128+ atoms) from a saved state, keeps the fastest, and
+leaves the ensemble's state (variables, energies, random streams, counters)
+exactly as it found it."""
 import numpy as np
 import pytest
 
@@ -23,12 +24,12 @@ def test_autotune_leaves_no_trace_and_keeps_parity(tmp_path, n):
         e.sweeps(5)
     v0, e0 = ens.vlvr(), ens.energies()
     a0, p0 = ens.acceptance()
-    rows, (ms_lists, ms_rows) = ens.autotune()
+    form, ms = ens.autotune()
     assert np.array_equal(ens.vlvr(), v0) and np.array_equal(ens.energies(), e0)
     a1, p1 = ens.acceptance()
     assert np.array_equal(a0, a1) and np.array_equal(p0, p1)
-    assert ms_lists > 0 and ms_rows > 0
-    assert rows == (ms_rows < ms_lists)
+    assert min(ms) > 0
+    assert form == Ensemble.AUTOTUNE_FORMS[int(np.argmin(ms))]
     # the random streams were restored: the next draws equal the twin's
     assert np.array_equal(ens.draw(3, 50), twin.draw(3, 50))
     ens.sweeps(5)
@@ -46,5 +47,5 @@ def test_autotune_without_row_form_is_a_no_op():
     from smmp.ensemble import Ensemble, Molecule, beta_of
     mol = Molecule(DATA + "enkefa.seq", DATA + "enkefa.var", libdir=DATA)
     ens = Ensemble([mol], [0] * 4, [1, 2, 3, 4], [beta_of(300.0)] * 4, fp32=True)
-    rows, ms = ens.autotune()
-    assert rows in (False, True)
+    form, ms = ens.autotune()
+    assert form in Ensemble.AUTOTUNE_FORMS
