@@ -398,4 +398,39 @@ double orc_bench_chains(void* h, int nchains, const int* seeds, const double* be
   return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
+// esolan.f area arithmetic on n free spheres (0-based xyz[3n], radii r[n]
+// with the probe already added): areas[n] and the return value sum_i A_i.
+// Re-orientation angles come from a stream seeded with `seed`.
+int orc_esolan_spheres(int n, const double* xyz, const double* r, int seed, double* areas,
+                       double* total) {
+  return guard([&] {
+    std::vector<double> x(n + 1), y(n + 1), z(n + 1), rv(n + 1), sg(n + 1, 1.0), as(n + 1);
+    for (int i = 1; i <= n; ++i) {
+      x[i] = xyz[3 * (i - 1)];
+      y[i] = xyz[3 * (i - 1) + 1];
+      z[i] = xyz[3 * (i - 1) + 2];
+      rv[i] = r[i - 1];
+    }
+    Smmp rng;
+    rng.sgrnd(seed);
+    *total = oracle::esolan_areas(n, x.data(), y.data(), z.data(), rv.data(), sg.data(),
+                          [&] { return rng.grnd(); }, as.data());
+    for (int i = 1; i <= n; ++i) areas[i - 1] = as[i];
+  });
+}
+
+// Per-atom SASA of the current conformation: the numerical areas of enysol
+// (surfc counts; heavy atoms with rvdw > 0) are not kept by the reference, so
+// this returns the analytic ones of esolan for all atoms (areas[natoms]).
+int orc_esolan_atoms(void* h, double* areas, double* total) {
+  Smmp* s = S(h);
+  return guard([&] {
+    int na = s->iatrs2[s->irsml2[s->ntlml]];
+    std::vector<double> sg(na + 1, 1.0), as(na + 1);
+    *total = oracle::esolan_areas(na, &s->xat_[2], &s->yat_[2], &s->zat_[2], s->rvdw.data(), sg.data(),
+                          [s] { return s->grnd(); }, as.data());
+    for (int i = 1; i <= na; ++i) areas[i - 1] = as[i];
+  });
+}
+
 }  // extern "C"

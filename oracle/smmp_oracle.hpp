@@ -12,6 +12,7 @@
 // separately rounded IEEE operation in the reference's evaluation order.
 #pragma once
 #include <cstdint>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -157,6 +158,7 @@ struct Smmp {
   double energy();
   double enyshe(int nml);
   double enysol(int nmol);
+  double esolan(int nmol);
 
   // random numbers
   void sgrnd(int32_t seed);
@@ -174,6 +176,14 @@ struct Smmp {
   double weight(const Weight& w, double x) const;
   void metropolis(double& eol1, double& acz, const Weight& w);
 };
+
+// esolan.f:12-1050 area arithmetic over atoms 1..numat (1-based arrays; radii
+// with the water probe added); returns sum_i sigma_i A_i and the areas A_i in
+// As_out[1..numat] when As_out is not null.  grnd draws the re-orientation
+// angles from the caller's stream.
+double esolan_areas(int numat, const double* x, const double* y, const double* z,
+                    const double* rvdw, const double* sigma, const std::function<double()>& grnd,
+                    double* As_out);
 
 // Angle helpers (difang.f:12-60): results wrapped into (-pi, pi].
 double difang(double a1, double a2);

@@ -278,8 +278,10 @@ double Smmp::energy() {
   if (itysol > 0) {
     esm = esm + enysol(0);
     teysl = teysl + eysl;
-  } else if (itysol < 0) {
-    throw std::runtime_error("energy: analytic solvation (esolan) is not restated here");
+  } else if (itysol < 0) {   // energy.f:79-82
+    eysl = esolan(0);
+    teysl = teysl + eysl;
+    esm = esm + eysl;
   } else {
     eysl = 0.0;
   }

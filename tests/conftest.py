@@ -85,8 +85,31 @@ class Oracle:
                       "orc_get_mt", "orc_destroy", "orc_get_toat", "orc_set_rndord",
                       "orc_get_axvr", "orc_get_names"]:
                 getattr(L, f).argtypes = None
+            L.orc_esolan_spheres.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+            L.orc_esolan_atoms.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
             cls._lib = L
         return cls._lib
+
+    @classmethod
+    def esolan_spheres(cls, xyz, radii, seed=1):
+        """esolan.f area arithmetic on free spheres: (areas, total)."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        r = np.ascontiguousarray(radii, dtype=np.float64)
+        a = np.zeros(len(r))
+        t = ctypes.c_double()
+        rc = cls.lib().orc_esolan_spheres(len(r), xyz.ctypes.data, r.ctypes.data, int(seed),
+                                          a.ctypes.data, ctypes.byref(t))
+        assert rc == 0, cls.lib().orc_last_error()
+        return a, t.value
+
+    def esolan_atoms(self):
+        """Analytic SASA of every atom of the current conformation."""
+        a = np.zeros(self.natoms)
+        t = ctypes.c_double()
+        rc = self.lib().orc_esolan_atoms(self.h, a.ctypes.data, ctypes.byref(t))
+        assert rc == 0, self.lib().orc_last_error()
+        return a, t.value
 
     def __init__(self, seq, var=None, ff="ecepp3", itysol=0, epsd=0, grpn="nh2", grpc="cooh",
                  _handle=None):
