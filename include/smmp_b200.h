@@ -43,11 +43,13 @@ extern "C" {
 
 /* Switches of the reference's COMMON blocks /epar_l/ (sh2, epsd, ientyp),
  * /isolty/ (itysol) and /updchois/ (rndord, upchswitch); INCL.H:224-327.
- * Only ientyp=0 (ECEPP/2-3), itysol in {0..9}, upchswitch=0 are on this path. */
+ * Only ientyp=0 (ECEPP/2-3), itysol in {-9..9}, upchswitch=0 are on this path
+ * (itysol < 0, the analytic SASA of esolan.f, for energy evaluations only). */
 typedef struct smmp_config {
   int sh2;        /* 1: ECEPP/2 library (lib.sh2), 0: ECEPP/3 (lib.sh3) */
   int epsd;       /* 1: sigmoidal distance-dependent dielectric */
-  int itysol;     /* 0: vacuum, 1..9: numerical SASA solvation model */
+  int itysol;     /* 0: vacuum, 1..9: numerical SASA model (enysol.f),
+                     -1..-9: analytic SASA, same parameter sets (esolan.f) */
   int ientyp;     /* must be 0 (ECEPP) */
   int rndord;     /* 1: random variable order in a sweep */
   int upchswitch; /* must be 0 (no biased Gaussian steps) */

@@ -24,7 +24,9 @@ NVFLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
 # host assembly code keeps the reference's separately rounded FP64 arithmetic
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I" + SRC, "-I" + INCLUDE]
 
-CUDA_SOURCES = ["kernels.cu", "runtime.cu", "capi.cu", "surrogate.cu"]
+CUDA_SOURCES = ["kernels.cu", "runtime.cu", "capi.cu", "surrogate.cu", "esolan.cu"]
+# the analytic SASA keeps the reference's separately rounded FP64 arithmetic
+CUDA_EXTRA = {"esolan.cu": ["-fmad=false"]}
 CXX_SOURCES = ["assembly_setup.cpp", "assembly_build.cpp", "topology.cpp"]
 
 
@@ -55,7 +57,7 @@ def build(force=False, verbose_ptxas=False):
         objs.append(obj)
         if force or _stale(obj, [src] + hdrs):
             extra = ["-Xptxas", "-v"] if verbose_ptxas else []
-            _run([NVCC] + NVFLAGS + extra + ["-c", src, "-o", obj])
+            _run([NVCC] + NVFLAGS + CUDA_EXTRA.get(f, []) + extra + ["-c", src, "-o", obj])
     for f in CXX_SOURCES:
         src = os.path.join(SRC, f)
         obj = os.path.join(OBJ, f + ".o")

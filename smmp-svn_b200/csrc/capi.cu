@@ -57,7 +57,8 @@ Config to_cfg(const smmp_config_t* c) {
   }
   need(k.ientyp == 0, "only ientyp=0 (ECEPP) is on this path");
   need(k.upchswitch == 0, "biased Gaussian steps (upchswitch!=0) are outside this path");
-  need(k.itysol >= 0 && k.itysol <= 9, "itysol must be 0 (vacuum) or a numerical SASA model 1..9");
+  need(k.itysol >= -9 && k.itysol <= 9,
+       "itysol must be 0 (vacuum), a numerical SASA model 1..9 or an analytic one -1..-9");
   return k;
 }
 

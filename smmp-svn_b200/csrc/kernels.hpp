@@ -25,6 +25,13 @@ cudaError_t launch_sweep(const DMolSet& set, const DChains& ch, const DWeight& w
 cudaError_t launch_sweep_pt(const DMolSet& set, const DChains& ch, const DWeight& w, int count,
                             int nsweeps, int flags, double check_tol, const DPTFused& pt,
                             cudaStream_t st);
+// Analytic SASA (esolan.cu): k_esolan over chains [first, first+count) adds
+// eysl to eol and terms; ch.coords must hold the chains' rebuilt coordinates.
+// scratch: esolan_scratch_bytes(count); area: nchains * tstride doubles.
+constexpr int kEsolanBatch = 16;
+size_t esolan_scratch_bytes(int count);
+cudaError_t launch_esolan(const DMolSet& set, const DChains& ch, int first, int count,
+                          double* scratch, double* area, cudaStream_t st);
 cudaError_t launch_exchange(const DChains& ch, int* temp_chain, const double* betas, int n,
                             uint32_t* mt, int* iswitch, int wrap, unsigned long long* stats,
                             cudaStream_t st);

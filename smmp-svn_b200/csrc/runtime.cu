@@ -318,6 +318,8 @@ Ensemble::~Ensemble() {
   if (own_stream_ && stream_ != own_stream_) cudaStreamSynchronize(own_stream_);
   for (void* p : allocs_) cudaFree(p);
   if (coords_buf_) cudaFree(coords_buf_);
+  if (esolan_scratch_) cudaFree(esolan_scratch_);
+  if (esolan_area_) cudaFree(esolan_area_);
   if (own_stream_) cudaStreamDestroy(own_stream_);
 }
 
@@ -446,16 +448,47 @@ void Ensemble::random_start() {
   check_cuda(cudaStreamSynchronize(stream_), "random_start sync");
 }
 
+// energy() of chains [first, first+count) (energy.f:12-119): setvar, rebuild
+// and the ECEPP/3 terms in k_energy, with the numerical SASA there when
+// itysol > 0; with itysol < 0 the rebuilt coordinates go to a buffer and
+// k_esolan adds the analytic solvation term (energy.f:79-82), a batch of
+// chains at a time.
+void Ensemble::energy_launch(int first, int count, bool fp32, bool want_coords) {
+  const bool analytic = set().f.itysol < 0;
+  DChains c2 = ch_;
+  if (analytic || want_coords) {
+    if (!coords_buf_)
+      check_cuda(cudaMalloc(&coords_buf_, (size_t)n_ * 3 * ch_.tstride * sizeof(double)), "malloc");
+    c2.coords = coords_buf_;
+  }
+  check_cuda(launch_energy(set(), c2, first, count, fp32, stream_), "energy");
+  if (!analytic) return;
+  if (!esolan_scratch_) {
+    check_cuda(cudaMalloc(&esolan_scratch_, esolan_scratch_bytes(kEsolanBatch)), "malloc");
+    check_cuda(cudaMalloc(&esolan_area_, (size_t)n_ * ch_.tstride * sizeof(double)), "malloc");
+  }
+  for (int b = first; b < first + count; b += kEsolanBatch)
+    check_cuda(launch_esolan(set(), c2, b, std::min(kEsolanBatch, first + count - b),
+                             esolan_scratch_, esolan_area_, stream_),
+               "esolan");
+}
+
+void Ensemble::require_numerical_solvation(const char* what) const {
+  if (set().f.itysol < 0)
+    throw std::runtime_error(std::string(what) +
+                             ": the analytic SASA model (itysol < 0) is built for energy "
+                             "evaluations only; sweeps need itysol >= 0");
+}
+
 void Ensemble::energy(bool fp32) {
-  check_cuda(launch_energy(set(), ch_, 0, n_, fp32, stream_), "energy");
+  energy_launch(0, n_, fp32, false);
   check_cuda(cudaStreamSynchronize(stream_), "energy sync");
 }
 
-void Ensemble::energy_chain(int c, bool fp32) {
-  check_cuda(launch_energy(set(), ch_, c, 1, fp32, stream_), "energy");
-}
+void Ensemble::energy_chain(int c, bool fp32) { energy_launch(c, 1, fp32, false); }
 
 void Ensemble::launch_sweep_range(int first, int count, int nsweeps, int flags, const DWeight& w) {
+  require_numerical_solvation("sweeps");
   double tol = (flags & kFlagFP32) ? check_tol_fp32 : check_tol;
   check_cuda(launch_sweep(set(), ch_, w, first, count, nsweeps, flags, tol, stream_), "sweep");
 }
@@ -527,6 +560,7 @@ void Ensemble::set_pt_fused(bool on, double timeout_s, unsigned barrier_extra) {
 
 void Ensemble::pt_sweeps(int nsweeps, int flags, bool serial, int graph_chunk) {
   if (pt_.n != n_) throw std::runtime_error("pt_sweeps: call set_pt first");
+  require_numerical_solvation("pt_sweeps");
   DWeight w{kWeightCanon, 0, 0, 1.0, nullptr, nullptr};
   pt_fused_last_ = false;
   if (serial) {
@@ -651,11 +685,7 @@ void Ensemble::set_toat(const std::vector<double>& t) {
 void Ensemble::get_coords(std::vector<double>& xyz) {
   // a full rebuild of every chain into a coordinate buffer (state unchanged
   // apart from the setvar call the reference's energy() also makes)
-  if (!coords_buf_)
-    check_cuda(cudaMalloc(&coords_buf_, (size_t)n_ * 3 * ch_.tstride * sizeof(double)), "malloc");
-  DChains c2 = ch_;
-  c2.coords = coords_buf_;
-  check_cuda(launch_energy(set(), c2, 0, n_, false, stream_), "coords");
+  energy_launch(0, n_, false, true);
   check_cuda(cudaStreamSynchronize(stream_), "coords sync");
   d2h(xyz, coords_buf_, (size_t)n_ * 3 * ch_.tstride);
 }

@@ -170,6 +170,12 @@ class Ensemble {
   int graph_len_ = 0, graph_flags_ = -1;
   bool pt_fused_last_ = false;   // the last batched pt_sweeps ran the fused launch
   double* coords_buf_ = nullptr;
+  // analytic SASA (itysol < 0): per-thread scratch of k_esolan for
+  // kEsolanBatch chains, the per-atom areas of every chain
+  double* esolan_scratch_ = nullptr;
+  double* esolan_area_ = nullptr;
+  void energy_launch(int first, int count, bool fp32, bool want_coords);
+  void require_numerical_solvation(const char* what) const;
 };
 
 }  // namespace smmpb200

@@ -1,0 +1,70 @@
+"""The analytic SASA model (itysol < 0, esolan.f) on the GPU against the
+oracle's restatement, through the C ABI: solvation term and total energy of
+Met-enkephalin and of the 60-residue protein on several conformations; sweeps
+with this model are refused."""
+import numpy as np
+import pytest
+
+from conftest import DATA, Oracle, seqfile
+
+pytestmark = pytest.mark.gpu
+
+
+def _confs(o, n, scale, seed):
+    rng = np.random.default_rng(seed)
+    idvr = o.idvr() - 1
+    out = [o.vlvr().copy()]
+    for _ in range(n - 1):
+        v = o.vlvr().copy()
+        v[idvr] = v[idvr] + rng.normal(0.0, scale, len(idvr))
+        out.append(v)
+    return out
+
+
+def _gpu_energies(mol, confs):
+    from smmp.ensemble import Ensemble
+    n = len(confs)
+    ens = Ensemble([mol], [0] * n, list(range(1, n + 1)), [1.0] * n)
+    V = np.zeros((n, ens.vstride))
+    for c, v in enumerate(confs):
+        V[c, :len(v)] = v
+    ens.set_vlvr(V)
+    e = ens.energy()
+    assert not ens.errors().any()
+    return e, ens.terms(), ens
+
+
+def _check(mol, o, confs):
+    got, terms, ens = _gpu_energies(mol, confs)
+    for g, t, v in zip(got, terms, confs):
+        o.set_vlvr(v[:o.ntlvr])
+        e, to = o.energy()
+        assert t[4] == pytest.approx(to[4], rel=1e-10, abs=1e-8)   # eysl
+        assert g == pytest.approx(e, rel=1e-10, abs=1e-8)
+    return ens
+
+
+def test_enkefa_analytic_solvation_matches_oracle():
+    from smmp.ensemble import Molecule
+    mol = Molecule(DATA + "enkefa.seq", DATA + "enkefa.var", libdir=DATA, itysol=-1)
+    o = Oracle(DATA + "enkefa.seq", DATA + "enkefa.var", itysol=-1)
+    _check(mol, o, _confs(o, 6, 0.3, 1))
+
+
+def test_protein60_analytic_solvation_matches_oracle(tmp_path):
+    from smmp.ensemble import Molecule
+    from smmp.sequences import natural_protein
+    s = seqfile(tmp_path, natural_protein(60), "protein60")
+    mol = Molecule(s, libdir=DATA, itysol=-1)
+    o = Oracle(s, itysol=-1)
+    _check(mol, o, _confs(o, 3, 0.05, 2))
+
+
+def test_sweeps_with_the_analytic_model_are_refused():
+    from smmp._lib import SmmpError
+    from smmp.ensemble import Ensemble, Molecule
+    mol = Molecule(DATA + "enkefa.seq", DATA + "enkefa.var", libdir=DATA, itysol=-1)
+    ens = Ensemble([mol], [0, 0], [1, 2], [1.0, 1.0])
+    ens.energy()
+    with pytest.raises(SmmpError):
+        ens.sweeps(1)
