@@ -3,6 +3,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -193,12 +194,25 @@ double universe_grnd() {
   return out[0];
 }
 
-// metropolis with a host weight callback: proposals driven from the host,
-// every energy on the GPU (metropolis.f:13-184).
-void metropolis_callback(double* eol1, double* acz, const smmp_weight_t* w) {
+// Sampling weight on the host for the host-driven sweep (canon.f:135-149,
+// mulcan_par_mod.f90:380-410), the arithmetic of the device's weight().
+double host_weight(const smmp_weight_t* w, double beta, double x) {
+  if (!w || w->kind == 0) return beta * x;
+  double v = x / w->ebin + std::copysign(0.5, x);
+  v = std::fmax((double)w->kmin, v);
+  v = std::fmin((double)w->kmax, v);
+  const int k = (int)v - w->kmin;
+  if (w->kind == 1) return (beta + w->b[k]) * x + w->alpha[k];
+  return w->b[k] * x + w->alpha[k];
+}
+
+// metropolis with proposals driven from the host and every energy() on the
+// GPU (metropolis.f:13-184): for a host weight callback, and for the
+// analytic SASA model, whose energy() may draw from the stream between a
+// proposal's numbers and its acceptance number.
+void metropolis_host(double* eol1, double* acz, const std::function<double(double)>& W) {
   Universe& u = U();
   const MolTopo& t = u.mol->topo;
-  auto W = [&](double x) { return w->callback(x, w->user); };
   std::vector<double> vl;
   double eol = universe_energy();
   for (int nsw = 0; nsw < t.nfree; ++nsw) {
@@ -354,7 +368,14 @@ int smmp_metropolis(double* eol, double* acz, const smmp_weight_t* w) {
     Universe& u = U();
     if (w && w->kind == 3) {
       need(w->callback != nullptr, "weight callback is NULL");
-      metropolis_callback(eol, acz, w);
+      metropolis_host(eol, acz, [w](double x) { return w->callback(x, w->user); });
+      return;
+    }
+    if (u.cfg.itysol < 0) {   // analytic SASA: energy() on the GPU, proposals here
+      need(!w || w->kind == 0 || (w->kmax >= w->kmin && w->b && w->alpha && w->ebin != 0.0),
+           "bad multicanonical table");
+      const double beta = u.beta;
+      metropolis_host(eol, acz, [w, beta](double x) { return host_weight(w, beta, x); });
       return;
     }
     TmpFree tmp;

@@ -1,7 +1,9 @@
 """The analytic SASA model (itysol < 0, esolan.f) on the GPU against the
 oracle's restatement, through the C ABI: solvation term and total energy of
-Met-enkephalin and of the 60-residue protein on several conformations; sweeps
-with this model are refused."""
+Met-enkephalin and of the 60-residue protein on several conformations; the
+legacy layer's metropolis with this model (proposals on the host, every
+energy() on the GPU) against the oracle's sweeps; batched sweeps with this
+model are refused."""
 import numpy as np
 import pytest
 
@@ -58,6 +60,30 @@ def test_protein60_analytic_solvation_matches_oracle(tmp_path):
     mol = Molecule(s, libdir=DATA, itysol=-1)
     o = Oracle(s, itysol=-1)
     _check(mol, o, _confs(o, 3, 0.05, 2))
+
+
+def test_legacy_metropolis_with_analytic_solvation_matches_oracle():
+    import smmp
+    smmp.reset()
+    smmp.epar_l.sh2 = 0
+    smmp.isolty.itysol = -1
+    smmp.init_energy(DATA)
+    smmp.init_molecule(1, "nh2", "cooh", DATA + "enkefa.seq", DATA + "enkefa.var")
+    o = Oracle(DATA + "enkefa.seq", DATA + "enkefa.var", itysol=-1)
+    e = smmp.energy()
+    assert e == pytest.approx(o.energy()[0], rel=1e-10)
+    smmp.sgrnd(4242)
+    o.sgrnd(4242)
+    smmp.bet.beta = 1.0 / (300 * 1.98773e-3)
+    o.set_beta(smmp.bet.beta)
+    eol, acz = e, 0.0
+    for _ in range(3):
+        eol, acz = smmp.metropolis(eol, acz, smmp.can_weight)
+        oe, _ = o.sweeps(1)
+        assert eol == pytest.approx(oe, rel=1e-10)
+        assert np.array_equal(smmp.var_r.vlvr, o.vlvr())
+    assert acz > 0
+    smmp.reset()
 
 
 def test_sweeps_with_the_analytic_model_are_refused():
