@@ -1165,6 +1165,83 @@ __global__ void k_random_start(DMolSet set, DChains ch, const int* order, int n)
   }
 }
 
+// Metropolis sweeps of the analytic SASA model, driven from the host one
+// proposal at a time across all chains (metropolis.f:13-184 with energy()
+// called per proposal, as the reference does, because esolan's random
+// re-orientation draws from the stream between a proposal's numbers and its
+// acceptance number).  One thread per chain in [first, first+n).
+// k_propose: the proposal's numbers (metropolis.f:41-60) and the new value.
+__global__ void k_propose(DMolSet set, DChains ch, int first, int n, int p, int rndord,
+                          double* vold, int* jvar) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int c = first + t;
+  const DMol& m = set.mols[ch.mol_of_chain[c]];
+  uint32_t* slot = ch.mt + (size_t)ch.mt_slot[c] * kMTWords;
+  int ivar = p;
+  if (rndord) {
+    ivar = (int)__dmul_rn((double)m.nfree, stream_next(slot));
+    if (ivar >= m.nfree) ivar = m.nfree - 1;
+  }
+  const int jv = m.idvr[ivar];
+  double* vl = ch.vlvr + (size_t)c * ch.vstride;
+  const double vo = vl[jv];
+  const double dv = __dmul_rn(m.axvr[jv], __dsub_rn(stream_next(slot), 0.5));
+  vl[jv] = addang(vo, dv);
+  vold[c] = vo;
+  jvar[c] = jv;
+}
+
+// k_decide: acceptance of the proposal whose energy() is now in ch.eol
+// (metropolis.f:72-87; -d against log r, exp only within 1e-10 of the
+// threshold, as in k_sweep); eolc holds each chain's current energy.
+__global__ void k_decide(DChains ch, DWeight w, int first, int n, const double* vold,
+                         const int* jvar, double* eolc) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int c = first + t;
+  const double enw = ch.eol[c], eol = eolc[c], beta = ch.beta[c];
+  const double delta = __dsub_rn(weight(w, beta, enw), weight(w, beta, eol));
+  int up;
+  if (delta <= 0.0) {
+    up = 1;
+  } else {
+    uint32_t* slot = ch.mt + (size_t)ch.mt_slot[c] * kMTWords;
+    const double rd = stream_next(slot);
+    const double d = fmin(delta, 100.0);
+    const double margin = -d - (rd > 0.0 ? log(rd) : -INFINITY);
+    if (margin > 1e-10) up = 1;
+    else if (margin < -1e-10) up = 0;
+    else up = exp(-d) >= rd ? 1 : 0;
+  }
+  if (up) {
+    eolc[c] = enw;
+    ch.nacc[c] += 1;
+  } else {
+    ch.vlvr[(size_t)c * ch.vstride + jvar[c]] = vold[c];
+  }
+  ch.nprop[c] += 1;
+  if (!isfinite(enw) && ch.err[c] == 0) ch.err[c] = kErrNonFinite;
+}
+
+// k_close: the closing energy() is in ch.eol; consistency check
+// (metropolis.f:172-179), then eol is the tracked energy again.
+__global__ void k_close(DChains ch, int first, int n, const double* eolc, int check,
+                        double check_tol) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int c = first + t;
+  const double eol = eolc[c], enew = ch.eol[c];
+  if (check && fabs(eol - enew) > check_tol && eol < 100000.0 && ch.err[c] == 0)
+    ch.err[c] = kErrConsistency;
+  ch.eol[c] = eol;
+}
+
+__global__ void k_copy_eol(DChains ch, int first, int n, double* eolc) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) eolc[first + t] = ch.eol[first + t];
+}
+
 // energy(): setvar + rebuild + energy for chains [first, first+gridDim.x).
 // The dihedral state is updated in place exactly as the reference's energy()
 // does; terms and eol of each chain receive the result.
@@ -2019,6 +2096,26 @@ cudaError_t launch_draw(uint32_t* mt, int slot, int n, double* out, cudaStream_t
 cudaError_t launch_random_start(const DMolSet& set, const DChains& ch, const int* order, int n,
                                 cudaStream_t st) {
   k_random_start<<<1, 1, 0, st>>>(set, ch, order, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_propose(const DMolSet& set, const DChains& ch, int first, int n, int p,
+                           int rndord, double* vold, int* jvar, cudaStream_t st) {
+  k_propose<<<(n + 127) / 128, 128, 0, st>>>(set, ch, first, n, p, rndord, vold, jvar);
+  return cudaGetLastError();
+}
+cudaError_t launch_decide(const DChains& ch, const DWeight& w, int first, int n,
+                          const double* vold, const int* jvar, double* eolc, cudaStream_t st) {
+  k_decide<<<(n + 127) / 128, 128, 0, st>>>(ch, w, first, n, vold, jvar, eolc);
+  return cudaGetLastError();
+}
+cudaError_t launch_close(const DChains& ch, int first, int n, const double* eolc, int check,
+                         double check_tol, cudaStream_t st) {
+  k_close<<<(n + 127) / 128, 128, 0, st>>>(ch, first, n, eolc, check, check_tol);
+  return cudaGetLastError();
+}
+cudaError_t launch_copy_eol(const DChains& ch, int first, int n, double* eolc, cudaStream_t st) {
+  k_copy_eol<<<(n + 127) / 128, 128, 0, st>>>(ch, first, n, eolc);
   return cudaGetLastError();
 }
 

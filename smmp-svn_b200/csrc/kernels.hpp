@@ -25,6 +25,16 @@ cudaError_t launch_sweep(const DMolSet& set, const DChains& ch, const DWeight& w
 cudaError_t launch_sweep_pt(const DMolSet& set, const DChains& ch, const DWeight& w, int count,
                             int nsweeps, int flags, double check_tol, const DPTFused& pt,
                             cudaStream_t st);
+// Metropolis steps of the analytic SASA model, driven from the host: the
+// proposal p of chains [first, first+n), the decision after its energy(),
+// the closing check; eolc holds the tracked energies.
+cudaError_t launch_propose(const DMolSet& set, const DChains& ch, int first, int n, int p,
+                           int rndord, double* vold, int* jvar, cudaStream_t st);
+cudaError_t launch_decide(const DChains& ch, const DWeight& w, int first, int n,
+                          const double* vold, const int* jvar, double* eolc, cudaStream_t st);
+cudaError_t launch_close(const DChains& ch, int first, int n, const double* eolc, int check,
+                         double check_tol, cudaStream_t st);
+cudaError_t launch_copy_eol(const DChains& ch, int first, int n, double* eolc, cudaStream_t st);
 // Analytic SASA (esolan.cu): k_esolan over chains [first, first+count) adds
 // eysl to eol and terms; ch.coords must hold the chains' rebuilt coordinates.
 // scratch: esolan_scratch_bytes(count); area: nchains * tstride doubles.

@@ -320,6 +320,9 @@ Ensemble::~Ensemble() {
   if (coords_buf_) cudaFree(coords_buf_);
   if (esolan_scratch_) cudaFree(esolan_scratch_);
   if (esolan_area_) cudaFree(esolan_area_);
+  if (an_vold_) cudaFree(an_vold_);
+  if (an_jvar_) cudaFree(an_jvar_);
+  if (an_eolc_) cudaFree(an_eolc_);
   if (own_stream_) cudaStreamDestroy(own_stream_);
 }
 
@@ -473,11 +476,47 @@ void Ensemble::energy_launch(int first, int count, bool fp32, bool want_coords) 
                "esolan");
 }
 
-void Ensemble::require_numerical_solvation(const char* what) const {
-  if (set().f.itysol < 0)
-    throw std::runtime_error(std::string(what) +
-                             ": the analytic SASA model (itysol < 0) is built for energy "
-                             "evaluations only; sweeps need itysol >= 0");
+// Metropolis sweeps with the analytic SASA model (itysol < 0) for chains
+// [first, first+count): metropolis.f:13-184 with one energy() per proposal,
+// as the reference calls it, because esolan may draw from the chain's stream
+// between a proposal's numbers and its acceptance number.  Each proposal is
+// three launches over all chains: k_propose, energy(), k_decide.
+void Ensemble::sweeps_analytic(int first, int count, int nsweeps, int flags, const DWeight& w) {
+  if (flags & kFlagExtraSetvar)
+    throw std::runtime_error("the serial PT schedule is not built for the analytic SASA model");
+  if (ch_.sur.w1 != nullptr)
+    throw std::runtime_error("delayed acceptance is not built for the analytic SASA model");
+  int nfree = -1;
+  for (int c = first; c < first + count; ++c) {   // no chain may see an extra energy()
+    const int nf = mols_[chain_mol_[c]]->topo.nfree;
+    if (nfree >= 0 && nf != nfree)
+      throw std::runtime_error("analytic SASA sweeps: chains of one launch need the same free "
+                               "dihedrals");
+    nfree = nf;
+  }
+  if (!an_vold_) {
+    check_cuda(cudaMalloc(&an_vold_, n_ * sizeof(double)), "malloc");
+    check_cuda(cudaMalloc(&an_jvar_, n_ * sizeof(int)), "malloc");
+    check_cuda(cudaMalloc(&an_eolc_, n_ * sizeof(double)), "malloc");
+  }
+  const bool fp32 = (flags & kFlagFP32) != 0;
+  const int rnd = (flags & kFlagRndOrd) ? 1 : 0;
+  const double tol = fp32 ? check_tol_fp32 : check_tol;
+  for (int sw = 0; sw < nsweeps; ++sw) {
+    energy_launch(first, count, fp32, false);   // metropolis.f:35
+    check_cuda(launch_copy_eol(ch_, first, count, an_eolc_, stream_), "copy eol");
+    for (int p = 0; p < nfree; ++p) {
+      check_cuda(launch_propose(set(), ch_, first, count, p, rnd, an_vold_, an_jvar_, stream_),
+                 "propose");
+      energy_launch(first, count, fp32, false);
+      check_cuda(launch_decide(ch_, w, first, count, an_vold_, an_jvar_, an_eolc_, stream_),
+                 "decide");
+    }
+    energy_launch(first, count, fp32, false);   // metropolis.f:172-179
+    check_cuda(launch_close(ch_, first, count, an_eolc_, (flags & kFlagNoCheck) ? 0 : 1, tol,
+                            stream_),
+               "close");
+  }
 }
 
 void Ensemble::energy(bool fp32) {
@@ -488,7 +527,10 @@ void Ensemble::energy(bool fp32) {
 void Ensemble::energy_chain(int c, bool fp32) { energy_launch(c, 1, fp32, false); }
 
 void Ensemble::launch_sweep_range(int first, int count, int nsweeps, int flags, const DWeight& w) {
-  require_numerical_solvation("sweeps");
+  if (set().f.itysol < 0) {
+    sweeps_analytic(first, count, nsweeps, flags, w);
+    return;
+  }
   double tol = (flags & kFlagFP32) ? check_tol_fp32 : check_tol;
   check_cuda(launch_sweep(set(), ch_, w, first, count, nsweeps, flags, tol, stream_), "sweep");
 }
@@ -560,7 +602,6 @@ void Ensemble::set_pt_fused(bool on, double timeout_s, unsigned barrier_extra) {
 
 void Ensemble::pt_sweeps(int nsweeps, int flags, bool serial, int graph_chunk) {
   if (pt_.n != n_) throw std::runtime_error("pt_sweeps: call set_pt first");
-  require_numerical_solvation("pt_sweeps");
   DWeight w{kWeightCanon, 0, 0, 1.0, nullptr, nullptr};
   pt_fused_last_ = false;
   if (serial) {
@@ -573,6 +614,16 @@ void Ensemble::pt_sweeps(int nsweeps, int flags, bool serial, int graph_chunk) {
                  "exchange");
       check_cuda(cudaStreamSynchronize(stream_), "pt sync");
     }
+    return;
+  }
+  if (set().f.itysol < 0) {   // analytic SASA: host-driven sweeps, then the exchange
+    for (int s = 0; s < nsweeps; ++s) {
+      launch_sweep_range(0, n_, 1, flags, w);
+      check_cuda(launch_exchange(ch_, pt_.temp_chain, pt_.betas, n_, pt_.mt, pt_.iswitch, pt_.wrap,
+                                 pt_.stats, stream_),
+                 "exchange");
+    }
+    check_cuda(cudaStreamSynchronize(stream_), "pt sync");
     return;
   }
   double tol = (flags & kFlagFP32) ? check_tol_fp32 : check_tol;

@@ -174,8 +174,13 @@ class Ensemble {
   // kEsolanBatch chains, the per-atom areas of every chain
   double* esolan_scratch_ = nullptr;
   double* esolan_area_ = nullptr;
+  // host-driven sweeps of the analytic model: old value, variable and
+  // tracked energy of each chain's current proposal
+  double* an_vold_ = nullptr;
+  int* an_jvar_ = nullptr;
+  double* an_eolc_ = nullptr;
   void energy_launch(int first, int count, bool fp32, bool want_coords);
-  void require_numerical_solvation(const char* what) const;
+  void sweeps_analytic(int first, int count, int nsweeps, int flags, const DWeight& w);
 };
 
 }  // namespace smmpb200

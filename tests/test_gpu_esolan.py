@@ -2,8 +2,8 @@
 oracle's restatement, through the C ABI: solvation term and total energy of
 Met-enkephalin and of the 60-residue protein on several conformations; the
 legacy layer's metropolis with this model (proposals on the host, every
-energy() on the GPU) against the oracle's sweeps; batched sweeps with this
-model are refused."""
+energy() on the GPU) and batched sweeps of several chains (proposal, energy()
+and decision launched across the chains) against the oracle's sweeps."""
 import numpy as np
 import pytest
 
@@ -86,11 +86,43 @@ def test_legacy_metropolis_with_analytic_solvation_matches_oracle():
     smmp.reset()
 
 
-def test_sweeps_with_the_analytic_model_are_refused():
-    from smmp._lib import SmmpError
-    from smmp.ensemble import Ensemble, Molecule
+def test_batched_sweeps_with_analytic_solvation_match_oracle():
+    """Four chains, each on its own stream: every proposal's energy() runs the
+    analytic SASA; after every sweep the variables equal the oracle's
+    metropolis on each chain (bit for bit) and the energies agree to 1e-10."""
+    from smmp.ensemble import Ensemble, Molecule, beta_of
     mol = Molecule(DATA + "enkefa.seq", DATA + "enkefa.var", libdir=DATA, itysol=-1)
-    ens = Ensemble([mol], [0, 0], [1, 2], [1.0, 1.0])
-    ens.energy()
-    with pytest.raises(SmmpError):
+    b = beta_of(300.0)
+    seeds = [901, 902, 903, 904]
+    ens = Ensemble([mol], [0] * 4, seeds, [b] * 4)
+    oracles = []
+    V = np.zeros((4, ens.vstride))
+    for c, sd in enumerate(seeds):
+        o = Oracle(DATA + "enkefa.seq", DATA + "enkefa.var", itysol=-1)
+        o.sgrnd(sd)
+        o.set_beta(b)
+        oracles.append(o)
+        V[c, :o.ntlvr] = o.vlvr()
+    ens.set_vlvr(V)
+    for k in range(3):
         ens.sweeps(1)
+        V, E = ens.vlvr(), ens.energies()
+        for c, o in enumerate(oracles):
+            oe, _ = o.sweeps(1)
+            assert np.array_equal(V[c, :o.ntlvr], o.vlvr()), (c, k)
+            assert E[c] == pytest.approx(oe, rel=1e-10)
+    assert not ens.errors().any()
+    acc, prop = ens.acceptance()
+    assert (prop == 3 * 24).all() and (acc > 0).all()
+
+
+def test_pt_with_analytic_solvation_runs():
+    from smmp.ensemble import Ensemble, Molecule, beta_of
+    mol = Molecule(DATA + "enkefa.seq", DATA + "enkefa.var", libdir=DATA, itysol=-1)
+    betas = [beta_of(t) for t in (300.0, 450.0, 700.0, 1000.0)]
+    ens = Ensemble([mol], [0] * 4, [11, 12, 13, 14], betas)
+    ens.set_pt(betas, wrap=False, exchange_seed=5)
+    ens.pt_sweeps(2)
+    assert not ens.errors().any()
+    assert sorted(ens.pt_map().tolist()) == [0, 1, 2, 3]
+    assert not ens.pt_fused_last()
