@@ -42,7 +42,7 @@ constexpr size_t kEsDoubles = 8 * kEsNb + 4 * kEsVert + 6 * kEsCircle;
 constexpr size_t kEsInts = 5 * (kEsNb + 2) + 2 * kEsNb + 2;
 constexpr size_t kEsPerThread = kEsDoubles + (kEsInts + 1) / 2;
 
-__device__ __forceinline__ double sq(double x) { return x * x; }   // Fortran x**2
+__host__ __device__ __forceinline__ double sq(double x) { return x * x; }   // Fortran x**2
 
 struct EsWork {
   double* dd;     // [4p + 0..3]: radius, x, y, z of neighbour p relative to atom i
@@ -52,7 +52,7 @@ struct EsWork {
   int *neib, *neibp, *fullarc, *al, *ta2, *atom;
 };
 
-__device__ EsWork es_work(double* base) {
+__host__ __device__ EsWork es_work(double* base) {
   EsWork w;
   double* p = base;
   w.dd = p;
@@ -94,9 +94,11 @@ enum EsStatus : int { kEsDone = 0, kEsNeedsDraws = 1, kEsOverflow = 2, kEsCoinci
 // position p in the neighbour list (neighbours in atom order, as the
 // reference's atom numbers order them); list entries neib[1..] hold p.
 // Without DRAW an atom that needs the random re-orientation returns
-// kEsNeedsDraws and draws nothing.
+// kEsNeedsDraws and draws nothing.  Host-callable so that a CPU test can
+// check this arithmetic against the oracle bit for bit (the library itself
+// calls it only from k_esolan).
 template <bool DRAW>
-__device__ int esolan_atom(const DMol& m, const double* xyz, int i, EsWork& w, uint32_t* slot,
+__host__ __device__ int esolan_atom(const DMol& m, const double* xyz, int i, EsWork& w, uint32_t* slot,
                            double* area) {
   const double R = m.rvdw[i];
   double As = kPi4E * (R * R);
