@@ -110,6 +110,10 @@ int smmp_setvar(int nml, const double* vlvrx);
  * eol and acz are updated in place as the f2py intent(in,out) arguments. */
 int smmp_metropolis(double* eol, double* acz, const smmp_weight_t* w);
 
+/* outvar(nml, fileName): outvar.f:12.  The current variables in the .var
+ * command language; fileName "" (or blanks): standard output.  nml 0 or 1. */
+int smmp_outvar(int nml, const char* fileName);
+
 /* sgrnd(seed) / grnd(): smmp.pyf:5620, twister.f:64 and :104. */
 int smmp_sgrnd(int32_t seed);
 double smmp_grnd(void);
@@ -153,6 +157,14 @@ int smmp_mol_info(const smmp_mol_t* m, long long info[6]);
 /* 0-based indices (into the molecule's variables) of its free dihedrals, in
  * idvr order (redvar.f); info[2] of them. */
 int smmp_mol_idvr(const smmp_mol_t* m, int* idvr);
+/* The molecule's variables as built (library values, then the .var file's
+ * settings; redvar.f): vlvr[nvar] in radians. */
+int smmp_mol_vlvr0(const smmp_mol_t* m, double* vlvr);
+/* outvar.f:50-121 (outvbs) for one molecule, host only: the text outvar
+ * writes for variables vlvr (radians, all variables of the molecule), with
+ * molecule number iml in the line prefix.  buf NULL: *len = the bytes needed
+ * (final NUL included); else *len is buf's size on entry. */
+int smmp_mol_outvar(const smmp_mol_t* m, const double* vlvr, int iml, char* buf, uint64_t* len);
 /* An ensemble of nchains chains; chain c is a copy of mols[chain_mol[c]].
  * betas[c] is its inverse temperature.  shared_stream=0: chain c draws from
  * its own MT19937 stream seeded seeds[c]; shared_stream=1: all chains share

@@ -398,6 +398,27 @@ int smmp_metropolis(double* eol, double* acz, const smmp_weight_t* w) {
   });
 }
 
+int smmp_outvar(int nml, const char* fileName) {
+  return guard([&] {
+    require_molecule();
+    need(nml == 0 || nml == 1, "outvar: no such molecule (one molecule on this path)");
+    Universe& u = U();
+    std::vector<double> vl;
+    u.ens->get_vlvr(vl);
+    const std::string s = outvar_text(u.mol->topo, vl.data(), 1);
+    if (fileName && fileName[0] != '\0' && std::string(fileName).find_first_not_of(' ') !=
+                                                   std::string::npos) {
+      std::FILE* f = std::fopen(fileName, "w");
+      need(f != nullptr, "outvar: cannot open the file");
+      std::fputs(s.c_str(), f);
+      std::fclose(f);
+    } else {
+      std::fputs(s.c_str(), stdout);
+      std::fflush(stdout);
+    }
+  });
+}
+
 int smmp_sgrnd(int32_t seed) {
   return guard([&] {
     Universe& u = U();
@@ -607,6 +628,27 @@ int smmp_mol_info(const smmp_mol_t* m, long long info[6]) {
     info[3] = t.npairs;
     info[4] = (long long)t.heavy.size();
     info[5] = t.nres;
+  });
+}
+
+int smmp_mol_outvar(const smmp_mol_t* m, const double* vlvr, int iml, char* buf,
+                    uint64_t* len) {
+  return guard([&] {
+    need(m && vlvr && len, "NULL argument");
+    const std::string s = outvar_text(m->m->topo, vlvr, iml);
+    if (buf) {
+      need(*len >= s.size() + 1, "buffer too small");
+      std::memcpy(buf, s.c_str(), s.size() + 1);
+    }
+    *len = s.size() + 1;
+  });
+}
+
+int smmp_mol_vlvr0(const smmp_mol_t* m, double* vlvr) {
+  return guard([&] {
+    need(m && vlvr, "NULL argument");
+    const MolTopo& t = m->m->topo;
+    for (size_t k = 0; k < t.vlvr0.size(); ++k) vlvr[k] = t.vlvr0[k];
   });
 }
 

@@ -2,6 +2,8 @@
 #include "topology.hpp"
 
 #include <algorithm>
+#include <cstdio>
+#include <string>
 #include <cmath>
 #include <stdexcept>
 
@@ -229,6 +231,35 @@ MolTopo flatten(Assembly& a, int nml) {
   }
   t.rows_ok = ok;
   return t;
+}
+
+// outvar.f:50-121.  crd is the reference's literal (INCL.H:41), not 180/pi.
+std::string outvar_text(const MolTopo& t, const double* vlvr, int iml) {
+  const double crd = 57.2957795130823;
+  char mlfd[32], line[256];
+  std::snprintf(mlfd, sizeof mlfd, "%4d : ", iml);   // (i4,a3)
+  std::string out;
+  bool any = false;
+  for (int k = 0; k < 6; ++k) any = any || t.gbpr[k] != 0.0;
+  if (any) {   // '@' line of the global parameters: (1x,2a,1x,12a), f17.6 trimmed
+    out += " @ ";
+    out += mlfd;
+    out += " ";
+    for (int k = 0; k < 6; ++k) {
+      std::snprintf(line, sizeof line, "%.6f", k < 3 ? t.gbpr[k] : t.gbpr[k] * crd);
+      out += line;
+      if (k < 5) out += ",";
+    }
+    out += "\n";
+  }
+  for (int v = 0; v < t.nvar; ++v) {   // (3x,a,i3,1x,a,1x,a,1x,a,1x,f10.3[,1x,a])
+    std::string name = t.var_name[v];
+    name.resize(3, ' ');   // character nmvr*3
+    std::snprintf(line, sizeof line, "   %s%3d : %s : %10.3f%s\n", mlfd, t.var_residue[v] + 1,
+                  name.c_str(), vlvr[v] * crd, t.var_fixed[v] ? "  &" : "");
+    out += line;   // every variable of these libraries is a torsion (ityvr = 3)
+  }
+  return out;
 }
 
 }  // namespace smmpb200

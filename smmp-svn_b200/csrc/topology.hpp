@@ -82,6 +82,11 @@ struct MolTopo {
   int nres = 0;
 };
 
+// outvar.f:50-121 (outvbs) for one molecule: the text outvar writes for the
+// variables vlvr (radians, all t.nvar of them), with molecule number iml in
+// each line's prefix.
+std::string outvar_text(const MolTopo& t, const double* vlvr, int iml);
+
 // Build a MolTopo from molecule nml of an assembled system.
 MolTopo flatten(Assembly& a, int nml);
 ForceField make_forcefield(const Assembly& a);

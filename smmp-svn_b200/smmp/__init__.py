@@ -23,7 +23,7 @@ import numpy as np
 from . import _lib
 from ._lib import SmmpError, check, lib
 
-__all__ = ["init_energy", "init_molecule", "energy", "setvar", "metropolis", "sgrnd",
+__all__ = ["init_energy", "init_molecule", "energy", "setvar", "metropolis", "outvar", "sgrnd",
            "grnd", "canon", "anneal", "can_weight", "MucaWeight", "SmmpError",
            "epar_l", "isolty", "updchois", "bet", "mol_par", "var_r", "var_i", "eny_r",
            "updstats", "gpu_available", "reset", "coordinates"]
@@ -268,6 +268,12 @@ def metropolis(eol, acz, dummy=None):
     check(lib.smmp_metropolis(ctypes.byref(e), ctypes.byref(a), ctypes.byref(ws)))
     del keep
     return e.value, a.value
+
+
+def outvar(nml, fileName=""):
+    """outvar(nml, fileName) -- outvar.f:12: the current variables in the .var
+    command language, to the file or (fileName blank) to standard output."""
+    check(lib.smmp_outvar(int(nml), (fileName or "").encode()))
 
 
 def sgrnd(seed):

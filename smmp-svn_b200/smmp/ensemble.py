@@ -52,6 +52,21 @@ class Molecule:
         idvr = np.zeros(max(self.nvr, 1), dtype=np.int32)
         check(lib.smmp_mol_idvr(self._h, idvr.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
         self.idvr = idvr[:self.nvr]          # 0-based variable index of each free dihedral
+        v0 = np.zeros(max(self.nvar, 1))
+        check(lib.smmp_mol_vlvr0(self._h, v0.ctypes.data_as(_D)))
+        self.vlvr0 = v0[:self.nvar]          # variables as built (library, then .var file)
+
+    def outvar(self, vlvr, iml=1):
+        """Text of outvar.f (outvbs, outvar.f:50-121) for the variables vlvr
+        (radians, all nvar of them); iml is the molecule number printed."""
+        v = np.ascontiguousarray(vlvr, dtype=np.float64)
+        if len(v) < self.nvar:
+            raise ValueError("vlvr needs all %d variables" % self.nvar)
+        n = ctypes.c_uint64(0)
+        check(lib.smmp_mol_outvar(self._h, v.ctypes.data_as(_D), int(iml), None, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value)
+        check(lib.smmp_mol_outvar(self._h, v.ctypes.data_as(_D), int(iml), buf, ctypes.byref(n)))
+        return buf.value.decode()
 
     def __del__(self):
         if getattr(self, "_h", None):

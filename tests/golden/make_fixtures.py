@@ -67,6 +67,13 @@ def main(ref):
             "lowest": fnum(ann[44].split()[-1]),
             "lowest_sweep": int(ann[44].split()[-2]),
         },
+        # annealing.f:139 calls outvar(0, ' '): the final conformation in the
+        # .var command language, as outvar.f:50-121 formats it
+        "anneal_outvar": {
+            "source": "EXAMPLES/annealing.out:20-43; EXAMPLES/annealing.f:139",
+            "setup": "enkefa.seq + enkefa.ann, ECEPP/2",
+            "lines": ann[19:43],
+        },
     }
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(golden, f, indent=1)
