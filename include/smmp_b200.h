@@ -113,6 +113,9 @@ int smmp_metropolis(double* eol, double* acz, const smmp_weight_t* w);
 /* outvar(nml, fileName): outvar.f:12.  The current variables in the .var
  * command language; fileName "" (or blanks): standard output.  nml 0 or 1. */
 int smmp_outvar(int nml, const char* fileName);
+/* outpdb(nml, fileName): outpdb.f:12.  The current conformation (rebuilt
+ * from the variables) in PDB format; fileName "" (or blanks): standard output. */
+int smmp_outpdb(int nml, const char* fileName);
 
 /* sgrnd(seed) / grnd(): smmp.pyf:5620, twister.f:64 and :104. */
 int smmp_sgrnd(int32_t seed);
@@ -165,6 +168,10 @@ int smmp_mol_vlvr0(const smmp_mol_t* m, double* vlvr);
  * molecule number iml in the line prefix.  buf NULL: *len = the bytes needed
  * (final NUL included); else *len is buf's size on entry. */
 int smmp_mol_outvar(const smmp_mol_t* m, const double* vlvr, int iml, char* buf, uint64_t* len);
+/* outpdb.f:12-185 for one molecule, host only: PDB text (80-column ATOM/HETATM,
+ * TER, CONECT and END lines) of coordinates xyz[3*natoms] (Angstrom).  buf
+ * and *len as for smmp_mol_outvar. */
+int smmp_mol_outpdb(const smmp_mol_t* m, const double* xyz, char* buf, uint64_t* len);
 /* An ensemble of nchains chains; chain c is a copy of mols[chain_mol[c]].
  * betas[c] is its inverse temperature.  shared_stream=0: chain c draws from
  * its own MT19937 stream seeded seeds[c]; shared_stream=1: all chains share

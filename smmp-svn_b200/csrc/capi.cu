@@ -398,6 +398,20 @@ int smmp_metropolis(double* eol, double* acz, const smmp_weight_t* w) {
   });
 }
 
+// Text to a file, or to standard output when the name is empty or blank
+// (ibegst(fileName) = 0 in outvar.f:38 / outpdb.f:62).
+void write_text(const std::string& s, const char* fileName, const char* who) {
+  if (fileName && std::string(fileName).find_first_not_of(' ') != std::string::npos) {
+    std::FILE* f = std::fopen(fileName, "w");
+    if (!f) throw std::invalid_argument(std::string(who) + ": cannot open the file");
+    std::fputs(s.c_str(), f);
+    std::fclose(f);
+  } else {
+    std::fputs(s.c_str(), stdout);
+    std::fflush(stdout);
+  }
+}
+
 int smmp_outvar(int nml, const char* fileName) {
   return guard([&] {
     require_molecule();
@@ -405,17 +419,18 @@ int smmp_outvar(int nml, const char* fileName) {
     Universe& u = U();
     std::vector<double> vl;
     u.ens->get_vlvr(vl);
-    const std::string s = outvar_text(u.mol->topo, vl.data(), 1);
-    if (fileName && fileName[0] != '\0' && std::string(fileName).find_first_not_of(' ') !=
-                                                   std::string::npos) {
-      std::FILE* f = std::fopen(fileName, "w");
-      need(f != nullptr, "outvar: cannot open the file");
-      std::fputs(s.c_str(), f);
-      std::fclose(f);
-    } else {
-      std::fputs(s.c_str(), stdout);
-      std::fflush(stdout);
-    }
+    write_text(outvar_text(u.mol->topo, vl.data(), 1), fileName, "outvar");
+  });
+}
+
+int smmp_outpdb(int nml, const char* fileName) {
+  return guard([&] {
+    require_molecule();
+    need(nml == 0 || nml == 1, "outpdb: no such molecule (one molecule on this path)");
+    Universe& u = U();
+    std::vector<double> xyz;
+    u.ens->get_coords(xyz);   // the rebuild of the current variables
+    write_text(outpdb_text(u.mol->topo, xyz.data()), fileName, "outpdb");
   });
 }
 
@@ -636,6 +651,18 @@ int smmp_mol_outvar(const smmp_mol_t* m, const double* vlvr, int iml, char* buf,
   return guard([&] {
     need(m && vlvr && len, "NULL argument");
     const std::string s = outvar_text(m->m->topo, vlvr, iml);
+    if (buf) {
+      need(*len >= s.size() + 1, "buffer too small");
+      std::memcpy(buf, s.c_str(), s.size() + 1);
+    }
+    *len = s.size() + 1;
+  });
+}
+
+int smmp_mol_outpdb(const smmp_mol_t* m, const double* xyz, char* buf, uint64_t* len) {
+  return guard([&] {
+    need(m && xyz && len, "NULL argument");
+    const std::string s = outpdb_text(m->m->topo, xyz);
     if (buf) {
       need(*len >= s.size() + 1, "buffer too small");
       std::memcpy(buf, s.c_str(), s.size() + 1);

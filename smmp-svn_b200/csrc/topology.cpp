@@ -88,6 +88,33 @@ MolTopo flatten(Assembly& a, int nml) {
     if (a.rvdw[i] > 0.0) t.heavy.push_back(k);
   }
   t.nres = a.irsml2[nml] - a.irsml1[nml] + 1;
+  // outpdb.f:137-176: bonded partners j > i (the first atom of the molecule
+  // also lists its parent), only for atoms with bonds
+  t.conect_off.assign(1, 0);
+  for (int r = a.irsml1[nml]; r <= a.irsml2[nml]; ++r) {
+    t.res_name.push_back(a.seq[r]);
+    t.res_atom0.push_back(A(a.iatrs1[r]));
+    for (int i = a.iatrs1[r]; i <= a.iatrs2[r]; ++i) {
+      if (a.nbdat[i] > 0) {
+        int ibd[4], jj;
+        if (r == a.irsml1[nml] && i == a.iatrs1[r]) {
+          ibd[0] = a.iowat[i];
+          ibd[1] = a.IBD(1, i);
+          ibd[2] = a.IBD(2, i);
+          ibd[3] = a.IBD(3, i);
+          jj = 4;
+        } else {
+          ibd[0] = a.IBD(1, i);
+          ibd[1] = a.IBD(2, i);
+          ibd[2] = a.IBD(3, i);
+          jj = 3;
+        }
+        for (int j = 0; j < jj; ++j)
+          if (ibd[j] > i) t.conect.push_back(A(ibd[j]));
+      }
+      t.conect_off.push_back((int)t.conect.size());
+    }
+  }
   // depth levels in bldmol order (every atom but i1 is built from its parent)
   std::vector<int> depth(n, -1);
   depth[t.i1] = 0;
@@ -259,6 +286,67 @@ std::string outvar_text(const MolTopo& t, const double* vlvr, int iml) {
                   name.c_str(), vlvr[v] * crd, t.var_fixed[v] ? "  &" : "");
     out += line;   // every variable of these libraries is a torsion (ityvr = 3)
   }
+  return out;
+}
+
+// outpdb.f:12-185 for a system of one molecule (chain id blank, atom
+// numbers from 1).  Lines are 80 characters, blank-filled, as (a80) writes
+// them; the formats are outpdb.f:181-183.
+std::string outpdb_text(const MolTopo& t, const double* xyz) {
+  auto pad80 = [](std::string s) {
+    s.resize(80, ' ');
+    return s + "\n";
+  };
+  auto upper = [](std::string s) {
+    for (char& ch : s)
+      if (ch >= 'a' && ch <= 'z') ch = char(ch - 'a' + 'A');
+    return s;
+  };
+  std::string out, res;
+  char line[128];
+  int iat = 0;
+  for (int r = 0; r < t.nres; ++r) {
+    const std::string raw = t.res_name[r].substr(0, 3);
+    const char* linty = (raw != "ace" && raw != "nme") ? "ATOM  " : "HETATM";
+    res = upper(raw);
+    res.resize(3, ' ');
+    const int a1 = t.res_atom0[r], a2 = r + 1 < t.nres ? t.res_atom0[r + 1] : t.natoms;
+    for (int i = a1; i < a2; ++i) {
+      ++iat;
+      std::string nm = t.atom_name[i];
+      nm.resize(4, ' ');
+      std::string atnm = " " + nm;   // atnm(2:5) = nmat(i)
+      if (atnm[1] == 'h') {           // hydrogens: a trailing digit moves to column 1
+        const size_t j = atnm.find_last_not_of(' ');
+        if (j != std::string::npos && atnm[j] >= '0' && atnm[j] <= '9') {
+          atnm[0] = atnm[j];
+          atnm[j] = ' ';
+        }
+      }
+      atnm = upper(atnm);
+      // (a6,i5,1x,a5,a3,1x,a1,i4,a1,3x,3f8.3,2(1x,f5.2))
+      std::snprintf(line, sizeof line, "%s%5d %s%s  %4d    %8.3f%8.3f%8.3f %5.2f %5.2f", linty,
+                    iat, atnm.c_str(), res.c_str(), r + 1, xyz[3 * i], xyz[3 * i + 1],
+                    xyz[3 * i + 2], 1.0, 0.0);
+      out += pad80(line);
+    }
+  }
+  ++iat;
+  std::snprintf(line, sizeof line, "TER   %5d      %s  ", iat, res.c_str());   // (a6,i5,6x,a3,1x,a1)
+  out += pad80(line);
+  for (int i = 0; i < t.natoms; ++i) {   // (a6,5i5)
+    const int b = t.conect_off[i], e = t.conect_off[i + 1];
+    if (e == b) continue;
+    std::string l = "CONECT";
+    std::snprintf(line, sizeof line, "%5d", i + 1);
+    l += line;
+    for (int k = b; k < e; ++k) {
+      std::snprintf(line, sizeof line, "%5d", t.conect[k] + 1);
+      l += line;
+    }
+    out += pad80(l);
+  }
+  out += pad80("END");
   return out;
 }
 

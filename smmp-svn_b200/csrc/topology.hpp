@@ -80,12 +80,20 @@ struct MolTopo {
   // solvation
   std::vector<int> heavy;              // atoms with rvdw > 0
   int nres = 0;
+  // output (outpdb.f): residue names (seq, lower case), first atom of each
+  // residue, and CSR of each atom's bonded partners after it, in outpdb order
+  std::vector<std::string> res_name;
+  std::vector<int> res_atom0;
+  std::vector<int> conect_off, conect;
 };
 
 // outvar.f:50-121 (outvbs) for one molecule: the text outvar writes for the
 // variables vlvr (radians, all t.nvar of them), with molecule number iml in
 // each line's prefix.
 std::string outvar_text(const MolTopo& t, const double* vlvr, int iml);
+// outpdb.f:12-185 for the only molecule of a system: PDB text (80-column
+// lines: ATOM/HETATM, TER, CONECT, END) of coordinates xyz[3*natoms].
+std::string outpdb_text(const MolTopo& t, const double* xyz);
 
 // Build a MolTopo from molecule nml of an assembled system.
 MolTopo flatten(Assembly& a, int nml);

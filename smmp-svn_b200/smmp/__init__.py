@@ -23,7 +23,8 @@ import numpy as np
 from . import _lib
 from ._lib import SmmpError, check, lib
 
-__all__ = ["init_energy", "init_molecule", "energy", "setvar", "metropolis", "outvar", "sgrnd",
+__all__ = ["init_energy", "init_molecule", "energy", "setvar", "metropolis", "outvar", "outpdb",
+           "sgrnd",
            "grnd", "canon", "anneal", "can_weight", "MucaWeight", "SmmpError",
            "epar_l", "isolty", "updchois", "bet", "mol_par", "var_r", "var_i", "eny_r",
            "updstats", "gpu_available", "reset", "coordinates"]
@@ -274,6 +275,12 @@ def outvar(nml, fileName=""):
     """outvar(nml, fileName) -- outvar.f:12: the current variables in the .var
     command language, to the file or (fileName blank) to standard output."""
     check(lib.smmp_outvar(int(nml), (fileName or "").encode()))
+
+
+def outpdb(nml, fileName=""):
+    """outpdb(nml, fileName) -- outpdb.f:12: the current conformation in PDB
+    format, to the file or (fileName blank) to standard output."""
+    check(lib.smmp_outpdb(int(nml), (fileName or "").encode()))
 
 
 def sgrnd(seed):

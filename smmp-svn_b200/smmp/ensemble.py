@@ -68,6 +68,18 @@ class Molecule:
         check(lib.smmp_mol_outvar(self._h, v.ctypes.data_as(_D), int(iml), buf, ctypes.byref(n)))
         return buf.value.decode()
 
+    def outpdb(self, xyz):
+        """PDB text of outpdb.f (outpdb.f:12-185) for coordinates xyz
+        (natoms x 3, Angstrom)."""
+        x = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1)
+        if len(x) < 3 * self.natoms:
+            raise ValueError("xyz needs %d atoms" % self.natoms)
+        n = ctypes.c_uint64(0)
+        check(lib.smmp_mol_outpdb(self._h, x.ctypes.data_as(_D), None, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value)
+        check(lib.smmp_mol_outpdb(self._h, x.ctypes.data_as(_D), buf, ctypes.byref(n)))
+        return buf.value.decode()
+
     def __del__(self):
         if getattr(self, "_h", None):
             lib.smmp_mol_free(self._h)

@@ -182,6 +182,19 @@ class Oracle:
         assert rc == 0, self.lib().orc_last_error()
         return eol.value, acz.value
 
+    def atom_table(self):
+        """Per atom (1-based atom numbers): ityat, iowat, nbdat, ibdat(1..3), ..."""
+        na, nv = self.natoms, self.ntlvr
+        ai = np.zeros((na, 11), np.int32)
+        ad = np.zeros((na, 4))
+        vi = np.zeros((nv, 9), np.int32)
+        ms = np.zeros((self.sizes[6], 2), np.int32)
+        vw = np.zeros((self.sizes[4], 3), np.int32)
+        l14 = np.zeros((self.sizes[5], 2), np.int32)
+        P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        self.lib().orc_get_topology(self.h, P(ai), P(ad), P(vi), P(ms), P(vw), P(l14))
+        return ai
+
     def pair_count(self):
         na, nv = self.natoms, self.ntlvr
         ai = np.zeros((na, 11), np.int32)
