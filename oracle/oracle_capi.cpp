@@ -398,6 +398,15 @@ double orc_bench_chains(void* h, int nchains, const int* seeds, const double* be
   return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
+// gradient.f: energy (vacuum) and dE/dvlvr of every variable (grad[ntlvr]).
+int orc_gradient(void* h, double* e, double* grad) {
+  Smmp* s = S(h);
+  return guard([&] {
+    *e = s->gradient();
+    for (int i = 1; i <= ntlvr(s); ++i) grad[i - 1] = s->gdeyvr[i];
+  });
+}
+
 // esolan.f area arithmetic on n free spheres (0-based xyz[3n], radii r[n]
 // with the probe already added): areas[n] and the return value sum_i A_i.
 // Re-orientation angles come from a stream seeded with `seed`.

@@ -159,6 +159,10 @@ struct Smmp {
   double enyshe(int nml);
   double enysol(int nmol);
   double esolan(int nmol);
+  // gradient (gradient.f, opeshe.f): energy and gdeyvr[iv] = dE/dvlvr[iv]
+  double opeshe(int nml);
+  double gradient();
+  std::vector<double> gdeyvr;
 
   // random numbers
   void sgrnd(int32_t seed);

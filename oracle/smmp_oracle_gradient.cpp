@@ -1,0 +1,174 @@
+// CPU oracle -- TEST INFRASTRUCTURE ONLY (see smmp_oracle.hpp).
+//
+// gradient.f:12-70 and opeshe.f:12-317: the ECEPP/3 energy of a molecule and
+// its derivatives with respect to the variables, by the recursive force and
+// torque sums over the moving sets (Noguti and Go 1984; Abe, Braun, Noguti
+// and Go 1984), in the reference's loop order: variables in descending
+// order, the atoms of each variable's moving sets, their van der Waals and
+// 1-4 partners, then the sums carried over from the variables added to it.
+#include <cmath>
+#include <stdexcept>
+#include <vector>
+
+#include "smmp_oracle.hpp"
+
+namespace oracle {
+
+// opeshe.f:12-317: energy terms of molecule nml (eyel, eyvw, eyhb, eyvr,
+// eysm) and gdeyvr[iv] = dE/d(variable iv) for its variables.
+double Smmp::opeshe(int nml) {
+  eyel = eyvw = eyhb = eyvr = eysm = 0.0;
+  const int ntlvr = nvrml[nml];
+  if (ntlvr == 0) return 0.0;
+  const int ifivr = ivrml1[nml], ilavr = ifivr + ntlvr - 1;
+  if ((int)gdeyvr.size() < ilavr + 1) gdeyvr.assign(ilavr + 1, 0.0);
+  std::vector<double> xfvr(ilavr + 1, 0.0), yfvr(ilavr + 1, 0.0), zfvr(ilavr + 1, 0.0),
+      xfrvr(ilavr + 1, 0.0), yfrvr(ilavr + 1, 0.0), zfrvr(ilavr + 1, 0.0);
+  const int ifiat = iatrs1[irsml1[nml]], ilaat = iatrs2[irsml2[nml]];
+  std::vector<double> xfat(ilaat + 1, 0.0), yfat(ilaat + 1, 0.0), zfat(ilaat + 1, 0.0);
+  for (int i = ifivr; i <= ilavr; ++i) gdeyvr[i] = 0.0;
+  (void)ifiat;
+
+  int i1s = imsml1[nml] + nmsml[nml];
+  int i1a = iadml1[nml] + nadml[nml];
+
+  // one pair (i, j): energies and the force on j from i (opeshe.f:165-225)
+  auto pair = [&](int i, int j, bool is14, double cqi, int ity, double xi, double yi, double zi,
+                  double& xfi, double& yfi, double& zfi) {
+    const int jty = ityat[j];
+    const double xij = xat(j) - xi, yij = yat(j) - yi, zij = zat(j) - zi;
+    const double rij2 = xij * xij + yij * yij + zij * zij;
+    const double rij4 = rij2 * rij2;
+    const double rij6 = rij4 * rij2;
+    const double rij = std::sqrt(rij2);
+    double eel, deel;
+    if (epsd) {
+      const double sr = slp * rij;
+      const double sr2 = sr * sr;
+      const double xsr = (plt - 1.0) * std::exp(-sr) / 2.0;
+      const double ep = plt - (sr2 + 2.0 * sr + 2.0) * xsr;
+      eel = cqi * cgat[j] / (rij * ep);
+      deel = eel + cqi * cgat[j] * (slp * sr2 * xsr) / (ep * ep);
+    } else {
+      eel = cqi * cgat[j] / rij;
+      deel = eel;
+    }
+    eyel = eyel + eel;
+    double c;
+    if (ihbty[ity][jty] != 0) {
+      const double eyrp = ahb[ity][jty] / (rij6 * rij6);
+      const double eyds = chb[ity][jty] / (rij6 * rij4);
+      eyhb = eyhb + eyrp - eyds;
+      c = (-12.0 * eyrp + 10.0 * eyds - deel) / rij2;
+    } else {
+      const double eyrp = (is14 ? a14[ity][jty] : aij[ity][jty]) / (rij6 * rij6);
+      const double eyds = cij[ity][jty] / rij6;
+      eyvw = eyvw + eyrp - eyds;
+      c = (-12.0 * eyrp + 6.0 * eyds - deel) / rij2;
+    }
+    const double xfji = c * xij, yfji = c * yij, zfji = c * zij;
+    xfi = xfi + xfji;
+    yfi = yfi + yfji;
+    zfi = zfi + zfji;
+    xfat[j] = xfat[j] - xfji;
+    yfat[j] = yfat[j] - yfji;
+    zfat[j] = zfat[j] - zfji;
+  };
+
+  for (int io = ilavr; io >= ifivr; --io) {   // variables in descending order
+    const int iv = iorvr[io];
+    const int ia = iatvr[iv];
+    const int ib = iowat[ia];
+    const double xb = xat(ib), yb = yat(ib), zb = zat(ib);
+    const int it = ityvr[iv], ic = iclvr[iv];
+    double fvr = 0.0, ex = 0.0, ey = 0.0, ez = 0.0;
+    if (it == 3) {   // torsion
+      ex = xtoat[ib];
+      ey = ytoat[ib];
+      ez = ztoat[ib];
+      const double vr = toat[ia];
+      const double e0 = e0to[ic];
+      if (e0 != 0.0) {
+        const double vrn = vr * rnto[ic];
+        eyvr = eyvr + e0 * (1.0 + sgto[ic] * std::cos(vrn));
+        fvr = esnto[ic] * std::sin(vrn);   // force from the variable
+      }
+    } else if (it == 2) {   // bond angle
+      ex = xbaat[ia];
+      ey = ybaat[ia];
+      ez = zbaat[ia];
+    } else if (it == 1) {   // bond length
+      ex = xtoat[ia];
+      ey = ytoat[ia];
+      ez = ztoat[ia];
+    }
+
+    double xfiv = 0.0, yfiv = 0.0, zfiv = 0.0, xfriv = 0.0, yfriv = 0.0, zfriv = 0.0;
+    const int i2s = i1s - 1;   // last moving set of iv
+    i1s = imsvr1[iv];          // first
+    for (int ims = i1s; ims <= i2s; ++ims) {
+      for (int i = latms1[ims]; i <= latms2[ims]; ++i) {
+        const int ity = ityat[i];
+        const double cqi = conv * cgat[i];
+        const double xi = xat(i), yi = yat(i), zi = zat(i);
+        double xfi = xfat[i], yfi = yfat[i], zfi = zfat[i];
+        for (int ivw = ivwat1[i]; ivw <= ivwat2[i]; ++ivw)
+          for (int j = lvwat1[ivw]; j <= lvwat2[ivw]; ++j)
+            pair(i, j, false, cqi, ity, xi, yi, zi, xfi, yfi, zfi);
+        for (int i14 = i14at1[i]; i14 <= i14at2[i]; ++i14)
+          pair(i, l14at[i14], true, cqi, ity, xi, yi, zi, xfi, yfi, zfi);
+        xfat[i] = xfi;
+        yfat[i] = yfi;
+        zfat[i] = zfi;
+        xfiv = xfiv + xfi;
+        yfiv = yfiv + yfi;
+        zfiv = zfiv + zfi;
+        xfriv = xfriv + yfi * zi - zfi * yi;
+        yfriv = yfriv + zfi * xi - xfi * zi;
+        zfriv = zfriv + xfi * yi - yfi * xi;
+      }
+    }
+    const int i2a = i1a - 1;   // last variable added to iv
+    i1a = iadvr1[iv];          // first
+    for (int iad = i1a; iad <= i2a; ++iad) {
+      const int lad = ladvr[iad];
+      xfiv = xfiv + xfvr[lad];
+      yfiv = yfiv + yfvr[lad];
+      zfiv = zfiv + zfvr[lad];
+      xfriv = xfriv + xfrvr[lad];
+      yfriv = yfriv + yfrvr[lad];
+      zfriv = zfriv + zfrvr[lad];
+    }
+    xfvr[iv] = xfiv;
+    yfvr[iv] = yfiv;
+    zfvr[iv] = zfiv;
+    xfrvr[iv] = xfriv;
+    yfrvr[iv] = yfriv;
+    zfrvr[iv] = zfriv;
+    if (it == 3 || it == 2)
+      gdeyvr[iv] = (ey * zb - ez * yb) * xfiv + (ez * xb - ex * zb) * yfiv +
+                   (ex * yb - ey * xb) * zfiv + ex * xfriv + ey * yfriv + ez * zfriv - fvr;
+    else if (it == 1)
+      gdeyvr[iv] = -(ex * xfiv + ey * yfiv + ez * zfiv) - fvr;
+  }
+  eysm = eyel + eyvw + eyhb + eyvr;
+  return eysm;
+}
+
+// gradient.f:12-70 for the vacuum model (itysol = 0); the reference stops
+// for itysol > 0, and opesol (itysol < 0) is not restated.
+double Smmp::gradient() {
+  if (itysol != 0)
+    throw std::runtime_error("gradient: only the vacuum model (itysol = 0) is restated");
+  double esm = 0.0;
+  for (int i = 1; i <= ntlml; ++i) {
+    setvar(i, vlvr.data());
+    opeshe(i);
+    esm = esm + eysm;
+    eysl = 0.0;
+  }
+  eysm = esm;
+  return esm;
+}
+
+}  // namespace oracle

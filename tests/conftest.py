@@ -88,8 +88,17 @@ class Oracle:
             L.orc_esolan_spheres.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                              ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
             L.orc_esolan_atoms.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+            L.orc_gradient.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
             cls._lib = L
         return cls._lib
+
+    def gradient(self):
+        """gradient.f: (energy, dE/dvlvr of every variable)."""
+        e = ctypes.c_double()
+        g = np.zeros(self.ntlvr)
+        rc = self.lib().orc_gradient(self.h, ctypes.byref(e), g.ctypes.data_as(ctypes.c_void_p))
+        assert rc == 0, self.lib().orc_last_error()
+        return e.value, g
 
     @classmethod
     def esolan_spheres(cls, xyz, radii, seed=1):

@@ -1,0 +1,53 @@
+"""The oracle's restatement of gradient.f / opeshe.f (energy derivatives with
+respect to the dihedrals, the recursive force and torque sums): its energy is
+the oracle's energy() and its derivatives equal central finite differences of
+that energy, for ECEPP/3, ECEPP/2 and the sigmoidal dielectric."""
+import numpy as np
+import pytest
+
+from conftest import DATA, Oracle
+
+
+def _check(o, v, h=1e-5):
+    o.set_vlvr(v)
+    e, g = o.gradient()
+    e0, _ = o.energy()
+    assert e == pytest.approx(e0, rel=1e-13, abs=1e-10)
+    num = np.zeros(len(v))
+    for k in range(len(v)):
+        vp = v.copy()
+        vp[k] += h
+        o.set_vlvr(vp)
+        ep, _ = o.energy()
+        vm = v.copy()
+        vm[k] -= h
+        o.set_vlvr(vm)
+        em, _ = o.energy()
+        num[k] = (ep - em) / (2 * h)
+    o.set_vlvr(v)
+    # central differences: truncation ~h^2, cancellation ~1e-16 * (largest
+    # term) / h, which the largest derivative bounds
+    tol = 1e-5 * np.maximum(1.0, np.abs(num)) + 1e-8 * np.abs(num).max()
+    assert np.all(np.abs(g - num) <= tol), np.c_[g, num]
+
+
+@pytest.mark.parametrize("ff,epsd", [("ecepp3", 0), ("ecepp2", 0), ("ecepp3", 1)])
+def test_gradient_equals_finite_differences(ff, epsd):
+    o = Oracle(DATA + "enkefa.seq", DATA + "enkefa.var", ff=ff, epsd=epsd)
+    v0 = o.vlvr().copy()
+    _check(o, v0)
+    rng = np.random.default_rng(11)
+    idvr = o.idvr() - 1
+    for _ in range(2):
+        v = v0.copy()
+        v[idvr] = v[idvr] + rng.normal(0.0, 0.05, len(idvr))
+        _check(o, v)
+
+
+def test_gradient_refuses_numerical_solvation():
+    o = Oracle(DATA + "enkefa.seq", DATA + "enkefa.var", itysol=1)
+    lib = o.lib()
+    import ctypes
+    e = ctypes.c_double()
+    g = np.zeros(o.ntlvr)
+    assert lib.orc_gradient(o.h, ctypes.byref(e), g.ctypes.data_as(ctypes.c_void_p)) != 0
