@@ -3,6 +3,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <algorithm>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -404,6 +405,23 @@ int orc_gradient(void* h, double* e, double* grad) {
   return guard([&] {
     *e = s->gradient();
     for (int i = 1; i <= ntlvr(s); ++i) grad[i - 1] = s->gdeyvr[i];
+  });
+}
+
+// minim.f (quasi-Newton, no regularisation): *nop function calls; log
+// receives up to logcap (energy, |grad|^2) pairs, *nlog the number of pairs.
+int orc_minim(void* h, int imin, int maxit, double eps, int* nop, double* log, int logcap,
+              int* nlog) {
+  Smmp* s = S(h);
+  return guard([&] {
+    std::vector<double> lg;
+    *nop = s->minim(imin, maxit, eps, &lg);
+    const int np = (int)lg.size() / 2;
+    *nlog = np;
+    for (int k = 0; k < std::min(np, logcap); ++k) {
+      log[2 * k] = lg[2 * k];
+      log[2 * k + 1] = lg[2 * k + 1];
+    }
   });
 }
 

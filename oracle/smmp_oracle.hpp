@@ -163,6 +163,11 @@ struct Smmp {
   double opeshe(int nml);
   double gradient();
   std::vector<double> gdeyvr;
+  // minimisation (minim.f imin = 1, minqsn.f); log: (energy, |grad|^2) per call
+  int minim(int imin, int maxit, double eps, std::vector<double>* log);
+  int minqsn(int n, double* x, double& f, double* g, const double* scal, double acur,
+             int maxfun, std::vector<double>* log);
+  void minim_move(int n, double& f, const double* x, double* g, std::vector<double>* log);
 
   // random numbers
   void sgrnd(int32_t seed);

@@ -89,6 +89,9 @@ class Oracle:
                                              ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
             L.orc_esolan_atoms.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
             L.orc_gradient.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+            L.orc_minim.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                    ctypes.c_void_p]
             cls._lib = L
         return cls._lib
 
@@ -99,6 +102,16 @@ class Oracle:
         rc = self.lib().orc_gradient(self.h, ctypes.byref(e), g.ctypes.data_as(ctypes.c_void_p))
         assert rc == 0, self.lib().orc_last_error()
         return e.value, g
+
+    def minim(self, imin=1, maxit=10000, eps=1e-9):
+        """minim.f: (function calls, [(energy, |grad|^2) of every call])."""
+        nop, nlog = ctypes.c_int(), ctypes.c_int()
+        cap = 100000
+        log = np.zeros(2 * cap)
+        rc = self.lib().orc_minim(self.h, int(imin), int(maxit), float(eps), ctypes.byref(nop),
+                                  log.ctypes.data_as(ctypes.c_void_p), cap, ctypes.byref(nlog))
+        assert rc == 0, self.lib().orc_last_error()
+        return nop.value, log[:2 * min(nlog.value, cap)].reshape(-1, 2)
 
     @classmethod
     def esolan_spheres(cls, xyz, radii, seed=1):

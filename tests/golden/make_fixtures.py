@@ -67,6 +67,23 @@ def main(ref):
             "lowest": fnum(ann[44].split()[-1]),
             "lowest_sweep": int(ann[44].split()[-2]),
         },
+        # README:389-514: EXAMPLES/minimization.f (enkefa.seq + enkefa.var,
+        # ECEPP/3, quasi-Newton, maxit 10000, eps 1e-9): one line per
+        # function call (energy, squared gradient; E13.6), the final energy
+        # terms and the final free variables (degrees, one decimal)
+        "minim_enkefa": {
+            "source": "README:395-480 (steps), README:484-486 (energies), "
+                      "README:490-513 (variables); EXAMPLES/minimization.f",
+            "steps": [[ln.split(":")[1].split()[1], ln.split("(")[1].split(")")[0].strip()]
+                      for ln in readme[394:480] if ln.strip().startswith("Step")],
+            "total": fnum(readme[483].split()[1]),
+            "coulomb": fnum(readme[484].split()[1]),
+            "lennard_jones": fnum(readme[484].split()[3]),
+            "hbond": fnum(readme[484].split()[5]),
+            "torsion": fnum(readme[485].split()[1]),
+            "variables": [[ln.split()[0], int(ln.split()[1]), float(ln.split()[2])]
+                          for ln in readme[489:513] if ln.strip()],
+        },
         # annealing.f:139 calls outvar(0, ' '): the final conformation in the
         # .var command language, as outvar.f:50-121 formats it
         "anneal_outvar": {
