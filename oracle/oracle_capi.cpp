@@ -408,6 +408,17 @@ int orc_gradient(void* h, double* e, double* grad) {
   });
 }
 
+// The order-free form of the same derivatives (total atomic forces, sums
+// over each variable's moved atoms), for tests of that formulation.
+int orc_gradient_by_sums(void* h, double* grad) {
+  Smmp* s = S(h);
+  return guard([&] {
+    std::vector<double> gd;
+    s->gradient_by_sums(1, gd);
+    for (int i = 1; i <= ntlvr(s); ++i) grad[i - 1] = gd[i];
+  });
+}
+
 // minim.f (quasi-Newton, no regularisation): *nop function calls; log
 // receives up to logcap (energy, |grad|^2) pairs, *nlog the number of pairs.
 int orc_minim(void* h, int imin, int maxit, double eps, int* nop, double* log, int logcap,

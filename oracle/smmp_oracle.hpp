@@ -163,6 +163,7 @@ struct Smmp {
   double opeshe(int nml);
   double gradient();
   std::vector<double> gdeyvr;
+  void gradient_by_sums(int nml, std::vector<double>& gd);   // order-free form (tests)
   // minimisation (minim.f imin = 1, minqsn.f); log: (energy, |grad|^2) per call
   int minim(int imin, int maxit, double eps, std::vector<double>* log);
   int minqsn(int n, double* x, double& f, double* g, const double* scal, double acur,

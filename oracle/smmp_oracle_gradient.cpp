@@ -171,4 +171,86 @@ double Smmp::gradient() {
   return esm;
 }
 
+// The same derivatives without the ordered recursion: total force on every
+// atom from all of its pairs, then for each variable the force and torque
+// sums over the atoms it moves (its moving sets and, recursively, those of
+// the variables added to it).  This is the order-free form a parallel
+// implementation computes; test infrastructure checks it against opeshe.
+void Smmp::gradient_by_sums(int nml, std::vector<double>& gd) {
+  setvar(nml, vlvr.data());
+  const int ifivr = ivrml1[nml], ilavr = ifivr + nvrml[nml] - 1;
+  const int ifiat = iatrs1[irsml1[nml]], ilaat = iatrs2[irsml2[nml]];
+  std::vector<double> fx(ilaat + 1, 0.0), fy(ilaat + 1, 0.0), fz(ilaat + 1, 0.0);
+  auto force = [&](int i, int j, bool is14) {
+    const int ity = ityat[i], jty = ityat[j];
+    const double cqi = conv * cgat[i];
+    const double xij = xat(j) - xat(i), yij = yat(j) - yat(i), zij = zat(j) - zat(i);
+    const double rij2 = xij * xij + yij * yij + zij * zij;
+    const double rij4 = rij2 * rij2, rij6 = rij4 * rij2, rij = std::sqrt(rij2);
+    double deel;
+    if (epsd) {
+      const double sr = slp * rij, sr2 = sr * sr;
+      const double xsr = (plt - 1.0) * std::exp(-sr) / 2.0;
+      const double ep = plt - (sr2 + 2.0 * sr + 2.0) * xsr;
+      const double eel = cqi * cgat[j] / (rij * ep);
+      deel = eel + cqi * cgat[j] * (slp * sr2 * xsr) / (ep * ep);
+    } else {
+      deel = cqi * cgat[j] / rij;
+    }
+    double c;
+    if (ihbty[ity][jty] != 0)
+      c = (-12.0 * ahb[ity][jty] / (rij6 * rij6) + 10.0 * chb[ity][jty] / (rij6 * rij4) - deel) /
+          rij2;
+    else
+      c = (-12.0 * (is14 ? a14[ity][jty] : aij[ity][jty]) / (rij6 * rij6) +
+           6.0 * cij[ity][jty] / rij6 - deel) /
+          rij2;
+    fx[i] += c * xij;
+    fy[i] += c * yij;
+    fz[i] += c * zij;
+    fx[j] -= c * xij;
+    fy[j] -= c * yij;
+    fz[j] -= c * zij;
+  };
+  for (int i = ifiat; i <= ilaat; ++i) {
+    for (int ivw = ivwat1[i]; ivw <= ivwat2[i]; ++ivw)
+      for (int j = lvwat1[ivw]; j <= lvwat2[ivw]; ++j) force(i, j, false);
+    for (int i14 = i14at1[i]; i14 <= i14at2[i]; ++i14) force(i, l14at[i14], true);
+  }
+  // the atoms each variable moves: its moving sets, then the variables added
+  // to it (whose indices the descending order has already completed)
+  std::vector<std::vector<int>> moved(ilavr + 1);
+  int i1s = imsml1[nml] + nmsml[nml], i1a = iadml1[nml] + nadml[nml];
+  gd.assign(ilavr + 1, 0.0);
+  for (int io = ilavr; io >= ifivr; --io) {
+    const int iv = iorvr[io];
+    const int i2s = i1s - 1;
+    i1s = imsvr1[iv];
+    for (int ims = i1s; ims <= i2s; ++ims)
+      for (int i = latms1[ims]; i <= latms2[ims]; ++i) moved[iv].push_back(i);
+    const int i2a = i1a - 1;
+    i1a = iadvr1[iv];
+    for (int iad = i1a; iad <= i2a; ++iad) {
+      const std::vector<int>& m = moved[ladvr[iad]];
+      moved[iv].insert(moved[iv].end(), m.begin(), m.end());
+    }
+    double sx = 0, sy = 0, sz = 0, tx = 0, ty = 0, tz = 0;
+    for (int i : moved[iv]) {
+      sx += fx[i];
+      sy += fy[i];
+      sz += fz[i];
+      tx += fy[i] * zat(i) - fz[i] * yat(i);
+      ty += fz[i] * xat(i) - fx[i] * zat(i);
+      tz += fx[i] * yat(i) - fy[i] * xat(i);
+    }
+    const int ia = iatvr[iv], ib = iowat[ia], ic = iclvr[iv];
+    const double ex = xtoat[ib], ey = ytoat[ib], ez = ztoat[ib];
+    const double xb = xat(ib), yb = yat(ib), zb = zat(ib);
+    double fvr = 0.0;
+    if (e0to[ic] != 0.0) fvr = esnto[ic] * std::sin(toat[ia] * rnto[ic]);
+    gd[iv] = (ey * zb - ez * yb) * sx + (ez * xb - ex * zb) * sy + (ex * yb - ey * xb) * sz +
+             ex * tx + ey * ty + ez * tz - fvr;
+  }
+}
+
 }  // namespace oracle

@@ -44,6 +44,28 @@ def test_gradient_equals_finite_differences(ff, epsd):
         _check(o, v)
 
 
+@pytest.mark.parametrize("ff,epsd", [("ecepp3", 0), ("ecepp2", 0), ("ecepp3", 1)])
+def test_order_free_sums_equal_the_recursion(ff, epsd):
+    """Total atomic forces from all pairs, then each variable's force and
+    torque sums over the atoms it moves (the form a parallel gradient kernel
+    computes) give opeshe's derivatives to rounding."""
+    import ctypes
+    o = Oracle(DATA + "enkefa.seq", DATA + "enkefa.var", ff=ff, epsd=epsd)
+    lib = o.lib()
+    lib.orc_gradient_by_sums.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    rng = np.random.default_rng(3)
+    idvr = o.idvr() - 1
+    for k in range(3):
+        v = o.vlvr().copy()
+        if k:
+            v[idvr] = v[idvr] + rng.normal(0.0, 0.05, len(idvr))
+        o.set_vlvr(v)
+        _, g = o.gradient()
+        g2 = np.zeros(o.ntlvr)
+        assert lib.orc_gradient_by_sums(o.h, g2.ctypes.data_as(ctypes.c_void_p)) == 0
+        assert np.abs(g - g2).max() <= 1e-12 * np.abs(g).max()
+
+
 def test_gradient_refuses_numerical_solvation():
     o = Oracle(DATA + "enkefa.seq", DATA + "enkefa.var", itysol=1)
     lib = o.lib()
