@@ -13,7 +13,7 @@ from conftest import DATA, Oracle, seqfile
 
 pytestmark = pytest.mark.gpu
 
-TOL_FP32 = 1e-3       # kcal/mol, north_star bar for FP32 pair terms
+TOL_FP32 = 1e-3       # kcal/mol, the required accuracy of FP32 pair terms
 
 
 def ensemble(mol, n, fp32=False, seeds=None, betas=None):
