@@ -164,6 +164,8 @@ struct Smmp {
   double gradient();
   std::vector<double> gdeyvr;
   void gradient_by_sums(int nml, std::vector<double>& gd);   // order-free form (tests)
+  // opesol.f: eysl and gdeysl[iv] = d(eysl)/d(variable iv) (itysol < 0)
+  void opesol(int nml, std::vector<double>& gdeysl);
   // minimisation (minim.f imin = 1, minqsn.f); log: (energy, |grad|^2) per call
   int minim(int imin, int maxit, double eps, std::vector<double>* log);
   int minqsn(int n, double* x, double& f, double* g, const double* scal, double acur,
@@ -187,13 +189,14 @@ struct Smmp {
   void metropolis(double& eol1, double& acz, const Weight& w);
 };
 
-// esolan.f:12-1050 area arithmetic over atoms 1..numat (1-based arrays; radii
-// with the water probe added); returns sum_i sigma_i A_i and the areas A_i in
-// As_out[1..numat] when As_out is not null.  grnd draws the re-orientation
-// angles from the caller's stream.
+// esolan.f:12-1050 over atoms 1..numat (1-based arrays; radii with the water
+// probe added); returns sum_i sigma_i A_i, the areas A_i in As_out[1..numat]
+// and gradan[3j + k] = sum_i sigma_i dA_i/dr_jk (esolan.f:1034-1042) when
+// those are not null.  grnd draws the re-orientation angles from the
+// caller's stream.
 double esolan_areas(int numat, const double* x, const double* y, const double* z,
                     const double* rvdw, const double* sigma, const std::function<double()>& grnd,
-                    double* As_out);
+                    double* As_out, double* gradan = nullptr);
 
 // Angle helpers (difang.f:12-60): results wrapped into (-pi, pi].
 double difang(double a1, double a2);

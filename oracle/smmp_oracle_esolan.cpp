@@ -8,6 +8,7 @@
 // neighbour list and the random re-orientation that draws from the global
 // MT19937 stream follow the Fortran statement by statement.  Arrays are
 // 1-based as in the reference.
+#include <algorithm>
 #include <cmath>
 #include <functional>
 #include <stdexcept>
@@ -29,7 +30,7 @@ inline double sq(double x) { return x * x; }   // Fortran x**2
 // sum_i sigma_i A_i and, when As_out is given, A_i in As_out[1..numat].
 double esolan_areas(int numat, const double* xa, const double* ya, const double* za,
                     const double* rvdw, const double* sigma, const std::function<double()>& grnd,
-                    double* As_out) {
+                    double* As_out, double* gradan) {
   auto xat = [&](int i) { return xa[i]; };
   auto yat = [&](int i) { return ya[i]; };
   auto zat = [&](int i) { return za[i]; };
@@ -50,10 +51,20 @@ double esolan_areas(int numat, const double* xa, const double* ya, const double*
   };
   std::vector<Vertex> vertex(1);   // 1-based
   std::vector<double> ayx1, ax1, ax2, ay1, ay2, probe;
+  std::vector<int> ivrx;
+  // gradient row of atom i: grad(i, j, 1..3) (esolan.f:553-575, 718-902)
+  std::vector<double> gr(gradan ? 3 * (numat + 1) : 0);
+  if (gradan)
+    for (int j = 0; j < 3 * (numat + 1); ++j) gradan[j] = 0.0;
 
   const double rdpcut = (double)1e-10f;   // esolan.f:133, a single-precision literal
 
   for (int i = 1; i <= numat; ++i) {   // do 1 i = 1, numat
+    if (gradan) std::fill(gr.begin(), gr.end(), 0.0);
+    bool assemble = false;   // label 11 reached with the circles known
+    int ifu_g = 0, ine_g = 0;
+    double cf = 0, sf = 0, cg = 0, sg = 0;
+    int jjj = 0;
     do {   // one pass; `break` is the Fortran `goto 1` / `goto 11`
       const double R = rvdw[i];
       int jj = 0;
@@ -87,7 +98,6 @@ double esolan_areas(int numat, const double* xa, const double* ya, const double*
 
       // north point too close to an intersection line: random re-orientation
       // (esolan.f:180-238)
-      int jjj = 0;
       int k = neib[1];
       double ddp = std::fabs(sq(DD(k, 2)) + sq(DD(k, 3)) + sq(R - DD(k, 4)) - pol[k]);
       for (int j = 2; j <= neib[0]; ++j) {
@@ -95,7 +105,6 @@ double esolan_areas(int numat, const double* xa, const double* ya, const double*
         double ddp2 = std::fabs(sq(DD(k, 2)) + sq(DD(k, 3)) + sq(R - DD(k, 4)) - pol[k]);
         if (ddp2 < ddp) ddp = ddp2;
       }
-      double cf = 0, sf = 0, cg = 0, sg = 0;
       while (ddp < 1.0e-6) {
         ++jjj;
         double uga = grnd();
@@ -282,14 +291,44 @@ double esolan_areas(int numat, const double* xa, const double* ya, const double*
       fullarc[0] = ifu;
       al[0] = ifu;
 
+      assemble = gradan != nullptr;
+      ifu_g = ifu;
+      ine_g = ine;
       for (int q = 1; q <= ifu; ++q) {   // esolan.f:533-578
         const double a = NB(fullarc[q], 1), aia = a < 0.0 ? -1.0 : 1.0;
         const double b = NB(fullarc[q], 2), c = NB(fullarc[q], 3), d = NB(fullarc[q], 4);
-        if (a != 0.0)
+        if (a != 0.0) {
           As[i] = As[i] - aia * R22p *
                               (1.0 + (-(d / a) - R42) * std::fabs(a) /
                                          std::sqrt(sq(R42 * a - d) + R42 * (b * b + c * c)));
-        else
+          if (gradan) {   // esolan.f:547-569
+            const int fk = fullarc[q];
+            double dadx[5][4];
+            dadx[1][1] = 2.0 * DD(fk, 2);
+            dadx[1][2] = 2.0 * DD(fk, 3);
+            dadx[1][3] = 2.0 * (DD(fk, 4) - R);
+            dadx[2][1] = -8.0 * pol[i];
+            dadx[2][2] = 0.0;
+            dadx[2][3] = 0.0;
+            dadx[3][1] = 0.0;
+            dadx[3][2] = dadx[2][1];
+            dadx[3][3] = 0.0;
+            dadx[4][1] = 8.0 * pol[i] * DD(fk, 2);
+            dadx[4][2] = 8.0 * pol[i] * DD(fk, 3);
+            dadx[4][3] = 8.0 * pol[i] * (DD(fk, 4) + R);
+            const double R42p = R22p + R22p;
+            const double div =
+                R22 * R42p / std::pow(sq(R42 * a - d) + R42 * (b * b + c * c), 1.5);
+            double gp[5];
+            gp[1] = (R42 * (b * b + c * c - 2.0 * a * d) + 2.0 * d * d) * div;
+            gp[2] = -b * (d + R42 * a) * div;
+            gp[3] = -c * (d + R42 * a) * div;
+            gp[4] = (b * b + c * c - 2.0 * a * d + (R42 + R42) * a * a) * div;
+            for (int x = 1; x <= 3; ++x)
+              gr[3 * fk + x - 1] = gp[1] * dadx[1][x] + gp[2] * dadx[2][x] +
+                                   gp[3] * dadx[3][x] + gp[4] * dadx[4][x];
+          }
+        } else
           As[i] = As[i] + R22p * d / std::sqrt(R42 * (b * b + c * c) + d * d);
       }
 
@@ -307,17 +346,20 @@ double esolan_areas(int numat, const double* xa, const double* ya, const double*
         int nyx = 0;
         ay1.assign(1, 0.0);
         ay2.assign(1, 0.0);
+        ivrx.assign(1, 0);
         for (int j = 1; j <= iv; ++j) {
           if (vertex[j].c3 == double(jk)) {
             ++nyx;
             ay1.push_back(vertex[j].t);
             ay2.push_back(vertex[j].s);
+            ivrx.push_back(j);
           }
           if (vertex[j].c4 == double(jk)) {
             ++nyx;
             ay1.push_back(vertex[j].t);
             ay2.push_back(vertex[j].s);
             std::swap(vertex[j].c3, vertex[j].c4);
+            ivrx.push_back(j);
           }
         }
         int ial = ifu;   // the other active circles (esolan.f:624-631)
@@ -355,9 +397,15 @@ double esolan_areas(int numat, const double* xa, const double* ya, const double*
               a1 = ayx1[jm];
               ayx1[jm] = ayx1[j];
               ayx1[j] = a1;
+              std::swap(ivrx[jm], ivrx[j]);
             }
           }
           ayx1[nyx + 1] = ayx1[1] + pi2;
+          ivrx.push_back(ivrx[1]);   // vrx(nyx+1, .) = vrx(1, .)
+          const double vv2 = vv1 * vv1;
+          const double xv = (d + R42 * a) * vv1;
+          const double yv = (bcd + 2.0 * R42 * ak) / daba * vv1;
+          const double zv = wv / a * vv1;
           for (int j = 1; j <= nyx; ++j) {
             if (std::fabs(ayx1[j + 1] - ayx1[j]) < 1e-8) continue;   // a 'bad' intersection
             const double prob = (ayx1[j] + ayx1[j + 1]) / 2.0;
@@ -373,6 +421,121 @@ double esolan_areas(int numat, const double* xa, const double* ya, const double*
             As[i] = As[i] + R2 * (aia * (alp - bet) +
                                   (d + R42 * a) * vv1 *
                                       (pi - 2.0 * std::atan(uv / (2.0 * ak * vv * dsbetmalp))));
+            if (gradan) {   // esolan.f:718-899
+              const double dsalp = std::sin(alp), dcalp = std::cos(alp);
+              const double dsbet = std::sin(bet), dcbet = std::cos(bet);
+              const double dcotbma = 1.0 / std::tan(5e-1 * (bet - alp));
+              const int kk = (int)vertex[ivrx[j]].c4, LL = (int)vertex[ivrx[j + 1]].c4;
+              const double P = b * dcbetpalp + c * dsbetpalp;
+              const double Q = -b * dsbetpalp + c * dcbetpalp;
+              const double s2 = dsbetmalp * dsbetmalp;
+              const double tt = yv * dcotbma - zv * P / dsbetmalp;
+              const double a1 = NB(kk, 1), b1 = NB(kk, 2), c1 = NB(kk, 3), d1 = NB(kk, 4);
+              const double a2 = NB(LL, 1), b2 = NB(LL, 2), c2 = NB(LL, 3), d2 = NB(LL, 4);
+              const double ab1 = a * b1 - b * a1, ac1 = a * c1 - c * a1;
+              const double ab2 = a * b2 - b * a2, ac2 = a * c2 - c * a2;
+              const double am1 = wv * aia * a1 * (ab1 * dsalp - ac1 * dcalp);
+              const double am2 = wv * aia * a2 * (ab2 * dsbet - ac2 * dcbet);
+              double dalp[5], dbet[5], daalp[5], dabet[5], dv[5], ddx[5], ddy[5], ddz[5],
+                  dt[5], di[5];
+              auto ang = [&](double* out, double A1, double B1, double C1, double D1, double AB,
+                             double AC, double cs_, double sn_, double am) {
+                out[1] = (B1 * AB + C1 * AC - 2.0 * d * A1 * A1 -
+                          a * (B1 * B1 + C1 * C1 - 4.0 * A1 * D1) -
+                          2.0 * d * aia * A1 * (AB * cs_ + AC * sn_) / wv +
+                          wv * aia * A1 * (B1 * cs_ + C1 * sn_)) /
+                         am;
+                out[2] = (-A1 * AB + b * A1 * A1 + b * aia * A1 * (AB * cs_ + AC * sn_) / wv -
+                          wv * aia * A1 * A1 * cs_) /
+                         am;
+                out[3] = (-A1 * AC + c * A1 * A1 + c * aia * A1 * (AB * cs_ + AC * sn_) / wv -
+                          wv * aia * A1 * A1 * sn_) /
+                         am;
+                out[4] = (-2.0 * a * A1 * A1 - 2.0 * daba * A1 * (AB * cs_ + AC * sn_) / wv) / am;
+              };
+              ang(dalp, a1, b1, c1, d1, ab1, ac1, dcalp, dsalp, am1);
+              ang(dbet, a2, b2, c2, d2, ab2, ac2, dcbet, dsbet, am2);
+              auto dang = [&](double* out, double A1, double B1, double C1, double D1, double AB,
+                              double AC, double cs_, double sn_, double am) {
+                out[1] = (-b * AB - c * AC + wv * wv * A1 + 2.0 * ak * D1 +
+                          wv * aia * ((AB - b * A1) * cs_ + (AC - c * A1) * sn_)) /
+                         am;
+                out[2] = (a * AB - ak * B1 + wv * daba * A1 * cs_) / am;
+                out[3] = (a * AC - ak * C1 + wv * daba * A1 * sn_) / am;
+                out[4] = (2.0 * ak * A1) / am;
+              };
+              dang(daalp, a1, b1, c1, d1, ab1, ac1, dcalp, dsalp, am1);
+              dang(dabet, a2, b2, c2, d2, ab2, ac2, dcbet, dsbet, am2);
+              dv[2] = R42 * b * vv1;
+              dv[3] = R42 * c * vv1;
+              dv[4] = (d - R42 * a) * vv1;
+              dv[1] = -dv[4] * R42;
+              ddx[1] = R42 * vv1 - (d + R42 * a) * dv[1] * vv2;
+              ddx[2] = -(d + R42 * a) * dv[2] * vv2;
+              ddx[3] = -(d + R42 * a) * dv[3] * vv2;
+              ddx[4] = 1.0 * vv1 - (d + R42 * a) * dv[4] * vv2;
+              const double Y = b * b + c * c - 2.0 * a * d + 2.0 * R42 * ak;
+              ddy[1] = (-2.0 * d + 4.0 * R42 * a) / daba * vv1 -
+                       Y * (aia * vv + daba * dv[1]) / ak * vv2;
+              ddy[2] = 2.0 * b / daba * vv1 - Y * aia * dv[2] / a * vv2;
+              ddy[3] = 2.0 * c / daba * vv1 - Y * aia * dv[3] / a * vv2;
+              ddy[4] = -2.0 * a / daba * vv1 - Y * aia * dv[4] / a * vv2;
+              ddz[1] = -2.0 * d / wv / a * vv1 - wv * (vv + a * dv[1]) / ak * vv2;
+              ddz[2] = b / wv / a * vv1 - wv * dv[2] / a * vv2;
+              ddz[3] = c / wv / a * vv1 - wv * dv[3] / a * vv2;
+              ddz[4] = -2.0 / wv * vv1 - wv * dv[4] / a * vv2;
+              for (int x = 1; x <= 4; ++x) {
+                const double extra =
+                    x == 2 ? dcbetpalp * 2.0 * dsbetmalp : (x == 3 ? dsbetpalp * 2.0 * dsbetmalp : 0.0);
+                dt[x] = dcotbma * ddy[x] - 5e-1 * yv * (dbet[x] - dalp[x]) / s2 -
+                        (P / dsbetmalp) * ddz[x] -
+                        5e-1 * zv *
+                            (Q * dsbetmalp * (dalp[x] + dbet[x]) -
+                             P * dcbetmalp * (dbet[x] - dalp[x]) + extra) /
+                            s2;
+                di[x] = R2 * (aia * (dalp[x] - dbet[x]) + (pi - 2.0 * std::atan(5e-1 * tt)) * ddx[x] -
+                              4.0 * xv * dt[x] / (4.0 + tt * tt));
+              }
+              double dii[5][4];
+              dii[1][1] = 2.0 * DD(jk, 2);
+              dii[1][2] = 2.0 * DD(jk, 3);
+              dii[1][3] = 2.0 * (DD(jk, 4) - R);
+              dii[2][1] = -R42 - R42;
+              dii[2][2] = 0.0;
+              dii[2][3] = 0.0;
+              dii[3][1] = 0.0;
+              dii[3][2] = dii[2][1];
+              dii[3][3] = 0.0;
+              dii[4][1] = dii[1][1] * R42;
+              dii[4][2] = dii[1][2] * R42;
+              dii[4][3] = 2.0 * (DD(jk, 4) + R) * R42;
+              for (int x = 1; x <= 3; ++x)
+                gr[3 * jk + x - 1] += di[1] * dii[1][x] + di[2] * dii[2][x] + di[3] * dii[3][x] +
+                                      di[4] * dii[4][x];
+              double dta[5], dtb[5], di1[5], di2[5];
+              for (int x = 1; x <= 4; ++x) {
+                dta[x] = 5e-1 * daalp[x] * ((yv - zv * (Q * dsbetmalp + P * dcbetmalp)) / s2);
+                dtb[x] = 5e-1 * dabet[x] * ((-yv - zv * (Q * dsbetmalp - P * dcbetmalp)) / s2);
+                di1[x] = R2 * (aia * daalp[x] - 4.0 * xv * dta[x] / (4.0 + tt * tt));
+                di2[x] = R2 * (-aia * dabet[x] - 4.0 * xv * dtb[x] / (4.0 + tt * tt));
+              }
+              auto rows = [&](int m) {
+                dii[1][1] = 2.0 * DD(m, 2);
+                dii[1][2] = 2.0 * DD(m, 3);
+                dii[1][3] = 2.0 * (DD(m, 4) - R);
+                dii[4][1] = dii[1][1] * R42;
+                dii[4][2] = dii[1][2] * R42;
+                dii[4][3] = 2.0 * (DD(m, 4) + R) * R42;
+              };
+              rows(kk);
+              for (int x = 1; x <= 3; ++x)
+                gr[3 * kk + x - 1] += di1[1] * dii[1][x] + di1[2] * dii[2][x] +
+                                      di1[3] * dii[3][x] + di1[4] * dii[4][x];
+              rows(LL);
+              for (int x = 1; x <= 3; ++x)
+                gr[3 * LL + x - 1] += di2[1] * dii[1][x] + di2[2] * dii[2][x] +
+                                      di2[3] * dii[3][x] + di2[4] * dii[4][x];
+            }
           }
         } else {   // the circle is a line (esolan.f:904-994)
           const double ang = std::atan2(b, c);
@@ -431,6 +594,29 @@ double esolan_areas(int numat, const double* xa, const double* ya, const double*
         }
       }
     } while (false);
+    if (assemble) {   // label 11 (esolan.f:998-1030): grad(i, i) and the frame turned back
+      for (int j = 1; j <= ine_g; ++j) al[ifu_g + j] = neib[j];
+      al[0] = ifu_g + ine_g;
+      for (int x = 0; x < 3; ++x) {
+        double ss = 0.0;
+        for (int j2 = 1; j2 <= al[0]; ++j2) ss = ss + gr[3 * al[j2] + x];
+        gr[3 * i + x] = -ss;
+      }
+      if (jjj != 0) {
+        const double sfsg = sf * sg, sfcg = sf * cg, cfsg = cf * sg, cfcg = cf * cg;
+        auto turn = [&](int j) {
+          const double xx = gr[3 * j], yy = gr[3 * j + 1], zz = gr[3 * j + 2];
+          gr[3 * j] = xx * cg - yy * sfsg + zz * cfsg;
+          gr[3 * j + 1] = yy * cf + zz * sf;
+          gr[3 * j + 2] = -xx * sg - yy * sfcg + zz * cfcg;
+        };
+        turn(i);
+        for (int j2 = 1; j2 <= al[0]; ++j2) turn(al[j2]);
+      }
+    }
+    if (gradan)   // esolan.f:1034-1042, in atom order i
+      for (int j = 1; j <= numat; ++j)
+        for (int x = 0; x < 3; ++x) gradan[3 * j + x] = gradan[3 * j + x] + sigma[i] * gr[3 * j + x];
     sss = sss + As[i] * sigma[i];   // label 1
   }
   if (As_out)
@@ -445,7 +631,7 @@ double Smmp::esolan(int nmol) {
   else
     numat = iatrs2[irsml2[nmol]] - iatrs1[irsml1[nmol]] + 1;
   return esolan_areas(numat, &xat_[2], &yat_[2], &zat_[2], rvdw.data(), sigma.data(),
-                      [this] { return grnd(); }, nullptr);
+                      [this] { return grnd(); }, nullptr, nullptr);
 }
 
 }  // namespace oracle

@@ -155,17 +155,128 @@ double Smmp::opeshe(int nml) {
   return eysm;
 }
 
-// gradient.f:12-70 for the vacuum model (itysol = 0); the reference stops
-// for itysol > 0, and opesol (itysol < 0) is not restated.
+// opesol.f:12-240: the analytic solvation energy (esolan) and its
+// derivatives with respect to the variables, by the same recursion over the
+// moving sets as opeshe with the atomic forces -gradan; a variable whose axis
+// is the molecule's reference axis (ixrfpt(2)) takes the forces of its
+// primary atom's interaction partners with the opposite sign.
+void Smmp::opesol(int nml, std::vector<double>& gdeysl) {
+  const int ntlvr = nvrml[nml];
+  if (ntlvr == 0) return;
+  const int ix2 = ixrfpt[2][nml];
+  const int ifivr = ivrml1[nml], ilavr = ifivr + ntlvr - 1;
+  gdeysl.assign(ilavr + 1, 0.0);
+  std::vector<double> xfvr(ilavr + 1, 0.0), yfvr(ilavr + 1, 0.0), zfvr(ilavr + 1, 0.0),
+      xfrvr(ilavr + 1, 0.0), yfrvr(ilavr + 1, 0.0), zfrvr(ilavr + 1, 0.0);
+  // esolan(nml): energy and gradan
+  int numat = iatrs2[irsml2[nml]] - iatrs1[irsml1[nml]] + 1;
+  std::vector<double> gradan(3 * (numat + 1));
+  eysl = esolan_areas(numat, &xat_[2], &yat_[2], &zat_[2], rvdw.data(), sigma.data(),
+                      [this] { return grnd(); }, nullptr, gradan.data());
+  const int ifiat = iatrs1[irsml1[nml]], ilaat = iatrs2[irsml2[nml]];
+  std::vector<double> xfat(ilaat + 1), yfat(ilaat + 1), zfat(ilaat + 1), xfrat(ilaat + 1),
+      yfrat(ilaat + 1), zfrat(ilaat + 1);
+  for (int i = ifiat; i <= ilaat; ++i) {   // f = -sigma dA/dr, g = f x r
+    const double dx = -gradan[3 * i], dy = -gradan[3 * i + 1], dz = -gradan[3 * i + 2];
+    xfat[i] = dx;
+    yfat[i] = dy;
+    zfat[i] = dz;
+    const double xi = xat(i), yi = yat(i), zi = zat(i);
+    xfrat[i] = dy * zi - dz * yi;
+    yfrat[i] = dz * xi - dx * zi;
+    zfrat[i] = dx * yi - dy * xi;
+  }
+  int i1s = imsml1[nml] + nmsml[nml], i1a = iadml1[nml] + nadml[nml];
+  for (int io = ilavr; io >= ifivr; --io) {
+    bool lnb = false;
+    const int iv = iorvr[io], it = ityvr[iv], ia = iatvr[iv], ib = iowat[ia];
+    const double xb = xat(ib), yb = yat(ib), zb = zat(ib);
+    double ex = 0, ey = 0, ez = 0;
+    if (it == 3) {
+      ex = xtoat[ib];
+      ey = ytoat[ib];
+      ez = ztoat[ib];
+      if (ib == ix2) lnb = true;
+    } else if (it == 2) {
+      ex = xbaat[ia];
+      ey = ybaat[ia];
+      ez = zbaat[ia];
+      if (ib == ix2) lnb = true;
+    } else if (it == 1) {
+      ex = xtoat[ia];
+      ey = ytoat[ia];
+      ez = ztoat[ia];
+      if (ia == ix2) lnb = true;
+    }
+    double xfiv = 0, yfiv = 0, zfiv = 0, xfriv = 0, yfriv = 0, zfriv = 0;
+    if (!lnb) {
+      const int i2s = i1s - 1;
+      i1s = imsvr1[iv];
+      for (int ims = i1s; ims <= i2s; ++ims)
+        for (int i = latms1[ims]; i <= latms2[ims]; ++i) {
+          xfiv = xfiv + xfat[i];
+          yfiv = yfiv + yfat[i];
+          zfiv = zfiv + zfat[i];
+          xfriv = xfriv + xfrat[i];
+          yfriv = yfriv + yfrat[i];
+          zfriv = zfriv + zfrat[i];
+        }
+      const int i2a = i1a - 1;
+      i1a = iadvr1[iv];
+      for (int iad = i1a; iad <= i2a; ++iad) {
+        const int lad = ladvr[iad];
+        xfiv = xfiv + xfvr[lad];
+        yfiv = yfiv + yfvr[lad];
+        zfiv = zfiv + zfvr[lad];
+        xfriv = xfriv + xfrvr[lad];
+        yfriv = yfriv + yfrvr[lad];
+        zfriv = zfriv + zfrvr[lad];
+      }
+    } else {
+      auto sub = [&](int j) {
+        xfiv = xfiv - xfat[j];
+        yfiv = yfiv - yfat[j];
+        zfiv = zfiv - zfat[j];
+        xfriv = xfriv - xfrat[j];
+        yfriv = yfriv - yfrat[j];
+        zfriv = zfriv - zfrat[j];
+      };
+      for (int ivw = ivwat1[ia]; ivw <= ivwat2[ia]; ++ivw)
+        for (int j = lvwat1[ivw]; j <= lvwat2[ivw]; ++j) sub(j);
+      for (int i14 = i14at1[ia]; i14 <= i14at2[ia]; ++i14) sub(l14at[i14]);
+    }
+    xfvr[iv] = xfiv;
+    yfvr[iv] = yfiv;
+    zfvr[iv] = zfiv;
+    xfrvr[iv] = xfriv;
+    yfrvr[iv] = yfriv;
+    zfrvr[iv] = zfriv;
+    if (it == 3 || it == 2)
+      gdeysl[iv] = (ey * zb - ez * yb) * xfiv + (ez * xb - ex * zb) * yfiv +
+                   (ex * yb - ey * xb) * zfiv + ex * xfriv + ey * yfriv + ez * zfriv;
+    else if (it == 1)
+      gdeysl[iv] = -(ex * xfiv + ey * yfiv + ez * zfiv);
+  }
+}
+
+// gradient.f:12-70: vacuum (itysol = 0) or analytic solvation (itysol < 0,
+// opesol); the reference stops for the numerical model (itysol > 0).
 double Smmp::gradient() {
-  if (itysol != 0)
-    throw std::runtime_error("gradient: only the vacuum model (itysol = 0) is restated");
+  if (itysol > 0) throw std::runtime_error("gradient> Set itysol < 0");
   double esm = 0.0;
   for (int i = 1; i <= ntlml; ++i) {
     setvar(i, vlvr.data());
     opeshe(i);
     esm = esm + eysm;
-    eysl = 0.0;
+    if (itysol < 0) {
+      std::vector<double> gs;
+      opesol(i, gs);
+      esm = esm + eysl;
+      const int ivr1 = ivrml1[i], ivr2 = ivr1 + nvrml[i] - 1;
+      for (int j = ivr1; j <= ivr2; ++j) gdeyvr[j] = gdeyvr[j] + gs[j];
+    } else {
+      eysl = 0.0;
+    }
   }
   eysm = esm;
   return esm;

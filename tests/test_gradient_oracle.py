@@ -1,7 +1,9 @@
 """The oracle's restatement of gradient.f / opeshe.f (energy derivatives with
-respect to the dihedrals, the recursive force and torque sums): its energy is
-the oracle's energy() and its derivatives equal central finite differences of
-that energy, for ECEPP/3, ECEPP/2 and the sigmoidal dielectric."""
+respect to the dihedrals, the recursive force and torque sums) and of
+opesol.f with esolan.f's area derivatives (the analytic solvation term): the
+energy is the oracle's energy() and the derivatives equal central finite
+differences of that energy, for ECEPP/3, ECEPP/2, the sigmoidal dielectric
+and the analytic SASA model."""
 import numpy as np
 import pytest
 
@@ -64,6 +66,42 @@ def test_order_free_sums_equal_the_recursion(ff, epsd):
         g2 = np.zeros(o.ntlvr)
         assert lib.orc_gradient_by_sums(o.h, g2.ctypes.data_as(ctypes.c_void_p)) == 0
         assert np.abs(g - g2).max() <= 1e-12 * np.abs(g).max()
+
+
+def test_solvation_gradient_equals_finite_differences():
+    """itysol = -1: the gradient minus the vacuum gradient is the derivative
+    of eysl alone (opesol.f, esolan.f:547-569, 718-899, 998-1042)."""
+    an = Oracle(DATA + "enkefa.seq", DATA + "enkefa.var", itysol=-1)
+    va = Oracle(DATA + "enkefa.seq", DATA + "enkefa.var")
+    v0 = an.vlvr().copy()
+    rng = np.random.default_rng(5)
+    idvr = an.idvr() - 1
+    for k in range(3):
+        v = v0.copy()
+        if k:
+            v[idvr] = v[idvr] + rng.normal(0.0, 0.05, len(idvr))
+        an.set_vlvr(v)
+        va.set_vlvr(v)
+        ea, ga = an.gradient()
+        e0, t = an.energy()
+        assert ea == pytest.approx(e0, rel=1e-13, abs=1e-10)
+        _, gv = va.gradient()
+        gs = ga - gv
+        h = 1e-5
+        num = np.zeros(len(v))
+        for j in range(len(v)):
+            vp = v.copy()
+            vp[j] += h
+            an.set_vlvr(vp)
+            _, tp = an.energy()
+            vm = v.copy()
+            vm[j] -= h
+            an.set_vlvr(vm)
+            _, tm = an.energy()
+            num[j] = (tp[4] - tm[4]) / (2 * h)
+        an.set_vlvr(v)
+        assert np.abs(num).max() > 1.0   # the solvation term does depend on the dihedrals
+        assert np.all(np.abs(gs - num) <= 1e-6 * np.maximum(1.0, np.abs(num))), np.c_[gs, num]
 
 
 def test_gradient_refuses_numerical_solvation():
