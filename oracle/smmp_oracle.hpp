@@ -171,6 +171,8 @@ struct Smmp {
   int minqsn(int n, double* x, double& f, double* g, const double* scal, double acur,
              int maxfun, std::vector<double>* log);
   void minim_move(int n, double& f, const double* x, double* g, std::vector<double>* log);
+  int mincjg(int n, double* x, double& f, double* g, double acur, int maxfun,
+             std::vector<double>* log);
 
   // random numbers
   void sgrnd(int32_t seed);

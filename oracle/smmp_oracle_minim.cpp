@@ -1,8 +1,9 @@
 // CPU oracle -- TEST INFRASTRUCTURE ONLY (see smmp_oracle.hpp).
 //
-// minim.f:12-258 (imin = 1, no regularisation) with move (minim.f:262-360),
-// and minqsn.f: the quasi-Newton minimiser (BFGS updates of a Cholesky-
-// factored Hessian, mc11a/mc11e; cubic line searches).  Arrays are 1-based;
+// minim.f:12-258 (no regularisation) with move (minim.f:262-360), minqsn.f
+// (imin = 1: quasi-Newton, BFGS updates of a Cholesky-factored Hessian,
+// mc11a/mc11e, cubic line searches) and mincjg.f (imin = 2: conjugate
+// gradients with restarts).  Arrays are 1-based;
 // the reference's single-precision literals (.01, .1) are kept as floats
 // promoted to double, as the Fortran evaluates them.
 #include <algorithm>
@@ -357,10 +358,204 @@ int Smmp::minqsn(int n, double* x, double& f, double* g, const double* scal, dou
   }
 }
 
-// minim.f:12-258 for imin = 1 (quasi-Newton) without regularisation: returns
-// the number of function calls; log receives (energy, |gradient|^2) of each.
+// mincjg.f: conjugate gradients with restarts (no scaling).  Returns nfun.
+int Smmp::mincjg(int n, double* x, double& f, double* g, double acur, int maxfun,
+                 std::vector<double>* log) {
+  const double AMF = 10.0, TOL = 1.e-7, EPS = .7;
+  const int MXFCON = 2, MAXLIN = 5;
+  std::vector<double> D(n + 1), XA(n + 1), GA(n + 1), DT(n + 1), YT(n + 1), GT(n + 1);
+  double *d = D.data(), *xa = XA.data(), *ga = GA.data(), *dt = DT.data(), *yt = YT.data(),
+         *gt = GT.data();
+  int ier = 0, iter = 0, iterfm = 0, iterrs = 0, nfun = 0, nfopt = nfun, nfbeg = 0, iretry = 0;
+  double gsqrd = 0.0, fmin = f, gsq2, gnew, dfpr, stmin, fuit = 0.0, gdit = 0.0, gdmi = 0.0,
+         sbound = 0.0, stepch = 0.0, step = 0.0, wo = 0.0, sum = 0.0, fch = 0.0, ddspln = 0.0,
+         gspln = 0.0, beta = 0.0, gama = 0.0, gamden = 0.0;
+  for (int i = 1; i <= n; ++i) {
+    const double t = g[i];
+    ga[i] = t;
+    d[i] = -t;
+    gsqrd = gsqrd + t * t;
+    xa[i] = x[i];
+  }
+  gsq2 = .2 * gsqrd;
+  gnew = -gsqrd;
+  dfpr = AMF;
+  stmin = AMF / gsqrd;
+  (void)gnew;
+  enum { L1, L2, L3, L4, L5, L6 } at = L1;
+  for (;;) {
+    switch (at) {
+      case L1:
+        iter = iter + 1;
+        fuit = f;
+        gdit = 0.0;
+        for (int i = 1; i <= n; ++i) {
+          gt[i] = g[i];
+          gdit = gdit + d[i] * g[i];
+        }
+        if (gdit >= 0.0) {   // uphill
+          ier = 3;
+          at = L6;
+          break;
+        }
+        gdmi = gdit;
+        sbound = -1.0;
+        nfbeg = nfun;
+        iretry = -1;
+        stepch = std::min(stmin, std::fabs(dfpr / gdit));
+        stmin = 0.0;
+        at = L2;
+        break;
+      case L2: {
+        step = stmin + stepch;
+        wo = 0.0;
+        for (int i = 1; i <= n; ++i) {
+          const double t = stepch * d[i];
+          wo = std::max(wo, std::fabs(t));
+          x[i] = xa[i] + t;
+        }
+        if (wo > TOL) {
+          nfun = nfun + 1;
+          minim_move(n, f, x, g, log);
+          gnew = 0.0;
+          sum = 0.0;
+          for (int i = 1; i <= n; ++i) {
+            const double t = g[i];
+            gnew = gnew + d[i] * t;
+            sum = sum + t * t;
+          }
+          fch = f - fmin;
+          if (fch <= 0.0) {
+            if (fch < 0.0 || (gnew / gdmi) >= -1.0) {
+              fmin = f;
+              gsqrd = sum;
+              gsq2 = .2 * gsqrd;
+              nfopt = nfun;
+              for (int i = 1; i <= n; ++i) {
+                xa[i] = x[i];
+                ga[i] = g[i];
+              }
+            }
+            if (sum <= acur) return nfun;   // normal end
+          }
+          if (nfun == maxfun) return nfun;   // ier = 1
+        } else {   // stepch is effectively zero
+          if (nfun > nfbeg + 1 || std::fabs(gdmi / gdit) > EPS) ier = 2;
+          at = L6;
+          break;
+        }
+        wo = (fch + fch) / stepch - gnew - gdmi;
+        ddspln = (gnew - gdmi) / stepch;
+        if (nfun <= nfopt) {
+          if (gdmi * gnew <= 0.0) sbound = stmin;
+          stmin = step;
+          gdmi = gnew;
+          stepch = -stepch;
+        } else {
+          sbound = step;
+        }
+        if (fch != 0.0) ddspln = ddspln + (wo + wo) / stepch;
+        if (gdmi == 0.0) {
+          at = L6;
+          break;
+        }
+        if (nfun <= nfbeg + 1) {
+          at = L4;
+          break;
+        }
+        if (std::fabs(gdmi / gdit) <= EPS) {
+          at = L6;
+          break;
+        }
+        at = L3;
+        break;
+      }
+      case L3:
+        if (nfun >= nfopt + MAXLIN) {
+          ier = 2;
+          at = L6;
+          break;
+        }
+        at = L4;
+        break;
+      case L4:
+        if (sbound < -.5)
+          stepch = 9.0 * stmin;
+        else
+          stepch = .5 * (sbound - stmin);
+        gspln = gdmi + stepch * ddspln;
+        if ((gdmi * gspln) < 0.0) stepch = stepch * gdmi / (gdmi - gspln);
+        at = L2;
+        break;
+      case L5: {
+        sum = 0.0;
+        for (int i = 1; i <= n; ++i) sum = sum + g[i] * gt[i];
+        beta = (gsqrd - sum) / (gdmi - gdit);
+        if (std::fabs(beta * gdmi) > gsq2) {
+          iretry = iretry + 1;
+          if (iretry <= 0) {
+            at = L3;
+            break;
+          }
+        }
+        if (f < fuit) iterfm = iter;
+        if (iter >= iterfm + MXFCON) return nfun;   // ier = 4
+        dfpr = stmin * gdit;
+        if (iretry > 0) {
+          for (int i = 1; i <= n; ++i) d[i] = -g[i];
+          iterrs = 0;
+        } else {
+          if (iterrs != 0 && (iter - iterrs) < (n - 1) && std::fabs(sum) < gsq2) {
+            gama = 0.0;
+            sum = 0.0;
+            for (int i = 1; i <= n; ++i) {
+              const double t = g[i];
+              gama = gama + t * yt[i];
+              sum = sum + t * dt[i];
+            }
+            gama = gama / gamden;
+            if (std::fabs(beta * gdmi + gama * sum) < gsq2) {
+              for (int i = 1; i <= n; ++i) d[i] = -g[i] + beta * d[i] + gama * dt[i];
+              at = L1;
+              break;
+            }
+          }
+          gamden = gdmi - gdit;
+          for (int i = 1; i <= n; ++i) {
+            const double t = g[i], di = d[i];
+            dt[i] = di;
+            yt[i] = t - gt[i];
+            d[i] = -t + beta * di;
+          }
+          iterrs = iter;
+        }
+        at = L1;
+        break;
+      }
+      case L6:
+        if (nfun != nfopt) {   // back to the best point
+          f = fmin;
+          for (int i = 1; i <= n; ++i) {
+            x[i] = xa[i];
+            g[i] = ga[i];
+          }
+        }
+        if (ier == 0) {
+          at = L5;
+          break;
+        }
+        nfun = nfun + 1;
+        minim_move(n, f, x, g, log);
+        return nfun;
+    }
+  }
+}
+
+// minim.f:12-258 without regularisation, imin = 1 (quasi-Newton) or 2
+// (conjugate gradients): returns the number of function calls; log receives
+// (energy, |gradient|^2) of each.
 int Smmp::minim(int imin, int maxit, double eps, std::vector<double>* log) {
-  if (imin != 1) throw std::runtime_error("minim: only the quasi-Newton minimiser is restated");
+  if (imin != 1 && imin != 2) throw std::runtime_error("minim: imin must be 1 or 2");
   gradient();
   const int ntlvr = ivrml1[ntlml] + nvrml[ntlml] - 1;
   std::vector<double> vlvrn(ntlvr + 1), gdvr(ntlvr + 1), scl(ntlvr + 1);
@@ -373,7 +568,9 @@ int Smmp::minim(int imin, int maxit, double eps, std::vector<double>* log) {
       gdvr[nv] = gdeyvr[i];
     }
   double esm = eysm;
-  const int nop = minqsn(nv, vlvrn.data(), esm, gdvr.data(), scl.data(), eps, maxit, log);
+  const int nop = imin == 1
+                      ? minqsn(nv, vlvrn.data(), esm, gdvr.data(), scl.data(), eps, maxit, log)
+                      : mincjg(nv, vlvrn.data(), esm, gdvr.data(), eps, maxit, log);
   energy();
   nv = 0;
   for (int i = 1; i <= ntlvr; ++i)   // minim.f:213-225

@@ -49,3 +49,19 @@ def test_minimisation_reproduces_the_published_run():
     want = np.array([w[2] for w in g["variables"]])
     d = (v - want + 180.0) % 360.0 - 180.0
     assert np.all(np.abs(d) <= 0.051), np.c_[v, want]
+
+
+def test_conjugate_gradients_reach_the_same_minimum():
+    """imin = 2 (mincjg.f) from the same start ends in the minimum the
+    published quasi-Newton run found."""
+    with open(os.path.join(ROOT, "tests", "golden", "golden.json")) as f:
+        g = json.load(f)["minim_enkefa"]
+    o = Oracle(DATA + "enkefa.seq", DATA + "enkefa.var")
+    nop, log = o.minim(2, 10000, 1e-9)
+    assert nop < 10000 and log[-1][1] < 1e-6
+    e, _ = o.energy()
+    assert abs(e - g["total"]) <= 5e-3
+    v = o.vlvr()[o.idvr() - 1] * CRD
+    want = np.array([w[2] for w in g["variables"]])
+    d = (v - want + 180.0) % 360.0 - 180.0
+    assert np.all(np.abs(d) <= 0.051)
