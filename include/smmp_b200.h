@@ -110,6 +110,16 @@ int smmp_setvar(int nml, const double* vlvrx);
  * eol and acz are updated in place as the f2py intent(in,out) arguments. */
 int smmp_metropolis(double* eol, double* acz, const smmp_weight_t* w);
 
+/* Multicanonical weight recursion of mulcan_par (mulcan_par_mod.f90:93-145),
+ * host only: the histogram ihist of the last sweeps (zeroed on return)
+ * updates xhist, g1, b, alpha, ent for bins kmin..kmax (arrays of
+ * kmax-kmin+1, index k-kmin); beta = 1/(k_B T).  smmp_muca_finish folds beta
+ * into b and recomputes alpha (mulcan_par_mod.f90:163-168), the weights of
+ * muca_weight2 (smmp_weight_t kind 2). */
+int smmp_muca_update(int kmin, int kmax, double ebin, double beta, int* ihist, double* xhist,
+                     double* g1, double* b, double* alpha, double* ent);
+int smmp_muca_finish(int kmin, int kmax, double ebin, double beta, double* b, double* alpha);
+
 /* outvar(nml, fileName): outvar.f:12.  The current variables in the .var
  * command language; fileName "" (or blanks): standard output.  nml 0 or 1. */
 int smmp_outvar(int nml, const char* fileName);

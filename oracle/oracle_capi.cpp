@@ -419,6 +419,15 @@ int orc_gradient_by_sums(void* h, double* grad) {
   });
 }
 
+// mulcan_par_mod.f90 weight recursion (see muca_update / muca_finish).
+int orc_muca_update(int kmin, int kmax, double ebin, double beta, int* ihist, double* xhist,
+                    double* g1, double* b, double* alpha, double* ent) {
+  return guard([&] { oracle::muca_update(kmin, kmax, ebin, beta, ihist, xhist, g1, b, alpha, ent); });
+}
+int orc_muca_finish(int kmin, int kmax, double ebin, double beta, double* b, double* alpha) {
+  return guard([&] { oracle::muca_finish(kmin, kmax, ebin, beta, b, alpha); });
+}
+
 // minim.f (quasi-Newton, no regularisation): *nop function calls; log
 // receives up to logcap (energy, |grad|^2) pairs, *nlog the number of pairs.
 int orc_minim(void* h, int imin, int maxit, double eps, int* nop, double* log, int logcap,

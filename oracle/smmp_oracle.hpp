@@ -200,6 +200,12 @@ double esolan_areas(int numat, const double* x, const double* y, const double* z
                     const double* rvdw, const double* sigma, const std::function<double()>& grnd,
                     double* As_out, double* gradan = nullptr);
 
+// mulcan_par_mod.f90:93-145 and :163-168: the multicanonical weight
+// recursion (arrays indexed k - kmin; ihist zeroed by the update).
+void muca_update(int kmin, int kmax, double ebin, double beta, int* ihist, double* xhist,
+                 double* g1, double* b, double* alpha, double* ent);
+void muca_finish(int kmin, int kmax, double ebin, double beta, double* b, double* alpha);
+
 // Angle helpers (difang.f:12-60): results wrapped into (-pi, pi].
 double difang(double a1, double a2);
 double addang(double a1, double a2);

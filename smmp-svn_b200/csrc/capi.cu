@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "../../include/smmp_b200.h"
+#include "muca.hpp"
 #include "runtime.hpp"
 #include "surrogate.hpp"
 
@@ -410,6 +411,23 @@ void write_text(const std::string& s, const char* fileName, const char* who) {
     std::fputs(s.c_str(), stdout);
     std::fflush(stdout);
   }
+}
+
+int smmp_muca_update(int kmin, int kmax, double ebin, double beta, int* ihist, double* xhist,
+                     double* g1, double* b, double* alpha, double* ent) {
+  return guard([&] {
+    need(kmax - kmin >= 2 && ebin > 0.0, "muca: need at least three bins and ebin > 0");
+    need(ihist && xhist && g1 && b && alpha && ent, "NULL argument");
+    muca_update(MucaBins{kmin, kmax, ebin, beta}, ihist, xhist, g1, b, alpha, ent);
+  });
+}
+
+int smmp_muca_finish(int kmin, int kmax, double ebin, double beta, double* b, double* alpha) {
+  return guard([&] {
+    need(kmax - kmin >= 2 && ebin > 0.0, "muca: need at least three bins and ebin > 0");
+    need(b && alpha, "NULL argument");
+    muca_finish(MucaBins{kmin, kmax, ebin, beta}, b, alpha);
+  });
 }
 
 int smmp_outvar(int nml, const char* fileName) {

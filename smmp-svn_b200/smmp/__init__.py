@@ -27,7 +27,8 @@ __all__ = ["init_energy", "init_molecule", "energy", "setvar", "metropolis", "ou
            "sgrnd",
            "grnd", "canon", "anneal", "can_weight", "MucaWeight", "SmmpError",
            "epar_l", "isolty", "updchois", "bet", "mol_par", "var_r", "var_i", "eny_r",
-           "updstats", "gpu_available", "reset", "coordinates"]
+           "updstats", "gpu_available", "reset", "coordinates", "MucaState",
+           "mulcan_par"]
 
 
 def gpu_available():
@@ -318,6 +319,95 @@ def anneal(nequi, nswp, nmes, tmax, tmin, lrand=1):
     check(lib.smmp_anneal(int(nequi), int(nswp), int(nmes), float(tmax), float(tmin),
                           int(lrand), out))
     return tuple(out[:5]) + (int(out[5]),)
+
+
+class MucaState:
+    """Weight parameters of the multicanonical recursion over the energy bins
+    kmin..kmax of width ebin (arrays indexed k - kmin), as mulcan_par keeps
+    them: accumulated histogram xhist, recursion weights g1, b, alpha and the
+    entropy estimate ent."""
+
+    def __init__(self, kmin, kmax, ebin):
+        if kmax - kmin < 2 or ebin <= 0:
+            raise ValueError("need at least three bins and ebin > 0")
+        self.kmin, self.kmax, self.ebin = int(kmin), int(kmax), float(ebin)
+        n = self.kmax - self.kmin + 1
+        self.xhist, self.g1, self.b, self.alpha, self.ent = (np.zeros(n) for _ in range(5))
+
+    def update(self, ihist, beta):
+        """mulcan_par_mod.f90:93-145: the histogram of the last sweeps
+        (int array, zeroed on return) updates the weights."""
+        h = np.ascontiguousarray(ihist, dtype=np.int32)
+        D = ctypes.POINTER(ctypes.c_double)
+        check(lib.smmp_muca_update(self.kmin, self.kmax, self.ebin, float(beta),
+                                   h.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                   *(a.ctypes.data_as(D) for a in
+                                     (self.xhist, self.g1, self.b, self.alpha, self.ent))))
+        ihist[:] = h
+
+    def finish(self, beta):
+        """mulcan_par_mod.f90:163-168: beta folded into b (weights of kind 2)."""
+        D = ctypes.POINTER(ctypes.c_double)
+        check(lib.smmp_muca_finish(self.kmin, self.kmax, self.ebin, float(beta),
+                                   self.b.ctypes.data_as(D), self.alpha.ctypes.data_as(D)))
+
+    def weight(self, kind=1):
+        return MucaWeight(self.b, self.alpha, self.kmin, self.kmax, self.ebin, kind=kind)
+
+
+def _addang(a1, a2):
+    """addang (difang.f:38-60): a1 + a2 wrapped into (-pi, pi]."""
+    pi2 = 2.0 * np.pi
+    d = float(np.fmod(a1 + a2, pi2))
+    return d if abs(d) <= np.pi else d - float(np.copysign(pi2, d))
+
+
+def mulcan_par(nsweep, nup, temp, kmin, kmax, binWidth, l_iter=False):
+    """mulcan_par(nsweep, nup, temp, kmin, kmax, binWidth, l_iter) --
+    mulcan_par_mod.f90:23: multicanonical weight iteration.  A random start,
+    then nsweep sweeps with muca_weight, the weights updated from the
+    histogram every nup sweeps (mpar_full.d written at each update, read
+    first when l_iter); the final weights (beta folded in) go to muca.d and
+    are returned as a MucaState."""
+    beta = 1.0 / (temp * 1.98773e-3)
+    bet.beta = beta
+    st = MucaState(kmin, kmax, binWidth)
+    if l_iter:
+        rows = np.loadtxt("mpar_full.d", ndmin=2)
+        for r in rows:
+            k = int(r[0]) - st.kmin
+            st.xhist[k], st.g1[k], st.b[k], st.alpha[k], st.ent[k] = r[1:6]
+    ihist = np.zeros(st.kmax - st.kmin + 1, dtype=np.int32)
+    v = var_r.vlvr
+    ax = var_r.axvr
+    for iv in np.asarray(var_i.idvr) - 1:   # random start (mulcan_par_mod.f90:79-84)
+        dv = ax[iv] * (grnd() - 0.5)
+        v[iv] = _addang(np.pi, dv)
+    var_r.vlvr = v
+    eol = energy()
+    outpdb(1, "start.pdb")
+    acz = 0.0
+    w = st.weight(1)
+    for nsw in range(1, nsweep + 1):
+        eol, acz = metropolis(eol, acz, w)
+        x = eol / st.ebin + np.copysign(0.5, eol)
+        muold = int(min(float(st.kmax), max(float(st.kmin), x)))
+        ihist[muold - st.kmin] += 1
+        if nsw % nup == 0:
+            st.update(ihist, beta)
+            with open("mpar_full.d", "w") as f:
+                for k in range(st.kmax, st.kmin - 1, -1):
+                    i = k - st.kmin
+                    f.write("%5d%15.4f%15.4f%15.4f%15.4f%15.4f\n" % (
+                        k, st.xhist[i], st.g1[i], st.b[i], st.alpha[i], st.ent[i]))
+            w = st.weight(1)
+    st.acceptance = acz / float((nsweep + 1) * mol_par.nvr)   # nsw = nsweep+1 after the DO loop
+    st.last_energy = eol
+    st.finish(beta)
+    with open("muca.d", "w") as f:
+        for k in range(st.kmin, st.kmax + 1):
+            f.write("%12d %24.16E %24.16E\n" % (k, st.b[k - st.kmin], st.alpha[k - st.kmin]))
+    return st
 
 
 def coordinates():

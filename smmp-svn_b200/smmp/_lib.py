@@ -63,6 +63,9 @@ _SIGS = {
     "smmp_mol_vlvr0": (c_int, [c_void_p, P(c_double)]),
     "smmp_mol_outvar": (c_int, [c_void_p, P(c_double), c_int, c_void_p, P(ctypes.c_uint64)]),
     "smmp_outvar": (c_int, [c_int, c_char_p]),
+    "smmp_muca_update": (c_int, [c_int, c_int, c_double, c_double, P(c_int), P(c_double),
+                                 P(c_double), P(c_double), P(c_double), P(c_double)]),
+    "smmp_muca_finish": (c_int, [c_int, c_int, c_double, c_double, P(c_double), P(c_double)]),
     "smmp_outpdb": (c_int, [c_int, c_char_p]),
     "smmp_mol_outpdb": (c_int, [c_void_p, P(c_double), c_void_p, P(ctypes.c_uint64)]),
     "smmp_ens_create": (c_void_p, [P(c_void_p), c_int, P(c_int), c_int, P(c_int), P(c_double),
