@@ -56,3 +56,53 @@ def test_addang_wraps_like_the_reference():
         d = np.fmod(a + b, 2 * pi)
         want = d if abs(d) <= pi else d - np.copysign(2 * pi, d)
         assert smmp._addang(a, b) == want
+
+
+def test_mulcan_par_driver_logic(tmp_path, monkeypatch):
+    """The driver's host logic with the GPU calls replaced by a seeded fake
+    walk: energies binned as mulcan_par_mod.f90:118 bins them, the weights
+    updated every nup sweeps from exactly those histograms (checked by
+    replaying the recursion), mpar_full.d and muca.d written, and the
+    acceptance normalised by (nsweep+1)*nvr as the Fortran loop leaves it."""
+    import smmp
+    rng = np.random.default_rng(2)
+    energies = list(rng.normal(5.0, 6.0, 64))
+    calls = {"metropolis": 0}
+
+    class FakeVar:
+        vlvr = np.zeros(10)
+        axvr = np.full(10, 2 * np.pi)
+
+    def fake_metropolis(eol, acz, w):
+        calls["metropolis"] += 1
+        assert isinstance(w, smmp.MucaWeight) and w.kind == 1
+        return energies[calls["metropolis"] - 1], acz + 3.0
+
+    monkeypatch.chdir(tmp_path)
+    monkeypatch.setattr(smmp, "metropolis", fake_metropolis)
+    monkeypatch.setattr(smmp, "energy", lambda: 0.0)
+    monkeypatch.setattr(smmp, "outpdb", lambda nml, f: None)
+    monkeypatch.setattr(smmp, "grnd", lambda: 0.25)
+    monkeypatch.setattr(smmp, "var_r", FakeVar())
+    monkeypatch.setattr(smmp, "var_i", type("I", (), {"idvr": np.array([1, 2, 3])})())
+    monkeypatch.setattr(smmp, "mol_par", type("M", (), {"nvr": 3})())
+    monkeypatch.setattr(smmp, "bet", type("B", (), {"beta": 0.0})())
+    kmin, kmax, ebin, nup, nsweep = -8, 16, 1.0, 16, 64
+    st = smmp.mulcan_par(nsweep, nup, 300.0, kmin, kmax, ebin)
+    assert calls["metropolis"] == nsweep
+    beta = 1.0 / (300.0 * 1.98773e-3)
+    ref = smmp.MucaState(kmin, kmax, ebin)
+    h = np.zeros(kmax - kmin + 1, dtype=np.int32)
+    for n, e in enumerate(energies, start=1):
+        k = int(min(float(kmax), max(float(kmin), e / ebin + np.copysign(0.5, e))))
+        h[k - kmin] += 1
+        if n % nup == 0:
+            ref.update(h, beta)
+    ref.finish(beta)
+    assert np.array_equal(st.b, ref.b) and np.array_equal(st.alpha, ref.alpha)
+    assert np.array_equal(st.xhist, ref.xhist)
+    assert st.acceptance == 3.0 * nsweep / ((nsweep + 1) * 3)
+    rows = np.loadtxt(tmp_path / "mpar_full.d")
+    assert rows.shape == (kmax - kmin + 1, 6) and rows[0, 0] == kmax
+    muca = np.loadtxt(tmp_path / "muca.d")
+    assert np.allclose(muca[:, 1], st.b) and np.allclose(muca[:, 2], st.alpha)
