@@ -173,6 +173,9 @@ int smmp_mol_idvr(const smmp_mol_t* m, int* idvr);
 /* The molecule's variables as built (library values, then the .var file's
  * settings; redvar.f): vlvr[nvar] in radians. */
 int smmp_mol_vlvr0(const smmp_mol_t* m, double* vlvr);
+/* The atoms each variable moves, as the contiguous 0-based range
+ * [lo[v], hi[v]] of the molecule's atom order (nvar entries each). */
+int smmp_mol_var_ranges(const smmp_mol_t* m, int* lo, int* hi);
 /* outvar.f:50-121 (outvbs) for one molecule, host only: the text outvar
  * writes for variables vlvr (radians, all variables of the molecule), with
  * molecule number iml in the line prefix.  buf NULL: *len = the bytes needed

@@ -428,6 +428,25 @@ int orc_muca_finish(int kmin, int kmax, double ebin, double beta, double* b, dou
   return guard([&] { oracle::muca_finish(kmin, kmax, ebin, beta, b, alpha); });
 }
 
+// Atoms moved by each variable (1-based atoms of the first molecule):
+// counts[v] atoms listed from atoms[offsets[v]]; offsets has ntlvr+1 entries
+// and atoms room for cap entries.
+int orc_moved_atoms(void* h, int* offsets, int* atoms, int cap) {
+  Smmp* s = S(h);
+  return guard([&] {
+    const auto moved = s->moved_atoms(1);
+    int k = 0;
+    for (int v = 1; v <= ntlvr(s); ++v) {
+      offsets[v - 1] = k;
+      for (int a : moved[v]) {
+        if (k >= cap) throw std::runtime_error("orc_moved_atoms: capacity");
+        atoms[k++] = a;
+      }
+    }
+    offsets[ntlvr(s)] = k;
+  });
+}
+
 // minim.f (quasi-Newton, no regularisation): *nop function calls; log
 // receives up to logcap (energy, |grad|^2) pairs, *nlog the number of pairs.
 int orc_minim(void* h, int imin, int maxit, double eps, int* nop, double* log, int logcap,

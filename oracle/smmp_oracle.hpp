@@ -164,6 +164,9 @@ struct Smmp {
   double gradient();
   std::vector<double> gdeyvr;
   void gradient_by_sums(int nml, std::vector<double>& gd);   // order-free form (tests)
+  // atoms moved by each variable of nml: its moving sets and, recursively,
+  // those of the variables added to it (setmvs.f)
+  std::vector<std::vector<int>> moved_atoms(int nml);
   // opesol.f: eysl and gdeysl[iv] = d(eysl)/d(variable iv) (itysol < 0)
   void opesol(int nml, std::vector<double>& gdeysl);
   // minimisation (minim.f imin = 1, minqsn.f); log: (energy, |grad|^2) per call

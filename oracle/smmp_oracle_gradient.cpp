@@ -282,6 +282,26 @@ double Smmp::gradient() {
   return esm;
 }
 
+std::vector<std::vector<int>> Smmp::moved_atoms(int nml) {
+  const int ifivr = ivrml1[nml], ilavr = ifivr + nvrml[nml] - 1;
+  std::vector<std::vector<int>> moved(ilavr + 1);
+  int i1s = imsml1[nml] + nmsml[nml], i1a = iadml1[nml] + nadml[nml];
+  for (int io = ilavr; io >= ifivr; --io) {   // descending: added variables come first
+    const int iv = iorvr[io];
+    const int i2s = i1s - 1;
+    i1s = imsvr1[iv];
+    for (int ims = i1s; ims <= i2s; ++ims)
+      for (int i = latms1[ims]; i <= latms2[ims]; ++i) moved[iv].push_back(i);
+    const int i2a = i1a - 1;
+    i1a = iadvr1[iv];
+    for (int iad = i1a; iad <= i2a; ++iad) {
+      const std::vector<int>& m = moved[ladvr[iad]];
+      moved[iv].insert(moved[iv].end(), m.begin(), m.end());
+    }
+  }
+  return moved;
+}
+
 // The same derivatives without the ordered recursion: total force on every
 // atom from all of its pairs, then for each variable the force and torque
 // sums over the atoms it moves (its moving sets and, recursively, those of
@@ -328,23 +348,10 @@ void Smmp::gradient_by_sums(int nml, std::vector<double>& gd) {
       for (int j = lvwat1[ivw]; j <= lvwat2[ivw]; ++j) force(i, j, false);
     for (int i14 = i14at1[i]; i14 <= i14at2[i]; ++i14) force(i, l14at[i14], true);
   }
-  // the atoms each variable moves: its moving sets, then the variables added
-  // to it (whose indices the descending order has already completed)
-  std::vector<std::vector<int>> moved(ilavr + 1);
-  int i1s = imsml1[nml] + nmsml[nml], i1a = iadml1[nml] + nadml[nml];
+  const std::vector<std::vector<int>> moved = moved_atoms(nml);
   gd.assign(ilavr + 1, 0.0);
   for (int io = ilavr; io >= ifivr; --io) {
     const int iv = iorvr[io];
-    const int i2s = i1s - 1;
-    i1s = imsvr1[iv];
-    for (int ims = i1s; ims <= i2s; ++ims)
-      for (int i = latms1[ims]; i <= latms2[ims]; ++i) moved[iv].push_back(i);
-    const int i2a = i1a - 1;
-    i1a = iadvr1[iv];
-    for (int iad = i1a; iad <= i2a; ++iad) {
-      const std::vector<int>& m = moved[ladvr[iad]];
-      moved[iv].insert(moved[iv].end(), m.begin(), m.end());
-    }
     double sx = 0, sy = 0, sz = 0, tx = 0, ty = 0, tz = 0;
     for (int i : moved[iv]) {
       sx += fx[i];

@@ -689,6 +689,17 @@ int smmp_mol_outpdb(const smmp_mol_t* m, const double* xyz, char* buf, uint64_t*
   });
 }
 
+int smmp_mol_var_ranges(const smmp_mol_t* m, int* lo, int* hi) {
+  return guard([&] {
+    need(m && lo && hi, "NULL argument");
+    const MolTopo& t = m->m->topo;
+    for (int v = 0; v < t.nvar; ++v) {
+      lo[v] = t.var_lo[v];
+      hi[v] = t.var_hi[v];
+    }
+  });
+}
+
 int smmp_mol_vlvr0(const smmp_mol_t* m, double* vlvr) {
   return guard([&] {
     need(m && vlvr, "NULL argument");

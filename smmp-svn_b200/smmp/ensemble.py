@@ -55,6 +55,11 @@ class Molecule:
         v0 = np.zeros(max(self.nvar, 1))
         check(lib.smmp_mol_vlvr0(self._h, v0.ctypes.data_as(_D)))
         self.vlvr0 = v0[:self.nvar]          # variables as built (library, then .var file)
+        lo = np.zeros(max(self.nvar, 1), dtype=np.int32)
+        hi = np.zeros(max(self.nvar, 1), dtype=np.int32)
+        check(lib.smmp_mol_var_ranges(self._h, lo.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                      hi.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+        self.var_lo, self.var_hi = lo[:self.nvar], hi[:self.nvar]   # atoms each variable moves
 
     def outvar(self, vlvr, iml=1):
         """Text of outvar.f (outvbs, outvar.f:50-121) for the variables vlvr

@@ -37,3 +37,25 @@ def test_sequences_are_seeded_and_valid():
     assert L == polyala_lengths(256) and min(L) >= 10 and max(L) <= 40 and len(L) == 256
     assert polyala(3) == ["ace", "ala", "ala", "ala", "nme"]
     assert abs(sum(NATURAL_COMPOSITION.values()) - 100.0) < 0.2   # rounded percentages
+
+
+def test_moved_atoms_are_the_contiguous_variable_ranges(tmp_path):
+    """The atoms a variable moves in the reference (its moving sets and,
+    recursively, those of the variables added to it; setmvs.f) are exactly
+    the contiguous range [var_lo, var_hi] the product rotates, so derivative
+    sums over them are prefix-sum differences over atoms."""
+    import ctypes
+    from smmp.ensemble import Molecule
+    for name, seq, var, ff, ity in _cases(tmp_path):
+        m = Molecule(seq, var, libdir=DATA, ff=ff, itysol=ity)
+        o = Oracle(seq, var, ff=ff, itysol=ity)
+        lib = o.lib()
+        lib.orc_moved_atoms.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int]
+        cap = 2_000_000
+        off = np.zeros(o.ntlvr + 1, np.int32)
+        at = np.zeros(cap, np.int32)
+        assert lib.orc_moved_atoms(o.h, off.ctypes.data_as(ctypes.c_void_p),
+                                   at.ctypes.data_as(ctypes.c_void_p), cap) == 0
+        for v in range(o.ntlvr):
+            got = np.sort(at[off[v]:off[v + 1]]) - 1
+            assert np.array_equal(got, np.arange(m.var_lo[v], m.var_hi[v] + 1)), (name, v)
