@@ -447,6 +447,17 @@ int orc_moved_atoms(void* h, int* offsets, int* atoms, int cap) {
   });
 }
 
+// Bond-axis frame vectors xtoat/ytoat/ztoat of every atom (3 per atom).
+void orc_get_frames(void* h, double* f) {
+  Smmp* s = S(h);
+  int na = s->iatrs2[s->irsml2[s->ntlml]];
+  for (int i = 1; i <= na; ++i) {
+    f[3 * (i - 1)] = s->xtoat[i];
+    f[3 * (i - 1) + 1] = s->ytoat[i];
+    f[3 * (i - 1) + 2] = s->ztoat[i];
+  }
+}
+
 // minim.f (quasi-Newton, no regularisation): *nop function calls; log
 // receives up to logcap (energy, |grad|^2) pairs, *nlog the number of pairs.
 int orc_minim(void* h, int imin, int maxit, double eps, int* nop, double* log, int logcap,
