@@ -274,7 +274,10 @@ int smmp_sur_gradients(smmp_sur_t* s, const double* ang, const double* energy, i
  * caller owns, and the intermediate activations live in one fixed 16 MiB
  * device array that every GPU loading the library holds until exit.  n above
  * the rows that fit (3,563 for 24 dihedrals, 2,757 for 365) is
- * rejected with SMMP_ERR_ARG.  The first call on a device looks up the
+ * rejected with SMMP_ERR_ARG.  The GPU on which the surrogate was created
+ * (it holds the weights) must be the current device; a call made while
+ * another device is current is rejected with SMMP_ERR_ARG before anything
+ * runs.  The first call on a device looks up the
  * array's device address; make it before any stream capture.  Calls share
  * the array: calls that overlap on the GPU race. stream: a cudaStream_t or
  * NULL (the default stream). */

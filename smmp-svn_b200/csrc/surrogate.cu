@@ -287,6 +287,7 @@ void gemm(cudaStream_t st, int M, int N, int K, const bf16* A, int lda, const bf
 
 Surrogate::Surrogate(int nang, uint64_t seed) : nang_(nang), L_(2 * nang) {
   if (nang <= 0) throw std::invalid_argument("Surrogate: no free dihedrals");
+  check_cuda(cudaGetDevice(&device_), "cudaGetDevice");
   const int H = kHidden;
   wb1_ = 0;
   wb2_ = wb1_ + (size_t)L_.nin_pad * H;
@@ -626,6 +627,12 @@ int Surrogate::noalloc_max_rows(int nin_pad) {
 
 void Surrogate::predict_noalloc(const float* ang_dev, int n, double* energy_dev,
                                 cudaStream_t st) const {
+  int dev = -1;
+  check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+  if (dev != device_)
+    throw std::invalid_argument("smmp_sur_predict_noalloc: device " + std::to_string(dev) +
+                                " is current, but the surrogate's parameters are on device " +
+                                std::to_string(device_) + "; make that device current");
   if (n <= 0) return;
   const int maxn = noalloc_max_rows(L_.nin_pad);
   if (n > maxn)

@@ -37,6 +37,7 @@ class Surrogate {
   Surrogate& operator=(const Surrogate&) = delete;
 
   int nang() const { return nang_; }
+  int device() const { return device_; }   // the GPU that holds the parameters
   const MlpLayout& layout() const { return L_; }
   void set_stream(cudaStream_t s) { stream_ = s; }
 
@@ -61,7 +62,9 @@ class Surrogate {
   DSurrogate device_view();
   // Forward pass that allocates nothing (for callers that cannot allocate
   // device memory): device-resident inputs and outputs, scratch in a fixed
-  // file-scope device array (kNoAllocScratchBytes).  See surrogate.cu.
+  // file-scope device array (kNoAllocScratchBytes).  The surrogate's own GPU
+  // (device()) must be current; another current device is rejected with
+  // std::invalid_argument before anything is launched.  See surrogate.cu.
   void predict_noalloc(const float* ang_dev, int n, double* energy_dev, cudaStream_t st) const;
   static int noalloc_max_rows(int nin_pad);
 
@@ -74,6 +77,7 @@ class Surrogate {
   void sync();
 
   int nang_;
+  int device_ = 0;
   MlpLayout L_;
   cudaStream_t stream_ = nullptr;
   float mu_ = 0.f, sigma_ = 1.f;

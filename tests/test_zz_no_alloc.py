@@ -15,15 +15,19 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _noalloc(s, ang):
+def _noalloc(s, ang, stream=None):
     import torch
     from smmp._lib import check, lib
     a = torch.tensor(np.asarray(ang, dtype=np.float32), device="cuda")
     out = torch.full((a.shape[0],), float("nan"), dtype=torch.float64, device="cuda")
     torch.cuda.synchronize()
+    h = None if stream is None else ctypes.c_void_p(stream.cuda_stream)
     check(lib.smmp_sur_predict_noalloc(s._h, ctypes.c_void_p(a.data_ptr()), a.shape[0],
-                                       ctypes.c_void_p(out.data_ptr()), None))
-    torch.cuda.synchronize()
+                                       ctypes.c_void_p(out.data_ptr()), h))
+    if stream is None:
+        torch.cuda.synchronize()
+    else:
+        stream.synchronize()
     return out.cpu().numpy()
 
 
@@ -50,3 +54,29 @@ def test_noalloc_rejects_more_rows_than_the_scratch_holds():
         _noalloc(s, np.zeros((5000, 24)))
     assert ei.value.status == 1
     assert "exceed the fixed scratch" in str(ei.value)
+
+
+def test_noalloc_allocates_no_device_memory_on_a_side_stream():
+    """After one warm-up call (which loads the kernels and looks up the
+    array's address), a call on a non-default stream leaves the device's free
+    memory unchanged and still equals predict()."""
+    import torch
+    from smmp._lib import check, lib
+    from smmp.surrogate import Surrogate
+    s = Surrogate(24, seed=5)
+    rng = np.random.default_rng(9)
+    ang = rng.uniform(-np.pi, np.pi, (700, 24))
+    want = s.predict(ang)
+    side = torch.cuda.Stream()
+    _noalloc(s, ang, side)                       # warm-up
+    a = torch.tensor(ang.astype(np.float32), device="cuda")
+    out = torch.full((700,), float("nan"), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    check(lib.smmp_sur_predict_noalloc(s._h, ctypes.c_void_p(a.data_ptr()), 700,
+                                       ctypes.c_void_p(out.data_ptr()),
+                                       ctypes.c_void_p(side.cuda_stream)))
+    side.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    np.testing.assert_allclose(out.cpu().numpy(), want, rtol=1e-6, atol=1e-6)
