@@ -176,6 +176,19 @@ int smmp_mol_vlvr0(const smmp_mol_t* m, double* vlvr);
 /* The atoms each variable moves, as the contiguous 0-based range
  * [lo[v], hi[v]] of the molecule's atom order (nvar entries each). */
 int smmp_mol_var_ranges(const smmp_mol_t* m, int* lo, int* hi);
+/* The atoms as built (init_molecule.f:60-136: getmol, addend, redvar), 0-based:
+ * parent[i] (-1 for the first atom), ECEPP class type[i] (1..18), charge[i],
+ * and geom[4*i..4*i+3] = bond length, valence angle, dihedral (radians; the
+ * dihedral state the variable file leaves), solvation radius. */
+int smmp_mol_atoms(const smmp_mol_t* m, int* parent, int* type, double* charge, double* geom);
+/* The variables (getmol.f:206-232, addend.f:583-660, redvar.f): per variable
+ * info[4*v..4*v+3] = primary atom (0-based), torsion class, 1 if fixed by the
+ * variable file, residue (0-based); nvar rows. */
+int smmp_mol_vars(const smmp_mol_t* m, int* info);
+/* The interaction lists (mklist.f:12-303): pairs[3*k..3*k+2] = listing atom,
+ * partner, 1 for a 1-4 pair (0 normal), for the info[3] pair terms of one
+ * energy evaluation, each pair once. */
+int smmp_mol_pairs(const smmp_mol_t* m, int* pairs);
 /* outvar.f:50-121 (outvbs) for one molecule, host only: the text outvar
  * writes for variables vlvr (radians, all variables of the molecule), with
  * molecule number iml in the line prefix.  buf NULL: *len = the bytes needed

@@ -399,6 +399,23 @@ double orc_bench_chains(void* h, int nchains, const int* seeds, const double* be
   return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
+// Test hook (not a reference routine): turn every atom's valence angle by a
+// pseudo-random amount in [-amp, amp] radians, so that geometric checks on
+// the rebuilt molecule meet no collinear atoms (a para ring atom on its
+// ring's rotation axis keeps its distances under that rotation).
+void orc_perturb_valence(void* h, unsigned seed, double amp) {
+  Smmp* s = S(h);
+  int na = s->iatrs2[s->irsml2[s->ntlml]];
+  unsigned long long x = 0x9E3779B97F4A7C15ull ^ seed;
+  for (int i = 1; i <= na; ++i) {
+    x = x * 6364136223846793005ull + 1442695040888963407ull;
+    const double u = (double)(x >> 11) / 9007199254740992.0;   // [0, 1)
+    s->baat[i] += amp * (2.0 * u - 1.0);
+    s->csbaat[i] = std::cos(s->baat[i]);
+    s->snbaat[i] = std::sin(s->baat[i]);
+  }
+}
+
 // gradient.f: energy (vacuum) and dE/dvlvr of every variable (grad[ntlvr]).
 int orc_gradient(void* h, double* e, double* grad) {
   Smmp* s = S(h);

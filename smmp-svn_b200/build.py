@@ -21,13 +21,13 @@ CXX = os.environ.get("CXX", "g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
                   "-I" + SRC, "-I" + INCLUDE]
-# host assembly code keeps the reference's separately rounded FP64 arithmetic
+# host set-up code keeps separately rounded FP64 arithmetic (no contraction)
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I" + SRC, "-I" + INCLUDE]
 
 CUDA_SOURCES = ["kernels.cu", "runtime.cu", "capi.cu", "surrogate.cu", "esolan.cu"]
 # the analytic SASA keeps the reference's separately rounded FP64 arithmetic
 CUDA_EXTRA = {"esolan.cu": ["-fmad=false"]}
-CXX_SOURCES = ["assembly_setup.cpp", "assembly_build.cpp", "topology.cpp", "muca.cpp"]
+CXX_SOURCES = ["molbuild.cpp", "ecepp.cpp", "topology.cpp", "muca.cpp"]
 
 
 def _headers():

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "../../include/smmp_b200.h"
+#include "molbuild.hpp"
 #include "muca.hpp"
 #include "runtime.hpp"
 #include "surrogate.hpp"
@@ -304,12 +305,12 @@ int smmp_init_energy(const char* libdir) {
     Universe& u = U();
     std::string d = libdir;
     if (!d.empty() && d.back() != '/') d += '/';
-    // validate: the library must be readable now, as init_energy reads it
-    Assembly probe;
-    probe.sh2 = u.cfg.sh2 != 0;
-    probe.itysol = u.cfg.itysol;
-    probe.epsd = u.cfg.epsd != 0;
-    probe.init_energy(d);
+    // validate: the library (and the sphere points of a solvation model)
+    // must be readable now, as init_energy reads them
+    need(u.cfg.ientyp == 0, "init_energy: only ientyp=0 (ECEPP) is on this path");
+    ecepp_forcefield(d, u.cfg.sh2 != 0, u.cfg.epsd != 0, u.cfg.itysol);
+    ResidueLibrary probe(library_path(d, u.cfg.sh2 != 0));
+    (void)probe;
     u.libdir = d;
     u.energy_ready = true;
   });
@@ -696,6 +697,56 @@ int smmp_mol_var_ranges(const smmp_mol_t* m, int* lo, int* hi) {
     for (int v = 0; v < t.nvar; ++v) {
       lo[v] = t.var_lo[v];
       hi[v] = t.var_hi[v];
+    }
+  });
+}
+
+int smmp_mol_atoms(const smmp_mol_t* m, int* parent, int* type, double* charge, double* geom) {
+  return guard([&] {
+    need(m && parent && type && charge && geom, "NULL argument");
+    const MolTopo& t = m->m->topo;
+    for (int i = 0; i < t.natoms; ++i) {
+      parent[i] = t.iow[i];
+      type[i] = t.type[i] + 1;
+      charge[i] = t.charge[i];
+      geom[4 * i] = t.blen[i];
+      geom[4 * i + 1] = std::atan2(t.sba[i], t.cba[i]);
+      geom[4 * i + 2] = t.toat0[i];
+      geom[4 * i + 3] = t.rvdw[i];
+    }
+  });
+}
+
+int smmp_mol_vars(const smmp_mol_t* m, int* info) {
+  return guard([&] {
+    need(m && info, "NULL argument");
+    const MolTopo& t = m->m->topo;
+    for (int v = 0; v < t.nvar; ++v) {
+      info[4 * v] = t.var_atom[v];
+      info[4 * v + 1] = t.var_class[v];
+      info[4 * v + 2] = t.var_fixed[v];
+      info[4 * v + 3] = t.var_residue[v];
+    }
+  });
+}
+
+int smmp_mol_pairs(const smmp_mol_t* m, int* pairs) {
+  return guard([&] {
+    need(m && pairs, "NULL argument");
+    const MolTopo& t = m->m->topo;
+    size_t k = 0;
+    for (uint32_t w : t.chunks) {
+      const int i = int(w & 0x3fffu), j0 = int((w >> 14) & 0x3fffu), len = int((w >> 28) & 7u) + 1;
+      for (int j = j0; j < j0 + len; ++j) {
+        pairs[k++] = i;
+        pairs[k++] = j;
+        pairs[k++] = 0;
+      }
+    }
+    for (uint32_t w : t.pairs14) {
+      pairs[k++] = int(w & 0x3fffu);
+      pairs[k++] = int(w >> 14);
+      pairs[k++] = 1;
     }
   });
 }

@@ -8,6 +8,7 @@
 #include <string>
 
 #include "kernels.hpp"
+#include "molbuild.hpp"
 
 namespace smmpb200 {
 
@@ -43,21 +44,16 @@ void d2h(std::vector<T>& h, const T* d, size_t n) {
 std::shared_ptr<Molecule> build_molecule(const std::string& libdir, const Config& cfg,
                                          const std::string& seqfile, const std::string& varfile,
                                          const std::string& grpn, const std::string& grpc) {
+  if (cfg.ientyp != 0) throw std::runtime_error("init_energy: only ientyp=0 (ECEPP) is on this path");
   auto m = std::make_shared<Molecule>();
-  m->assembly = std::make_shared<Assembly>();
-  Assembly& a = *m->assembly;
-  a.sh2 = cfg.sh2 != 0;
-  a.epsd = cfg.epsd != 0;
-  a.itysol = cfg.itysol;
-  a.ientyp = cfg.ientyp;
-  a.rndord = cfg.rndord != 0;
-  std::string dir = libdir;
-  if (!dir.empty() && dir.back() != '/') dir += '/';
-  a.init_energy(dir);
-  a.init_molecule(seqfile, varfile.empty() ? " " : varfile, grpn, grpc);
-  if (a.ntlml != 1) throw std::runtime_error("build_molecule: one molecule per sequence file");
-  m->topo = flatten(a, 1);
-  m->ff = make_forcefield(a);
+  m->ff = ecepp_forcefield(libdir, cfg.sh2 != 0, cfg.epsd != 0, cfg.itysol);
+  const ResidueLibrary lib(library_path(libdir, cfg.sh2 != 0));
+  BuildOptions opt;
+  opt.sh2 = cfg.sh2 != 0;
+  opt.itysol = cfg.itysol;
+  opt.grpn = grpn;
+  opt.grpc = grpc;
+  m->topo = build_topology(lib, m->ff, opt, seqfile, varfile);
   m->cfg = cfg;
   return m;
 }

@@ -8,7 +8,6 @@
 #include <string>
 #include <vector>
 
-#include "assembly.hpp"
 #include "device.cuh"
 #include "topology.hpp"
 
@@ -23,7 +22,6 @@ void check_cuda(cudaError_t e, const char* what);
 
 // A molecule assembled from a residue library, a sequence and a .var file.
 struct Molecule {
-  std::shared_ptr<Assembly> assembly;
   MolTopo topo;
   ForceField ff;
   Config cfg;

@@ -1,6 +1,6 @@
 // Flattened, 0-based topology of one molecule as the GPU kernels read it.
 //
-// flatten() walks an assembled molecule (assembly.hpp) and emits:
+// build_topology() (molbuild.hpp) emits:
 //  * rebuild data: parent atom, bond length, cos/sin of the valence angle, the
 //    atoms grouped by depth below the first backbone atom (one parallel
 //    Eyring step per depth level, bldmol.f:64-78);
@@ -15,8 +15,6 @@
 #include <cstdint>
 #include <string>
 #include <vector>
-
-#include "assembly.hpp"
 
 namespace smmpb200 {
 
@@ -46,6 +44,12 @@ struct ForceField {
   int itysol = 0;
   std::vector<double> spoint;   // npnt*3 unit-sphere points
   int npnt = 0;
+  // torsion constants per torsion class (index 1..19): e0, sign, periodicity
+  std::vector<double> tor_e0, tor_sg, tor_rn;
+  // solvation coefficient and radius per atom class (index 1..18) of the
+  // chosen model, and the probe radius added to heavy atoms
+  std::vector<double> sol_sigma, sol_radius;
+  double probe = 0.0;
 };
 
 struct MolTopo {
@@ -94,9 +98,5 @@ std::string outvar_text(const MolTopo& t, const double* vlvr, int iml);
 // outpdb.f:12-185 for the only molecule of a system: PDB text (80-column
 // lines: ATOM/HETATM, TER, CONECT, END) of coordinates xyz[3*natoms].
 std::string outpdb_text(const MolTopo& t, const double* xyz);
-
-// Build a MolTopo from molecule nml of an assembled system.
-MolTopo flatten(Assembly& a, int nml);
-ForceField make_forcefield(const Assembly& a);
 
 }  // namespace smmpb200

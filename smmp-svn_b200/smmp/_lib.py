@@ -62,6 +62,9 @@ _SIGS = {
     "smmp_mol_idvr": (c_int, [c_void_p, P(c_int)]),
     "smmp_mol_vlvr0": (c_int, [c_void_p, P(c_double)]),
     "smmp_mol_var_ranges": (c_int, [c_void_p, P(c_int), P(c_int)]),
+    "smmp_mol_atoms": (c_int, [c_void_p, P(c_int), P(c_int), P(c_double), P(c_double)]),
+    "smmp_mol_pairs": (c_int, [c_void_p, P(c_int)]),
+    "smmp_mol_vars": (c_int, [c_void_p, P(c_int)]),
     "smmp_mol_outvar": (c_int, [c_void_p, P(c_double), c_int, c_void_p, P(ctypes.c_uint64)]),
     "smmp_outvar": (c_int, [c_int, c_char_p]),
     "smmp_muca_update": (c_int, [c_int, c_int, c_double, c_double, P(c_int), P(c_double),

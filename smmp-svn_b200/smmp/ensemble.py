@@ -61,6 +61,31 @@ class Molecule:
                                       hi.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
         self.var_lo, self.var_hi = lo[:self.nvar], hi[:self.nvar]   # atoms each variable moves
 
+    def atoms(self):
+        """Per atom (0-based): parent (-1 for the first atom), ECEPP class,
+        charge, and [bond length, valence angle, dihedral, solvation radius]."""
+        n = self.natoms
+        par = np.zeros(n, np.int32)
+        typ = np.zeros(n, np.int32)
+        chg = np.zeros(n)
+        geom = np.zeros((n, 4))
+        ip = ctypes.POINTER(ctypes.c_int)
+        check(lib.smmp_mol_atoms(self._h, par.ctypes.data_as(ip), typ.ctypes.data_as(ip),
+                                 chg.ctypes.data_as(_D), geom.ctypes.data_as(_D)))
+        return par, typ, chg, geom
+
+    def variables(self):
+        """Per variable: primary atom (0-based), torsion class, fixed, residue."""
+        out = np.zeros((max(self.nvar, 1), 4), np.int32)
+        check(lib.smmp_mol_vars(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+        return out[:self.nvar]
+
+    def pairs(self):
+        """The interaction lists: rows (listing atom, partner, 1 if 1-4)."""
+        out = np.zeros((max(self.npairs, 1), 3), np.int32)
+        check(lib.smmp_mol_pairs(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+        return out[:self.npairs]
+
     def outvar(self, vlvr, iml=1):
         """Text of outvar.f (outvbs, outvar.f:50-121) for the variables vlvr
         (radians, all nvar of them); iml is the molecule number printed."""

@@ -217,6 +217,21 @@ class Oracle:
         self.lib().orc_get_topology(self.h, P(ai), P(ad), P(vi), P(ms), P(vw), P(l14))
         return ai
 
+    def topology(self):
+        """All of orc_get_topology: (atom_i [n,11], atom_d [n,4], var_i [nv,9],
+        moving sets [nms,2], vdW domains [nvw,3], 1-4 entries [n14,2]);
+        1-based values as in the reference arrays."""
+        na, nv = self.natoms, self.ntlvr
+        ai = np.zeros((na, 11), np.int32)
+        ad = np.zeros((na, 4))
+        vi = np.zeros((nv, 9), np.int32)
+        ms = np.zeros((max(self.sizes[6], 1), 2), np.int32)
+        vw = np.zeros((max(self.sizes[4], 1), 3), np.int32)
+        l14 = np.zeros((max(self.sizes[5], 1), 2), np.int32)
+        P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        self.lib().orc_get_topology(self.h, P(ai), P(ad), P(vi), P(ms), P(vw), P(l14))
+        return ai, ad, vi, ms[:self.sizes[6]], vw[:self.sizes[4]], l14[:self.sizes[5]]
+
     def pair_count(self):
         na, nv = self.natoms, self.ntlvr
         ai = np.zeros((na, 11), np.int32)

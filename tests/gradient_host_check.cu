@@ -14,8 +14,8 @@
 #include <cstdio>
 #include <vector>
 
-#include "assembly.hpp"
 #include "gradient_core.cuh"
+#include "molbuild.hpp"
 #include "topology.hpp"
 
 extern "C" void* orc_create(const char*, int, int, int);
@@ -32,11 +32,9 @@ using namespace smmpb200;
 int main(int argc, char** argv) {
   if (argc < 3) return 2;
   const std::string var = argc > 3 ? argv[3] : " ";
-  Assembly a;
-  a.init_energy(argv[1]);
-  a.init_molecule(argv[2], var, "nh2", "cooh");
-  const MolTopo t = flatten(a, 1);
-  const ForceField ff = make_forcefield(a);
+  const ForceField ff = ecepp_forcefield(argv[1], false, false, 0);
+  const ResidueLibrary lib(library_path(argv[1], false));
+  const MolTopo t = build_topology(lib, ff, BuildOptions{}, argv[2], var);
   const GradTables tab{ff.pair.a, ff.pair.a14, ff.pair.c, ff.pair.hb, ff.conv, ff.plt, ff.slp,
                        ff.epsd};
   void* h = orc_create(argv[1], 0, 0, 0);

@@ -29,7 +29,7 @@ def harness():
         [nvcc, "-std=c++17", "-O2", "-Xcompiler", "-ffp-contract=off", "-I" + SRC,
          "-I" + os.path.join(ROOT, "include"), "-x", "cu",
          os.path.join(ROOT, "tests", "gradient_host_check.cu"), "-x", "c++"] +
-        [os.path.join(SRC, f) for f in ("assembly_setup.cpp", "assembly_build.cpp", "topology.cpp")] +
+        [os.path.join(SRC, f) for f in ("molbuild.cpp", "ecepp.cpp", "topology.cpp")] +
         ["-o", HARNESS, "-L" + odir, "-loracle_smmp", "-Xlinker", "-rpath", "-Xlinker", odir])
     return HARNESS
 
