@@ -315,6 +315,23 @@ int smmp_ens_set_surrogate(smmp_ens_t* e, smmp_sur_t* s, double floor, int min_s
  * winner; ms[3] = the three times in milliseconds (zeros when no molecule
  * allows rows). */
 int smmp_ens_autotune(smmp_ens_t* e, int* choice, double* ms);
+/* Speculative windows (no counterpart in the reference): in the sweep's
+ * incremental mode (FP32 pair terms, row-form pair work, relaxed states, no
+ * SASA) up to `window` consecutive proposals are evaluated at once from the
+ * same state, each as if the earlier ones had been rejected, and the first
+ * accepted one is kept -- the same trajectory bit for bit as one proposal at
+ * a time, with fewer block barriers.  smmp_ens_autotune also times the row
+ * form with windows of 2, 4 and 8 and keeps a window when it is faster.
+ * smmp_ens_set_window sets it by hand (1: one proposal at a time; larger
+ * molecules get a smaller window, see *applied).  smmp_ens_window reports the
+ * window in use and ms[3], the autotuner's times of one sweep with windows of
+ * 2, 4 and 8 (0: not timed). */
+int smmp_ens_set_window(smmp_ens_t* e, int window, int* applied);
+int smmp_ens_window(smmp_ens_t* e, int* window, double* ms);
+/* The pair-work form by hand, as smmp_ens_autotune's choice (0 chunk lists,
+ * 1 rows, 2 rows for molecules of 128+ atoms; molecules without the row
+ * form keep the lists). */
+int smmp_ens_set_pair_work(smmp_ens_t* e, int form);
 /* Per chain: proposals that passed stage 1, and that were then accepted. */
 int smmp_ens_da_stats(smmp_ens_t* e, uint64_t* stage1, uint64_t* stage2);
 /* Parameters and normalisation norm[2] = {mu, sigma}. */

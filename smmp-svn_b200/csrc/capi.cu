@@ -1152,6 +1152,32 @@ int smmp_ens_autotune(smmp_ens_t* e, int* choice, double* ms) {
   });
 }
 
+int smmp_ens_set_window(smmp_ens_t* e, int window, int* applied) {
+  return guard([&] {
+    need(e != nullptr, "NULL ensemble");
+    need(window >= 1, "window must be at least 1");
+    const int k = e->e->set_window(window);
+    if (applied) *applied = k;
+  });
+}
+
+int smmp_ens_window(smmp_ens_t* e, int* window, double* ms) {
+  return guard([&] {
+    need(e != nullptr, "NULL ensemble");
+    if (window) *window = e->e->window();
+    if (ms)
+      for (int k = 0; k < 3; ++k) ms[k] = e->e->window_ms()[k];
+  });
+}
+
+int smmp_ens_set_pair_work(smmp_ens_t* e, int form) {
+  return guard([&] {
+    need(e != nullptr, "NULL ensemble");
+    need(form >= 0 && form <= 2, "pair-work form must be 0, 1 or 2");
+    e->e->set_pair_work(form);
+  });
+}
+
 int smmp_ens_da_stats(smmp_ens_t* e, uint64_t* stage1, uint64_t* stage2) {
   return guard([&] {
     need(e && stage1 && stage2, "NULL argument");

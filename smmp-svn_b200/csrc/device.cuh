@@ -11,6 +11,9 @@ constexpr int kThreads = 512;            // threads per chain (one CTA per chain
 constexpr int kWarps = kThreads / 32;
 constexpr int kMaxNeighbours = 96;       // SASA neighbours per atom (per-warp buffer)
 constexpr int kSasaQueue = 64;           // SASA neighbour candidates queued per warp
+// Speculative window of the sweep (k_sweep): up to this many consecutive
+// proposals evaluated at once from the same state.
+constexpr int kMaxWindow = 8;
 
 // An MT19937 stream slot: 624 state words, mti, the head and tail counters
 // of a queue of tempered values already drawn from the state but not yet
@@ -81,6 +84,7 @@ struct DMolSet {
   int stage_lists;           // 1: the pair lists are staged too (they fit)
   int any_rows;              // 1: some molecule evaluates its pairs by rows
   int da;                    // 1: shared memory for the surrogate's first stage
+  int window;                // proposals per speculative window (<= 1: one at a time)
   const DForceField* ff;     // device
   FFScalars f;
 };

@@ -64,14 +64,14 @@ __device__ __forceinline__ double addang(double a1, double a2) { return wrap_pi(
 // MT19937 stream slots: mt.cuh (mt_seed, mt_twist, temper, mt_grnd, qbuf,
 // stream_next).
 
-// Append 32 values to the queue, and their logarithms to lq (one warp).
-__device__ void rng_refill_warp(uint32_t* slot, double* lq) {
+// Append cnt (<= 32) values to the queue, and their logarithms to lq (one warp).
+__device__ void rng_refill_warp(uint32_t* slot, double* lq, int cnt = 32) {
   const int lane = threadIdx.x & 31;
   if (lane == 0 && slot[kMTIdx] == 625) mt_seed(slot, 4357u);
   __syncwarp();
   uint32_t mti = slot[kMTIdx], qt = slot[kQTail];
   double* q = qbuf(slot);
-  int n1 = min(32, 624 - (int)mti);
+  int n1 = min(cnt, 624 - (int)mti);
   if (lane < n1) {
     double v = temper(slot[mti + lane]);
     int k = (qt + lane) & (kQueue - 1);
@@ -79,10 +79,10 @@ __device__ void rng_refill_warp(uint32_t* slot, double* lq) {
     lq[k] = v > 0.0 ? log(v) : -INFINITY;
   }
   __syncwarp();
-  if (n1 < 32) {
+  if (n1 < cnt) {
     if (lane == 0) mt_twist(slot);
     __syncwarp();
-    int n2 = 32 - n1;
+    int n2 = cnt - n1;
     if (lane < n2) {
       double v = temper(slot[lane]);
       int k = (qt + n1 + lane) & (kQueue - 1);
@@ -91,12 +91,12 @@ __device__ void rng_refill_warp(uint32_t* slot, double* lq) {
     }
     mti = n2;
   } else {
-    mti += 32;
+    mti += cnt;
   }
   __syncwarp();
   if (lane == 0) {
     slot[kMTIdx] = mti;
-    slot[kQTail] = qt + 32;
+    slot[kQTail] = qt + cnt;
   }
   __syncwarp();
 }
@@ -115,6 +115,7 @@ struct Scalars {
   int refill;
   int hlo, hhi;          // heavy-atom indices of the proposal's subtree range
   int gsync;             // result of the last grid barrier
+  int wn;                // proposals of the current speculative window
 };
 
 struct Smem {
@@ -146,13 +147,21 @@ struct Smem {
   __nv_bfloat16* dh1;
   float* dsv;            // surrogate energies of the batch's rows [16]
   Proposal* dprop;       // the batch's proposals [16]
+  // speculative window: per proposal k, the moved atoms' rotated positions
+  // ([k * n + atom]: FP64 and the FP32 hi+lo copies), the warps' partial
+  // energy changes [warp * kMaxWindow + k], and the proposals of this window
+  // and the next ([2][kMaxWindow], alternating)
+  double *wx, *wy, *wz;
+  float4 *wp4, *wl4;
+  double* wred;
+  Proposal* wprop;
   DMol* mol;
   char* pool;            // staged topology (see stage_mol)
 };
 
 __host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~size_t(15); }
 
-__host__ __device__ inline size_t smem_layout(int n, int v, int npnt, bool sasa, bool da,
+__host__ __device__ inline size_t smem_layout(int n, int v, int npnt, bool sasa, bool da, int win,
                                               Smem* s, char* base) {
   size_t off = 0;
   auto take = [&](size_t bytes) -> char* {
@@ -206,6 +215,14 @@ __host__ __device__ inline size_t smem_layout(int n, int v, int npnt, bool sasa,
   t.dh1 = (__nv_bfloat16*)take(da ? 2 * 16 * 264 : 16);
   t.dsv = (float*)take(da ? 4 * 16 : 16);
   t.dprop = (Proposal*)take(da ? sizeof(Proposal) * 16 : 16);
+  const size_t wn = win >= 2 ? (size_t)win * n : 1;
+  t.wx = (double*)take(8 * wn);
+  t.wy = (double*)take(8 * wn);
+  t.wz = (double*)take(8 * wn);
+  t.wp4 = (float4*)take(16 * wn);
+  t.wl4 = (float4*)take(16 * wn);
+  t.wred = (double*)take(win >= 2 ? 8 * kWarps * kMaxWindow : 8);
+  t.wprop = (Proposal*)take(win >= 2 ? sizeof(Proposal) * 2 * kMaxWindow : 16);
   t.sc = (Scalars*)take(sizeof(Scalars));
   t.mol = (DMol*)take(sizeof(DMol));
   t.pool = take(0);
@@ -216,7 +233,8 @@ __host__ __device__ inline size_t smem_layout(int n, int v, int npnt, bool sasa,
 __device__ Smem carve(const DMolSet& set, bool sasa) {
   extern __shared__ __align__(16) char smem_raw[];
   Smem s;
-  smem_layout(set.max_atoms, set.max_vars, set.f.npnt, sasa, set.da != 0, &s, smem_raw);
+  smem_layout(set.max_atoms, set.max_vars, set.f.npnt, sasa, set.da != 0, sasa ? 0 : set.window,
+              &s, smem_raw);
   return s;
 }
 
@@ -351,12 +369,15 @@ __device__ void load_static(const DForceField& ff, const DMol& m, Smem& s, bool 
 // FP32 copy of atom k's position as a hi+lo pair of floats, so that FP32
 // differences of two positions keep FP64-difference accuracy; p4.w holds the
 // charge and l4.w the atom type (as int bits).
-__device__ __forceinline__ void f32_copy(Smem& s, int k) {
-  double x = s.x[k], y = s.y[k], z = s.z[k];
+__device__ __forceinline__ void split_hi_lo(double x, double y, double z, float q, float tbits,
+                                            float4& p4, float4& l4) {
   float xh = (float)x, yh = (float)y, zh = (float)z;
-  s.p4[k] = make_float4(xh, yh, zh, (float)s.cq[k]);
-  s.l4[k] = make_float4((float)(x - (double)xh), (float)(y - (double)yh), (float)(z - (double)zh),
-                        __int_as_float((int)s.type[k]));
+  p4 = make_float4(xh, yh, zh, q);
+  l4 = make_float4((float)(x - (double)xh), (float)(y - (double)yh), (float)(z - (double)zh), tbits);
+}
+__device__ __forceinline__ void f32_copy(Smem& s, int k) {
+  split_hi_lo(s.x[k], s.y[k], s.z[k], (float)s.cq[k], __int_as_float((int)s.type[k]), s.p4[k],
+              s.l4[k]);
 }
 
 // ---------------------------------------------------------------- setvar
@@ -490,9 +511,11 @@ __device__ void full_rebuild(const DMol& m, Smem& s) {
 // One ECEPP/3 pair (enyshe.f:112-184): Coulomb with constant or sigmoidal
 // dielectric, 12-6 Lennard-Jones or 12-10 hydrogen bond.
 template <bool F32>
-__device__ __forceinline__ void pair_term(const FFScalars& ff, const Smem& s, int i, int j,
-                                          bool is14, double& el, double& vw, double& hb) {
-  double dx = s.x[j] - s.x[i], dy = s.y[j] - s.y[i], dz = s.z[j] - s.z[i];
+__device__ __forceinline__ void pair_term_at(const FFScalars& ff, const Smem& s, int i, int j,
+                                             bool is14, double xi, double yi, double zi,
+                                             double xj, double yj, double zj, double& el,
+                                             double& vw, double& hb) {
+  double dx = xj - xi, dy = yj - yi, dz = zj - zi;
   double r2 = dx * dx + dy * dy + dz * dz;
   int tp = s.type[i] * kTypes + s.type[j];
   double A = is14 ? s.ta14[tp] : s.ta[tp];
@@ -524,6 +547,11 @@ __device__ __forceinline__ void pair_term(const FFScalars& ff, const Smem& s, in
     else
       hb += (double)(Af * r6i * r6i - Cf * r6i * r2i * r2i);
   }
+}
+template <bool F32>
+__device__ __forceinline__ void pair_term(const FFScalars& ff, const Smem& s, int i, int j,
+                                          bool is14, double& el, double& vw, double& hb) {
+  pair_term_at<F32>(ff, s, i, j, is14, s.x[i], s.y[i], s.z[i], s.x[j], s.y[j], s.z[j], el, vw, hb);
 }
 
 // Kahan-compensated FP32 accumulator.
@@ -577,21 +605,62 @@ __device__ __noinline__ void pair_term_clash(const FFScalars& ff, const Smem& s,
   pair_term<false>(ff, s, i, j, is14, acc[0], acc[1], acc[2]);
 }
 
+// Positions of the atoms as the current state holds them.
+struct StatePos {
+  const Smem& s;
+  __device__ __forceinline__ float4 p(int a) const { return s.p4[a]; }
+  __device__ __forceinline__ float4 l(int a) const { return s.l4[a]; }
+  __device__ __forceinline__ void clash(const FFScalars& ff, int i, int j, bool is14,
+                                        double* acc) const {
+    pair_term_clash(ff, s, i, j, is14, acc);
+  }
+};
+
+// FP64 term of a clashing pair at given positions (out of line, as above).
+__device__ __noinline__ void pair_term_clash_at(const FFScalars& ff, const Smem& s, int i, int j,
+                                                bool is14, double xi, double yi, double zi,
+                                                double xj, double yj, double zj, double* acc) {
+  pair_term_at<false>(ff, s, i, j, is14, xi, yi, zi, xj, yj, zj, acc[0], acc[1], acc[2]);
+}
+
+// Positions after proposal k of a speculative window: the atoms the
+// proposal turns come from the window buffer k, the rest from the state.
+// The proposal turns the range [lo, hi], or, when that range holds the third
+// backbone atom, everything else but the axis atoms a and b.
+struct WindowPos {
+  const Smem& s;
+  int base, lo, hi, a, b;   // base = k * atoms
+  bool flip;
+  __device__ __forceinline__ bool moved(int t) const {
+    return flip ? ((t < lo || t > hi) && t != a && t != b) : (t >= lo && t <= hi);
+  }
+  __device__ __forceinline__ float4 p(int t) const { return moved(t) ? s.wp4[base + t] : s.p4[t]; }
+  __device__ __forceinline__ float4 l(int t) const { return moved(t) ? s.wl4[base + t] : s.l4[t]; }
+  __device__ __forceinline__ void clash(const FFScalars& ff, int i, int j, bool is14,
+                                        double* acc) const {
+    const bool mi = moved(i), mj = moved(j);
+    pair_term_clash_at(ff, s, i, j, is14, mi ? s.wx[base + i] : s.x[i], mi ? s.wy[base + i] : s.y[i],
+                       mi ? s.wz[base + i] : s.z[i], mj ? s.wx[base + j] : s.x[j],
+                       mj ? s.wy[base + j] : s.y[j], mj ? s.wz[base + j] : s.z[j], acc);
+  }
+};
+
 // One FP32 pair term of the row loop: t = {Coulomb, 12-6, 12-10} for pair
 // (i, j), zero unless `use`; a clashing pair (closer than its guard) goes
 // to the FP64 sums a64 instead.  j must be a valid atom even when !use.
-template <bool TOTAL>
-__device__ __forceinline__ void row_term(const FFScalars& ff, const Smem& s, int i, int j,
-                                         bool use, bool is14, const float4& pi, const float4& li,
-                                         float qi, const float4* trow, double* a64, float* t) {
-  const float4 pj = s.p4[j], lj = s.l4[j];
+template <bool TOTAL, class Pos>
+__device__ __forceinline__ void row_term_at(const FFScalars& ff, const Pos& pos, int i, int j,
+                                            bool use, bool is14, const float4& pi,
+                                            const float4& li, float qi, const float4* trow,
+                                            double* a64, float* t) {
+  const float4 pj = pos.p(j), lj = pos.l(j);
   const float dx = (pj.x - pi.x) + (lj.x - li.x);
   const float dy = (pj.y - pi.y) + (lj.y - li.y);
   const float dz = (pj.z - pi.z) + (lj.z - li.z);
   const float r2 = dx * dx + dy * dy + dz * dz;
   const float4 pr = trow[__float_as_int(lj.w)];
   const bool clash = r2 < fabsf(pr.w);
-  if (use && clash) pair_term_clash(ff, s, i, j, is14, a64);
+  if (use && clash) pos.clash(ff, i, j, is14, a64);
   const float ri = rsqrtf(r2);
   const float r2i = ri * ri;
   const float r6i = r2i * r2i * r2i;
@@ -606,6 +675,12 @@ __device__ __forceinline__ void row_term(const FFScalars& ff, const Smem& s, int
     t[1] = keep && !ishb ? elj : 0.f;
     t[2] = keep && ishb ? elj : 0.f;
   }
+}
+template <bool TOTAL>
+__device__ __forceinline__ void row_term(const FFScalars& ff, const Smem& s, int i, int j,
+                                         bool use, bool is14, const float4& pi, const float4& li,
+                                         float qi, const float4* trow, double* a64, float* t) {
+  row_term_at<TOTAL>(ff, StatePos{s}, i, j, use, is14, pi, li, qi, trow, a64, t);
 }
 
 // Pair sums by rows, for molecules whose pair set has the row form (m.rows):
@@ -691,9 +766,9 @@ __device__ void pair_rows(const FFScalars& ff, const DMol& m, const Smem& s, int
 // partners beyond hi (row form: the first 64 partners of a row are masked).
 // A proposal's energy change is this sum after the rotation minus the same
 // sum before it, computed by the same threads over the same pairs.
-template <bool F32>
-__device__ double cross_rows(const FFScalars& ff, const DMol& m, const Smem& s, int nw, int lo,
-                             int hi) {
+template <bool F32, class Pos>
+__device__ double cross_rows_at(const FFScalars& ff, const DMol& m, const Smem& s, const Pos& pos,
+                                int nw, int lo, int hi) {
   const int lane = threadIdx.x & 31, n = m.natoms;
   double e64[3] = {0.0, 0.0, 0.0};
   KSum ke;
@@ -703,7 +778,7 @@ __device__ double cross_rows(const FFScalars& ff, const DMol& m, const Smem& s, 
     const int je = i < lo ? hi : n - 1;
     if (jb > je) continue;
     const unsigned long long nm = m.near_mask[i], n14 = m.near14[i];
-    if (!F32 || ff.epsd) {
+    if (!F32 || ff.epsd) {   // FP64 terms read the state (the one-at-a-time sweep only)
       for (int j = jb + lane; j <= je; j += 32) {
         const int d = j - i - 1;
         bool use = true, is14 = false;
@@ -715,7 +790,7 @@ __device__ double cross_rows(const FFScalars& ff, const DMol& m, const Smem& s, 
       }
       continue;
     }
-    const float4 pi = s.p4[i], li = s.l4[i];
+    const float4 pi = pos.p(i), li = pos.l(i);
     const float qi = convf * pi.w;
     const float4* trow = s.tab4 + __float_as_int(li.w) * kTypes;
     for (int j0 = jb; j0 <= je; j0 += 32) {
@@ -726,11 +801,16 @@ __device__ double cross_rows(const FFScalars& ff, const DMol& m, const Smem& s, 
         is14 = ((n14 >> d) & 1ull) != 0;
       }
       float t[3];
-      row_term<true>(ff, s, i, use ? j : jb, use, is14, pi, li, qi, trow, e64, t);
+      row_term_at<true>(ff, pos, i, use ? j : jb, use, is14, pi, li, qi, trow, e64, t);
       ke.add(t[0] + t[1]);
     }
   }
   return ((ke.value() + e64[0]) + e64[1]) + e64[2];
+}
+template <bool F32>
+__device__ double cross_rows(const FFScalars& ff, const DMol& m, const Smem& s, int nw, int lo,
+                             int hi) {
+  return cross_rows_at<F32>(ff, m, s, StatePos{s}, nw, lo, hi);
 }
 
 // Pair sums of the threads [0, nthr): by rows when the molecule has the row
@@ -1378,6 +1458,293 @@ __device__ __forceinline__ int moved_atom(int t, int lo, int span, bool flip) {
   return flip ? (t < lo ? t : t + span) : lo + t;
 }
 
+// The rotation a proposal applies: about the unit axis a -> b through b, by
+// (cth, sth); by -theta when the complement of the subtree turns.
+struct Axis {
+  double px, py, pz, kx, ky, kz, cth, sth;
+};
+__device__ __forceinline__ Axis proposal_axis(const Smem& s, const Proposal& cur, bool flip) {
+  Axis ax;
+  ax.cth = cur.cth;
+  ax.sth = flip ? -cur.sth : cur.sth;
+  ax.px = s.x[cur.b];
+  ax.py = s.y[cur.b];
+  ax.pz = s.z[cur.b];
+  double kx = ax.px - s.x[cur.a], ky = ax.py - s.y[cur.a], kz = ax.pz - s.z[cur.a];
+  double inv = rsqrt(kx * kx + ky * ky + kz * kz);
+  ax.kx = kx * inv;
+  ax.ky = ky * inv;
+  ax.kz = kz * inv;
+  return ax;
+}
+// Rodrigues' rotation of one point (the in-place move of the one-at-a-time
+// sweep and the copies of the speculative window use this one expression).
+__device__ __forceinline__ void rotate_point(const Axis& ax, double x, double y, double z,
+                                             double& ox, double& oy, double& oz) {
+  double vx = x - ax.px, vy = y - ax.py, vz = z - ax.pz;
+  double kd = ax.kx * vx + ax.ky * vy + ax.kz * vz;
+  double cx = ax.ky * vz - ax.kz * vy, cy = ax.kz * vx - ax.kx * vz, cz = ax.kx * vy - ax.ky * vx;
+  double f = kd * (1.0 - ax.cth);
+  ox = ax.px + vx * ax.cth + cx * ax.sth + ax.kx * f;
+  oy = ax.py + vy * ax.cth + cy * ax.sth + ax.ky * f;
+  oz = ax.pz + vz * ax.cth + cz * ax.sth + ax.kz * f;
+}
+
+// Proposal k of a speculative window (metropolis.f:42-66) from the window's
+// state, as the one-at-a-time sweep would make it after k rejected
+// proposals: those leave the coordinates, the other variables and the
+// energies as they were, the stream k * (used + 1) numbers further on, and
+// the dihedral state after k more setvar replays, which on this variable's
+// own atom (its base carries no other variable) move it towards its value
+// until it stops changing.
+__device__ void make_proposal_w(const DMol& m, const Smem& s, int p, uint32_t pos, bool rndord,
+                                int replays, Proposal& out) {
+  const double* q = qbuf(s.mt);
+  uint32_t k = pos;
+  int ivar = p;
+  if (rndord) {
+    ivar = (int)__dmul_rn((double)m.nfree, q[k & (kQueue - 1)]);
+    if (ivar >= m.nfree) ivar = m.nfree - 1;
+    ++k;
+  }
+  int jv = m.idvr[ivar];
+  double vold = s.vlvr[jv];
+  double dv = __dmul_rn(m.axvr[jv], __dsub_rn(q[k & (kQueue - 1)], 0.5));
+  ++k;
+  double vnew = addang(vold, dv);
+  double sv, cv;
+  sincos(difang(vold, vnew), &sv, &cv);
+  int iat = m.var_atom[jv];
+  double t0 = s.toat[iat];
+  for (int r = 0; r < replays; ++r) {   // setvar_one on iat with vlvr = vold
+    const double tsh = difang(t0, vold);
+    if (tsh == 0.0) break;
+    t0 = __dadd_rn(t0, tsh);
+    if (fabs(t0) > kPi) t0 = __dsub_rn(t0, copysign(kPi2, t0));
+  }
+  double to = __dadd_rn(t0, difang(t0, vnew));
+  if (fabs(to) > kPi) to = __dsub_rn(to, copysign(kPi2, to));
+  out.jv = jv;
+  out.ivar = ivar;
+  out.used = (int)(k - pos);
+  out.b = m.var_base[jv];
+  out.a = m.iow[out.b];
+  out.vold = vold;
+  out.vnew = vnew;
+  out.cth = cv;
+  out.sth = sv;
+  out.enew = torsion_term(m, jv, to);
+  out.eold = s.et[jv];
+}
+
+// The speculative window of the next proposals from p0 (one warp): up to
+// set.window of them, ending before the 16th-proposal re-sum point and
+// before a variable the window already holds; written to wp[0..wn).
+__device__ void build_window(const DMolSet& set, const DMol& m, Smem& s, int p0, uint32_t hd,
+                             bool rndord, Proposal* wp, int* err) {
+  const int lane = threadIdx.x & 31;
+  const int u = rndord ? 2 : 1;
+  int wn = min(min(set.window, kMaxWindow), m.nfree - p0);
+  wn = min(wn, 16 - (p0 & 15));
+  // The window's numbers are in the queue: the sweep's first window tops it
+  // up before any decision reads it, and every window's pair-sum phase tops
+  // it up to 48 past its head, so a window of up to 8 (rndord: 3 numbers
+  // each) finds its numbers without a refill here, where other warps may
+  // still read the queue.  Anything else is a bug: the window shrinks to
+  // what is queued and the chain reports a consistency error.
+  const uint32_t avail = s.mt[kQTail] - hd;
+  if ((uint32_t)(wn * (u + 1)) > avail) {
+    wn = max(1, (int)(avail / (u + 1)));
+    if (lane == 0) set_err(err, kErrConsistency);
+  }
+  Proposal P;
+  int jv = -1;
+  if (lane < wn) {
+    make_proposal_w(m, s, p0 + lane, hd + (uint32_t)(lane * (u + 1)), rndord, lane, P);
+    jv = P.jv;
+  }
+  bool again = false;
+  for (int j = 0; j < kMaxWindow - 1; ++j) {
+    const int jj = __shfl_sync(0xffffffffu, jv, j);
+    if (j < lane && lane < wn && jj == jv) again = true;
+  }
+  const unsigned rm = __ballot_sync(0xffffffffu, again);
+  if (rm) wn = min(wn, __ffs(rm) - 1);
+  if (lane < wn) wp[lane] = P;
+  if (lane == 0) s.sc->wn = wn;
+  __syncwarp();
+}
+
+// The proposals of the rest of a sweep in speculative windows (FP32 pair
+// terms, row-form molecules, relaxed states: the sweep's incremental mode).
+// The proposals of a window are made from the same state, each as if the
+// earlier ones had been rejected, which is exactly the state a rejection
+// leaves.  Their energy changes are summed in one pass; the first accepted
+// proposal ends the window and the later ones are dropped.  Each proposal
+// draws the same numbers, is summed over the same pairs by the same threads
+// in the same order and decided with the same arithmetic as in the
+// one-at-a-time loop of k_sweep, so the trajectory is the same bit for bit:
+// a window of w proposals costs three block barriers instead of 3w.
+template <bool F32>
+__device__ __noinline__ void sweep_windows(const DMolSet& set, const DMol& m, Smem& s,
+                                           const DWeight& w, double beta, int* err, bool rndord,
+                                           double& eol, double& etor, double& ep, uint32_t& head,
+                                           unsigned long long& nacc, unsigned long long& nprop) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int spec_warp = kWarps - 1;
+  const int n = m.natoms;
+  const int u = rndord ? 2 : 1;
+  if (warp == spec_warp) {
+    while (s.mt[kQTail] - head < 24) rng_refill_warp(s.mt, s.lq);   // nobody reads the queue yet
+    build_window(set, m, s, 0, head, rndord, s.wprop, err);
+  }
+  __syncthreads();
+  int p = 0, half = 0;
+  while (p < m.nfree) {
+    const Proposal* wp = s.wprop + half * kMaxWindow;
+    const int wn = s.sc->wn;
+    const bool resum = p > 0 && (p & 15) == 0;
+    // ---- phase R: each proposal's moved atoms, turned, into its buffer;
+    // the state's pair energy summed afresh every 16 proposals
+    for (int idx = threadIdx.x; idx < wn * n; idx += blockDim.x) {
+      const int k = idx / n, t = idx - k * n;
+      const Proposal& P = wp[k];
+      const int lo = m.var_lo[P.jv], hi = m.var_hi[P.jv];
+      const bool flip = lo <= m.i3 && m.i3 <= hi;
+      const int span = hi - lo + 1;
+      if (t >= (flip ? n - span : span)) continue;
+      const int a = moved_atom(t, lo, span, flip);
+      if (flip && (a == P.a || a == P.b)) continue;   // on the axis
+      const Axis ax = proposal_axis(s, P, flip);
+      double ox, oy, oz;
+      rotate_point(ax, s.x[a], s.y[a], s.z[a], ox, oy, oz);
+      const int o = k * n + a;
+      s.wx[o] = ox;
+      s.wy[o] = oy;
+      s.wz[o] = oz;
+      split_hi_lo(ox, oy, oz, s.p4[a].w, s.l4[a].w, s.wp4[o], s.wl4[o]);
+    }
+    if (resum) {
+      double el = 0.0, vw = 0.0, hb = 0.0;
+      pair_rows<F32, true>(set.f, m, s, kWarps, el, vw, hb);
+      double v = el;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) s.red[warp * 8 + 2] = v;
+    }
+    __syncthreads();
+    if (resum) {
+      double fresh_ep = 0.0;
+      for (int k = 0; k < kWarps; ++k) fresh_ep += s.red[k * 8 + 2];
+      eol = (eol - ep) + fresh_ep;
+      ep = fresh_ep;
+    }
+    // ---- phase S: every proposal's energy change over the pairs across its
+    // bond (after minus before, per thread, as the one-at-a-time sweep forms
+    // it); meanwhile the last warp tops the stream's queue up to 48 numbers
+    // past the head (16 at a time: at most 63 of its 64 places are taken)
+    if (warp == spec_warp) {
+      while (s.mt[kQTail] - head < 48) rng_refill_warp(s.mt, s.lq, 16);
+    } else {
+      for (int k = 0; k < wn; ++k) {
+        const Proposal& P = wp[k];
+        const int lo = m.var_lo[P.jv], hi = m.var_hi[P.jv];
+        const bool flip = lo <= m.i3 && m.i3 <= hi;
+        const double before = cross_rows_at<F32>(set.f, m, s, StatePos{s}, kWarps - 1, lo, hi);
+        const double after = cross_rows_at<F32>(
+            set.f, m, s, WindowPos{s, k * n, lo, hi, P.a, P.b, flip}, kWarps - 1, lo, hi);
+        double v = ((after - before) + 0.0) + 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) s.wred[warp * kMaxWindow + k] = v;
+      }
+    }
+    __syncthreads();
+    // ---- phase D: every warp decides the window the same way; lane k
+    // takes proposal k (metropolis.f:72-87)
+    double dpair = 0.0, enw = 0.0, etn = 0.0;
+    int up = 0, drew = 1;
+    if (lane < wn) {
+      const Proposal& P = wp[lane];
+      for (int k = 0; k < kWarps - 1; ++k) dpair += s.wred[k * kMaxWindow + lane];
+      const double epair = (ep + dpair) + 0.0;
+      etn = (etor - P.eold) + P.enew;
+      enw = epair + etn;
+      const double delta = __dsub_rn(weight(w, beta, enw), weight(w, beta, eol));
+      if (delta <= 0.0) {
+        up = 1;
+        drew = 0;
+      } else {
+        const uint32_t kq = (head + (uint32_t)(lane * (u + 1) + P.used)) & (kQueue - 1);
+        const double rd = qbuf(s.mt)[kq], lrd = s.lq[kq];
+        const double d = fmin(delta, 100.0);
+        const double margin = -d - lrd;
+        if (margin > 1e-10)
+          up = 1;
+        else if (margin < -1e-10)
+          up = 0;
+        else
+          up = exp(-d) >= rd ? 1 : 0;
+      }
+    }
+    const unsigned am = __ballot_sync(0xffffffffu, lane < wn && up);
+    const int ks = am ? __ffs(am) - 1 : -1;
+    const int last = ks >= 0 ? ks : wn - 1;
+    const unsigned bad = __ballot_sync(0xffffffffu, lane <= last && !isfinite(enw));
+    if (threadIdx.x == 0 && bad) set_err(err, kErrNonFinite);
+    const int src = ks >= 0 ? ks : 0;
+    const double enw_k = __shfl_sync(0xffffffffu, enw, src);
+    const double etn_k = __shfl_sync(0xffffffffu, etn, src);
+    const double dpair_k = __shfl_sync(0xffffffffu, dpair, src);
+    const int drew_last = ks >= 0 ? __shfl_sync(0xffffffffu, drew, src) : 1;
+    // ---- phase C: the accepted proposal's atoms take their turned copies;
+    // the last warp replays the window's setvar calls on the dihedral state
+    // and makes the next window
+    if (ks >= 0) {
+      const Proposal& P = wp[ks];
+      const int lo = m.var_lo[P.jv], hi = m.var_hi[P.jv];
+      const bool flip = lo <= m.i3 && m.i3 <= hi;
+      const int span = hi - lo + 1;
+      const int nmoved = flip ? n - span : span;
+      for (int t = threadIdx.x; t < nmoved; t += blockDim.x) {
+        const int a = moved_atom(t, lo, span, flip);
+        if (flip && (a == P.a || a == P.b)) continue;
+        const int o = ks * n + a;
+        s.x[a] = s.wx[o];
+        s.y[a] = s.wy[o];
+        s.z[a] = s.wz[o];
+        s.p4[a] = s.wp4[o];
+        s.l4[a] = s.wl4[o];
+      }
+    }
+    head += (uint32_t)(last * (u + 1) + u + drew_last);
+    nprop += (unsigned long long)(last + 1);
+    if (ks >= 0) {
+      ++nacc;
+      eol = enw_k;
+      etor = etn_k;
+      ep += dpair_k;
+    }
+    p += last + 1;
+    if (warp == spec_warp) {
+      for (int j = 0; j <= last; ++j) {   // metropolis.f:53-87 through energy()'s setvar
+        if (lane == 0) s.vlvr[wp[j].jv] = wp[j].vnew;
+        __syncwarp();
+        setvar_warp(m, s);
+        __syncwarp();
+        if (lane == 0 && j != ks) s.vlvr[wp[j].jv] = wp[j].vold;
+        __syncwarp();
+      }
+      if (lane == 0 && ks >= 0) s.et[wp[ks].jv] = wp[ks].enew;
+      __syncwarp();
+      if (p < m.nfree)
+        build_window(set, m, s, p, head, rndord, s.wprop + (half ^ 1) * kMaxWindow, err);
+    }
+    half ^= 1;
+    __syncthreads();
+  }
+}
+
 // nsweeps Metropolis sweeps (metropolis.f:13-184) of chains
 // [first, first+gridDim.x).  Per sweep the reference calls energy() nvr+2
 // times; here the start of every sweep does a full setvar+rebuild+evaluation,
@@ -1457,14 +1824,21 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
     check_pending = false;
     eol = enew;
     const bool relaxed = fabs(eol) < 1e4;
-    if (m.nfree > 0 && threadIdx.x == 0) {
+    bool windowed = false;
+    if constexpr (ROWS && F32 && !SASA) {
+      // the incremental mode in speculative windows (same trajectory, fewer barriers)
+      windowed = m.rows && !set.f.epsd && relaxed && set.window >= 2 && m.nfree > 0;
+      if (windowed)
+        sweep_windows<F32>(set, m, s, w, beta, err, rndord, eol, etor, ep, head, nacc, nprop);
+    }
+    if (!windowed && m.nfree > 0 && threadIdx.x == 0) {
       make_proposal(m, s, 0, head, rndord, sc.cur);
       s.vlvr[sc.cur.jv] = sc.cur.vnew;
       sc.refill = 0;
     }
     __syncthreads();
 
-    for (int p = 0; p < m.nfree; ++p) {
+    for (int p = 0; p < (windowed ? 0 : m.nfree); ++p) {
       const Proposal cur = sc.cur;
       const int lo = m.var_lo[cur.jv], hi = m.var_hi[cur.jv];
       // The rebuild holds the first three backbone atoms in place (setgbl):
@@ -1520,26 +1894,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       }
       // ---- phase A: rotate the subtree of cur.jv about its bond (+theta)
       {
-        const double sth = flip ? -cur.sth : cur.sth;
-        double px = s.x[cur.b], py = s.y[cur.b], pz = s.z[cur.b];
-        double kx = px - s.x[cur.a], ky = py - s.y[cur.a], kz = pz - s.z[cur.a];
-        double inv = rsqrt(kx * kx + ky * ky + kz * kz);
-        kx *= inv;
-        ky *= inv;
-        kz *= inv;
+        const Axis ax = proposal_axis(s, cur, flip);
         for (int t = threadIdx.x; t < nmoved; t += blockDim.x) {
           const int k = moved_atom(t, lo, span, flip);
           if (flip && (k == cur.a || k == cur.b)) continue;   // on the axis
-          double vx = s.x[k] - px, vy = s.y[k] - py, vz = s.z[k] - pz;
           s.bx[k] = s.x[k];
           s.by[k] = s.y[k];
           s.bz[k] = s.z[k];
-          double kd = kx * vx + ky * vy + kz * vz;
-          double cx = ky * vz - kz * vy, cy = kz * vx - kx * vz, cz = kx * vy - ky * vx;
-          double f = kd * (1.0 - cur.cth);
-          s.x[k] = px + vx * cur.cth + cx * sth + kx * f;
-          s.y[k] = py + vy * cur.cth + cy * sth + ky * f;
-          s.z[k] = pz + vz * cur.cth + cz * sth + kz * f;
+          rotate_point(ax, s.bx[k], s.by[k], s.bz[k], s.x[k], s.y[k], s.z[k]);
           if (F32) f32_copy(s, k);
         }
       }
@@ -2073,8 +2435,9 @@ __global__ void __launch_bounds__(32) k_exchange(DChains ch, int* temp_chain, co
 // ============================================================================ host wrappers
 
 size_t sweep_smem_bytes(const DMolSet& set) {
-  return smem_layout(set.max_atoms, set.max_vars, set.f.npnt, set.f.itysol > 0, set.da != 0,
-                     nullptr, nullptr) +
+  const bool sasa = set.f.itysol > 0;
+  return smem_layout(set.max_atoms, set.max_vars, set.f.npnt, sasa, set.da != 0,
+                     sasa ? 0 : set.window, nullptr, nullptr) +
          (size_t)set.stage_bytes;
 }
 

@@ -927,7 +927,17 @@ MolTopo build_topology(const ResidueLibrary& lib, const ForceField& ff, const Bu
     std::vector<int> fill(t.level_off.begin(), t.level_off.end() - 1);
     for (int i = 0; i < n; ++i) t.level_atoms[fill[depth[i]]++] = i;
   }
-  // variables: the base's children turn; their subtrees form one run
+  // variables: the base's children turn; their subtrees form one run.  A
+  // base carries one torsion (setmvs.f:15-17): the sweep relies on it, since
+  // a variable's replayed setvar then moves no other variable's atom.
+  {
+    std::vector<int> seen(n, -1);
+    for (int v = 0; v < nv; ++v) {
+      const int base = atoms[vars[v].atom].parent;
+      if (seen[base] >= 0) fail("setmvs> two torsion variables turn about one base atom");
+      seen[base] = v;
+    }
+  }
   std::vector<int> axis_o(nv);
   t.sib_off.push_back(0);
   for (int v = 0; v < nv; ++v) {

@@ -8,12 +8,15 @@
 //  * a torsion variable turns the subtrees hanging from its base atom (the
 //    parent of its primary atom) about the bond base -> parent(base); those
 //    subtrees are one contiguous atom range [lo, hi] (checked);
-//  * the pair set is every atom pair whose distance some variable changes:
-//    the variable's range holds exactly one atom of the pair and the other
-//    atom is not on the variable's axis (neither its base nor the base's
-//    parent).  A pair whose distance exactly one variable changes is a 1-4
-//    pair (Scheraga's "depends on one dihedral" definition), every other
-//    changing pair a normal one;
+//  * every atom belongs to the rigid group of the innermost variable whose
+//    range holds it; the pair set is every pair whose distance some variable
+//    changes: an atom of a variable's group with any atom of a group whose
+//    range starts earlier, except the two atoms on the variable's axis (its
+//    base and the base's parent);
+//  * a pair is a 1-4 pair when its partner holds the axis's outer atom: the
+//    outer atom's other children with the rest of their contiguous group
+//    runs, the outer atom's parent, and the base's own run (the reference's
+//    rule; every such pair depends on that one variable alone);
 //  * each pair is listed under the atom of the innermost-moved rigid group
 //    (the group whose variable's range starts later), partners as runs of
 //    consecutive atoms.

@@ -203,6 +203,16 @@ void DeviceSet::set_rows(int mode) {
   size_staging();
 }
 
+int DeviceSet::set_window(int k) {
+  k = std::max(1, std::min(k, kMaxWindow));
+  if (set_.f.itysol > 0) k = 1;
+  const size_t per = (size_t)std::max(set_.max_atoms, 1) * (3 * 8 + 2 * 16);   // FP64 + hi/lo
+  while (k >= 2 && (size_t)k * per > 64 * 1024) --k;
+  set_.window = k >= 2 ? k : 0;
+  size_staging();
+  return k;
+}
+
 void DeviceSet::set_da(bool on) {
   set_.da = on ? 1 : 0;
   size_staging();
@@ -346,13 +356,34 @@ void Ensemble::set_surrogate(const DSurrogate* view, float floor, int min_stage1
   graph_len_ = 0;
 }
 
+void Ensemble::set_pair_work(int form) {
+  if (form < 0 || form > 2) throw std::invalid_argument("pair-work form must be 0, 1 or 2");
+  const int rows_mode[3] = {0, 1, -1};
+  dev_->set_rows(rows_mode[form]);
+  if (graph_) cudaGraphExecDestroy(graph_);   // kernel arguments changed
+  graph_ = nullptr;
+  graph_len_ = 0;
+}
+
+int Ensemble::set_window(int k) {
+  const int got = dev_->set_window(k);
+  if (graph_) cudaGraphExecDestroy(graph_);   // kernel arguments changed
+  graph_ = nullptr;
+  graph_len_ = 0;
+  return got;
+}
+
 // Autotuner: time one sweep of every chain with each pair-work form (0:
 // chunk lists; 1: 32-partner row passes; 2: row passes for molecules of 128
-// atoms or more, lists for the rest) from the same saved state, keep the
-// fastest, and put the state back.  The timed sweeps leave no trace.
+// atoms or more, lists for the rest), then the row form with speculative
+// windows of 2, 4 and 8 proposals, each from the same saved state (best of
+// three timed sweeps after a warm-up), keep the fastest, and put the state
+// back.  The timed sweeps leave no trace.
 int Ensemble::autotune(int flags, double* ms_out) {
+  window_ms_[0] = window_ms_[1] = window_ms_[2] = 0.0;
   if (!dev_->any_rows_possible()) {
     if (ms_out) ms_out[0] = ms_out[1] = ms_out[2] = 0.0;
+    set_window(1);
     return 0;
   }
   check_cuda(cudaStreamSynchronize(stream_), "autotune sync");
@@ -388,27 +419,49 @@ int Ensemble::autotune(int flags, double* ms_out) {
   cudaEvent_t e0, e1;
   check_cuda(cudaEventCreate(&e0), "event");
   check_cuda(cudaEventCreate(&e1), "event");
-  double ms[3] = {0.0, 0.0, 0.0};
-  const int rows_mode[3] = {0, 1, -1};   // DeviceSet::set_rows argument of each form
-  for (int mode = 0; mode < 3; ++mode) {
-    dev_->set_rows(rows_mode[mode]);
+  auto time_sweep = [&]() {
     restore();
     launch_sweep_range(0, n_, 1, flags | kFlagNoCheck, w);   // warm-up
     check_cuda(cudaStreamSynchronize(stream_), "autotune sync");
-    restore();
-    check_cuda(cudaEventRecord(e0, stream_), "event");
-    launch_sweep_range(0, n_, 1, flags | kFlagNoCheck, w);
-    check_cuda(cudaEventRecord(e1, stream_), "event");
-    check_cuda(cudaEventSynchronize(e1), "event sync");
-    float f = 0.f;
-    check_cuda(cudaEventElapsedTime(&f, e0, e1), "event time");
-    ms[mode] = f;
+    double best_ms = 1e300;
+    for (int rep = 0; rep < 3; ++rep) {
+      restore();
+      check_cuda(cudaEventRecord(e0, stream_), "event");
+      launch_sweep_range(0, n_, 1, flags | kFlagNoCheck, w);
+      check_cuda(cudaEventRecord(e1, stream_), "event");
+      check_cuda(cudaEventSynchronize(e1), "event sync");
+      float f = 0.f;
+      check_cuda(cudaEventElapsedTime(&f, e0, e1), "event time");
+      best_ms = std::min(best_ms, (double)f);
+    }
+    return best_ms;
+  };
+  double ms[3] = {0.0, 0.0, 0.0};
+  const int rows_mode[3] = {0, 1, -1};   // DeviceSet::set_rows argument of each form
+  dev_->set_window(1);
+  for (int mode = 0; mode < 3; ++mode) {
+    dev_->set_rows(rows_mode[mode]);
+    ms[mode] = time_sweep();
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   int best = 0;
   for (int mode = 1; mode < 3; ++mode)
     if (ms[mode] < ms[best]) best = mode;
+  double best_ms = ms[best];
+  int best_window = 1;
+  const int windows[3] = {2, 4, 8};
+  for (int k = 0; k < 3; ++k) {   // speculative windows need the row form
+    dev_->set_rows(1);
+    if (dev_->set_window(windows[k]) != windows[k]) break;
+    window_ms_[k] = time_sweep();
+    if (window_ms_[k] < best_ms) {
+      best_ms = window_ms_[k];
+      best = 1;
+      best_window = windows[k];
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  dev_->set_window(best_window);
   dev_->set_rows(rows_mode[best]);
   restore();
   if (graph_) cudaGraphExecDestroy(graph_);   // kernel arguments changed

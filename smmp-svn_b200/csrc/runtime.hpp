@@ -44,6 +44,11 @@ class DeviceSet {
   // -1 the size-based default
   void set_rows(int mode);
   int any_rows_possible() const;
+  // proposals per speculative window of the sweep (1: one at a time); the
+  // window's buffers take up to 64 KB of shared memory, which caps it for
+  // large molecules, and SASA sweeps run one at a time.  Returns the size set.
+  int set_window(int k);
+  int window() const { return set_.window >= 2 ? set_.window : 1; }
 
  private:
   void size_staging();
@@ -97,6 +102,15 @@ class Ensemble {
   // saved state, keeps the fastest and restores the state.  Returns the
   // winner; ms_out[3] the three times.
   int autotune(int flags, double* ms_out);
+  // The speculative window the autotuner chose (1: none) and the times of
+  // one sweep with windows of 2, 4 and 8 proposals on the row form (0: not
+  // timed); set_window fixes it by hand.
+  int window() const { return dev_->window(); }
+  int set_window(int k);
+  const double* window_ms() const { return window_ms_; }
+  // pair-work form by hand (as autotune's choice: 0 chunk lists, 1 rows,
+  // 2 rows for molecules of 128+ atoms)
+  void set_pair_work(int form);
   cudaStream_t stream() const { return stream_; }
   const DChains& chains() const { return ch_; }
   const DMolSet& set() const { return dev_->set(); }
@@ -167,6 +181,7 @@ class Ensemble {
   cudaGraphExec_t graph_ = nullptr;
   int graph_len_ = 0, graph_flags_ = -1;
   bool pt_fused_last_ = false;   // the last batched pt_sweeps ran the fused launch
+  double window_ms_[3] = {0.0, 0.0, 0.0};
   double* coords_buf_ = nullptr;
   // analytic SASA (itysol < 0): per-thread scratch of k_esolan for
   // kEsolanBatch chains, the per-atom areas of every chain

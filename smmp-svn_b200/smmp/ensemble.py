@@ -279,6 +279,25 @@ class Ensemble:
         check(lib.smmp_ens_autotune(self._h, ctypes.byref(choice), ms))
         return self.AUTOTUNE_FORMS[choice.value], (ms[0], ms[1], ms[2])
 
+    def set_window(self, k):
+        """Proposals per speculative window of the sweep (1: one at a time);
+        returns the size applied (large molecules get smaller windows)."""
+        got = ctypes.c_int()
+        check(lib.smmp_ens_set_window(self._h, int(k), ctypes.byref(got)))
+        return got.value
+
+    def window(self):
+        """(window in use, autotuner's one-sweep times with windows 2, 4, 8)."""
+        k = ctypes.c_int()
+        ms = (ctypes.c_double * 3)()
+        check(lib.smmp_ens_window(self._h, ctypes.byref(k), ms))
+        return k.value, (ms[0], ms[1], ms[2])
+
+    def set_pair_work(self, form):
+        """Pair-work form by hand: one of AUTOTUNE_FORMS (or its index)."""
+        k = self.AUTOTUNE_FORMS.index(form) if isinstance(form, str) else int(form)
+        check(lib.smmp_ens_set_pair_work(self._h, k))
+
     def da_stats(self):
         """(stage-1 passes, stage-2 accepts) per chain."""
         a = np.zeros(self.nchains, dtype=np.uint64)

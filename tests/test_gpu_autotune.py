@@ -1,5 +1,6 @@
 """The autotuner: it times the pair-work decompositions (chunk lists, rows,
-rows for molecules of 128+ atoms) from a saved state, keeps the fastest, and
+rows for molecules of 128+ atoms, rows with speculative windows of 2, 4 and 8
+proposals) from a saved state, keeps the fastest, and
 leaves the ensemble's state (variables, energies, random streams, counters)
 exactly as it found it."""
 import numpy as np
@@ -29,7 +30,11 @@ def test_autotune_leaves_no_trace_and_keeps_parity(tmp_path, n):
     a1, p1 = ens.acceptance()
     assert np.array_equal(a0, a1) and np.array_equal(p0, p1)
     assert min(ms) > 0
-    assert form == Ensemble.AUTOTUNE_FORMS[int(np.argmin(ms))]
+    win, wms = ens.window()
+    if win > 1:   # a speculative window on the row form beat every one-at-a-time form
+        assert form == "rows" and wms[(2, 4, 8).index(win)] <= min(ms)
+    else:
+        assert form == Ensemble.AUTOTUNE_FORMS[int(np.argmin(ms))]
     # the random streams were restored: the next draws equal the twin's
     assert np.array_equal(ens.draw(3, 50), twin.draw(3, 50))
     ens.sweeps(5)

@@ -9,8 +9,8 @@ valence angles and the dihedral state the variable file leaves; the variables
 lists pair for pair, normal and 1-4 separately, each under the same listing
 atom as mklist.f; and both lists against brute force: turning each variable
 alone on the oracle's own rebuild, a pair whose distance some variable
-changes is an interaction pair, and it is a 1-4 pair exactly when one
-variable changes it.
+changes is an interaction pair, and every 1-4 pair is one that exactly one
+variable changes.
 """
 import numpy as np
 import pytest
