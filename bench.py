@@ -6,10 +6,14 @@ free dihedrals), ECEPP/3 in vacuum, temperatures geometric 100-1000 K,
 neighbour exchange after every sweep, seeded uniform random start.  Inputs are
 synthetic (seeded random starts of the reference's own Met-enkephalin deck).
 
-A step is one CUDA-graph launch of 16 parallel-tempering sweeps (each: one
+A step is one cooperative launch of 16 parallel-tempering rounds (each: one
 sweep of every replica, then one exchange).  value = replica sweeps per second
 of the whole job.  Every step is timed with CUDA events on the stream the
-kernels run on; L2 is flushed (a 256 MiB write) between steps.
+kernels run on; L2 is flushed (a 256 MiB write) between steps.  e2e times the
+same steps from the same starting state through the C ABI with the state
+copied from and to pinned host memory every step.  The default run also
+measures the other two configurations with a few steps each
+(other_workloads).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload pt_enkefa64|polyala256|protein60_pt128]
@@ -22,10 +26,13 @@ from the natural amino-acid composition (926 atoms, 365 dihedrals) with SASA,
 
 --impl reference times the reference's algorithm on the host cores: the CPU
 oracle (a C++ restatement of the Fortran, which no Fortran compiler here can
-build) running the same chains with all host threads.
+build), compiled for the host's CPU (-O2 -march=native), running the same
+chains, temperatures and exchanges with all host threads; its chains persist
+from step to step.
 """
 import argparse
 import ctypes
+import hashlib
 import json
 import os
 import statistics
@@ -209,78 +216,132 @@ class Clocks:
 
 
 # ------------------------------------------------------------------ CPU baseline
-def oracle_lib():
-    if not os.path.exists(ORACLE_SO):
-        subprocess.check_call(["make", "-C", os.path.join(ROOT, "oracle")],
-                              stdout=subprocess.DEVNULL)
-    L = ctypes.CDLL(ORACLE_SO)
+def _cpu_model():
+    model, flags = "", ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if not model and line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                if not flags and line.startswith("flags"):
+                    flags = line.split(":", 1)[1].strip()
+                if model and flags:
+                    break
+    except OSError:
+        pass
+    return model, hashlib.sha1((model + "|" + flags).encode()).hexdigest()[:12]
+
+
+def oracle_lib(native=False):
+    """The CPU oracle as a library: the checker build (oracle/liboracle_smmp.so)
+    or, for timing, a build for this host's own CPU (-O2 -march=native, made
+    on first use under oracle/_native/<cpu>/; still no contraction and no
+    fast-math, so its arithmetic is the checker's)."""
+    if native:
+        _, key = _cpu_model()
+        d = os.path.join(ROOT, "oracle", "_native", key)
+        path = os.path.join(d, "liboracle_smmp.so")
+        if not os.path.exists(path):
+            os.makedirs(d, exist_ok=True)
+            odir = os.path.join(ROOT, "oracle")
+            srcs = sorted(os.path.join(odir, f) for f in os.listdir(odir) if f.endswith(".cpp"))
+            tmp = path + ".%d" % os.getpid()
+            subprocess.check_call([os.environ.get("CXX", "g++"), "-O2", "-march=native",
+                                   "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math",
+                                   "-shared", "-o", tmp] + srcs + ["-lpthread"])
+            os.replace(tmp, path)
+    else:
+        path = ORACLE_SO
+        if not os.path.exists(path):
+            subprocess.check_call(["make", "-C", os.path.join(ROOT, "oracle")],
+                                  stdout=subprocess.DEVNULL)
+    L = ctypes.CDLL(path)
     L.orc_create.restype = ctypes.c_void_p
     L.orc_create.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
-    L.orc_bench_chains.restype = ctypes.c_double
-    L.orc_bench_chains.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
-                                   ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_int,
-                                   ctypes.POINTER(ctypes.c_double)]
+    L.orc_init_molecule.argtypes = [ctypes.c_void_p] + [ctypes.c_char_p] * 4
+    L.orc_pt_create.restype = ctypes.c_void_p
+    L.orc_pt_create.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int,
+                                ctypes.c_int, ctypes.c_int]
+    L.orc_pt_run.restype = ctypes.c_double
+    L.orc_pt_run.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.orc_pt_free.argtypes = [ctypes.c_void_p]
+    L.orc_last_error.restype = ctypes.c_char_p
     return L
 
 
-class OracleChains:
-    """The reference algorithm (CPU oracle, FP64) on the workload's chains,
-    every host thread busy: one handle per distinct molecule, seeded random
-    start."""
+class CpuChains:
+    """The reference algorithm (the CPU oracle, FP64) on the workload's chains
+    with every host thread busy: one persistent ensemble per distinct
+    molecule, each chain with its own stream and random start, parallel
+    tempering workloads exchanging after every round as the GPU arm does.
+    Successive samples continue the trajectories.  A workload of several
+    molecules keeps `cores` chains of each and weights each molecule's
+    per-chain-sweep cost by its number of chains in the workload."""
 
-    def __init__(self, wl, files):
-        self.L = oracle_lib()
+    def __init__(self, wl, files, native=True):
+        self.L = oracle_lib(native)
         self.cores = os.cpu_count() or 1
-        self.handles = []
-        for seq, var in files:
+        self.cpu = _cpu_model()[0]
+        self.build = "-O2 -march=native" if native else "-O2"
+        self.cm = wl.chain_mol()
+        temps = wl.temperatures()
+        self.nch = len(self.cm)
+        self.objs = []
+        for m, (seq, var) in enumerate(files):
             h = ctypes.c_void_p(self.L.orc_create(DATA.encode(), 0, 0, wl.itysol))
             rc = self.L.orc_init_molecule(h, seq.encode(), (var or " ").encode(), b"nh2", b"cooh")
-            assert rc == 0
-            self.L.orc_sgrnd(h, ctypes.c_int(31433))
-            self.L.orc_random_start(h)
-            self.handles.append(h)
-        self.cm = wl.chain_mol()
-        self.temps = wl.temperatures()
+            assert rc == 0, self.L.orc_last_error()
+            chains = [c for c in range(self.nch) if self.cm[c] == m]
+            if len(files) > 1:
+                chains = (chains * (1 + self.cores // len(chains)))[:self.cores]
+            n = len(chains)
+            betas = (ctypes.c_double * n)(*[1.0 / (temps[c] * GAS) for c in chains])
+            seeds = (ctypes.c_int * n)(*[31433 + 1000 * c + 7 * k for k, c in enumerate(chains)])
+            pt = self.L.orc_pt_create(h, n, betas, seeds, 4711, 0, self.cores, 1 if wl.pt else 0)
+            assert pt, self.L.orc_last_error()
+            self.objs.append((h, ctypes.c_void_p(pt), n, self.cm.count(m)))
 
-    def run(self, mol, nchains, nsweeps):
-        """Seconds for nchains chains of molecule `mol` x nsweeps on all threads."""
-        chains = [c for c, m in enumerate(self.cm) if m == mol]
-        chains = (chains * (1 + nchains // max(1, len(chains))))[:nchains]
-        seeds = (ctypes.c_int * nchains)(*[31433 + 1000 * c for c in chains])
-        betas = (ctypes.c_double * nchains)(*[1.0 / (self.temps[c] * GAS) for c in chains])
-        out = (ctypes.c_double * nchains)()
-        return self.L.orc_bench_chains(self.handles[mol], nchains, seeds, betas, nsweeps,
-                                       self.cores, out)
+    def rounds(self, m, n):
+        t = self.L.orc_pt_run(self.objs[m][1], int(n))
+        if t < 0:
+            raise RuntimeError(self.L.orc_last_error().decode())
+        return t
 
     def sample(self, target_seconds):
-        """(chain sweeps per second, description, seconds) from one bounded
-        sample.  One molecule: all chains for as many sweeps as fit
-        target_seconds.  Several: for each molecule, `cores` chains (every
-        thread busy) for one sweep; each molecule's per-chain-sweep cost is
-        weighted by its number of chains in the workload."""
-        n = len(self.handles)
-        nchains = len(self.cm)
-        if n == 1:
-            probe = self.run(0, min(self.cores, nchains), 1)
-            per_round = probe * max(1, nchains // self.cores)
-            nsw = max(1, int(target_seconds / max(per_round, 1e-6)))
-            t = self.run(0, nchains, nsw)
-            return nchains * nsw / t, "%d chains x %d sweeps, %.1f s" % (nchains, nsw, t), t
-        cost = 0.0
-        total = 0.0
-        for m in range(n):
-            t = self.run(m, self.cores, 1)
+        """(chain sweeps per second, description, seconds): one warm-up round,
+        then as many rounds as fit target_seconds (one molecule), or one
+        round of each molecule (several)."""
+        if len(self.objs) == 1:
+            probe = self.rounds(0, 1)
+            if probe > 0.25 * target_seconds:   # a large molecule: the probe is the sample
+                return self.nch / probe, "%d chains x 1 round, %.1f s" % (self.nch, probe), probe
+            nr = max(1, int(target_seconds / max(probe, 1e-6)))
+            t = self.rounds(0, nr)
+            return self.nch * nr / t, "%d chains x %d rounds, %.1f s" % (self.nch, nr, t), t
+        cost = total = 0.0
+        for m, (_, _, n, count) in enumerate(self.objs):
+            self.rounds(m, 1)
+            t = self.rounds(m, 1)
             total += t
-            cost += self.cm.count(m) * t / self.cores
-        return nchains / cost, ("%d chains x 1 sweep of each of %d molecules, weighted by the "
-                                "workload's chain counts, %.1f s" % (self.cores, n, total)), total
+            cost += count * t / n
+        return self.nch / cost, ("%d chains of each of %d molecules x 1 round, weighted by the "
+                                 "workload's chain counts, %.1f s" % (self.cores, len(self.objs),
+                                                                      total)), total
+
+    def close(self):
+        for h, pt, _, _ in self.objs:
+            self.L.orc_pt_free(pt)
+        self.objs = []
 
 
-def cpu_baseline(wl, files, target_seconds=15.0):
-    oc = OracleChains(wl, files)
+def cpu_baseline(wl, files, target_seconds=12.0):
+    oc = CpuChains(wl, files)
     value, sample, _ = oc.sample(target_seconds)
+    oc.close()
     return {"value": value, "unit": "sweeps/s", "cores": oc.cores, "kind": "port",
-            "sample": sample + " (no exchanges)"}
+            "cpu": oc.cpu, "build": oc.build,
+            "sample": sample + ("" if not wl.pt else " with an exchange after every round")}
 
 
 def max_over_ranks(values, world, device=None):
@@ -300,30 +361,69 @@ def job_rate(units_per_rank, world, ms):
 
 
 # ------------------------------------------------------------------ our arm
-def run_ours(args, rank, world):
+def fp32_peak_tflops():
+    """FP32 FMA issue peak of the device (148 SMs x 128 lanes x 2 flops at
+    the measured maximum SM clock; no measured FP32 peak exists)."""
+    mhz = 1965.0
+    if os.path.exists(PEAKS):
+        try:
+            mhz = float(json.load(open(PEAKS)).get("sm_max_mhz", mhz))
+        except Exception:
+            pass
+    return 148 * 128 * 2 * mhz * 1e6 / 1e12
+
+
+def max_dE_vs_oracle(ens, files, wl, mols, nsample=16):
+    """Largest |E_GPU - E_FP64 oracle| (kcal/mol) over a sample of chains:
+    the GPU's tracked energy of each chain's current conformation against the
+    oracle's FP64 energy() of the same variables."""
+    L = oracle_lib(False)
+    L.orc_energy.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                             ctypes.POINTER(ctypes.c_double)]
+    L.orc_set_vlvr.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+    L.orc_destroy.argtypes = [ctypes.c_void_p]
+    cm = wl.chain_mol()
+    V, E = ens.vlvr(), ens.energies()
+    handles = {}
+    worst = 0.0
+    picks = sorted(set(int(round(x)) for x in
+                       [k * (len(cm) - 1) / max(1, nsample - 1) for k in range(nsample)]))
+    for c in picks:
+        m = cm[c]
+        if m not in handles:
+            h = ctypes.c_void_p(L.orc_create(DATA.encode(), 0, 0, wl.itysol))
+            seq, var = files[m]
+            assert L.orc_init_molecule(h, seq.encode(), (var or " ").encode(), b"nh2",
+                                       b"cooh") == 0
+            handles[m] = h
+        v = (ctypes.c_double * mols[m].nvar)(*V[c, :mols[m].nvar])
+        L.orc_set_vlvr(handles[m], v)
+        e, t = ctypes.c_double(), (ctypes.c_double * 6)()
+        assert L.orc_energy(handles[m], ctypes.byref(e), t) == 0
+        worst = max(worst, abs(E[c] - e.value))
+    for h in handles.values():
+        L.orc_destroy(h)
+    return worst, len(picks)
+
+
+def measure(wl, args, rank, world, dev, stream, flush, steps, warmup, headline):
+    """Our arm on one workload: the device-timed region (steps x one step of
+    spp sweeps, L2 flushed before each), the kernel's own launches, the same
+    steps end to end through the C ABI from the same starting state, and the
+    checks and rooflines that explain them."""
     import torch
     from smmp.ensemble import Ensemble, Molecule
-
-    wl = WORKLOADS[args.workload]()
     spp = wl.sweeps_per_step
-    dev = int(os.environ.get("LOCAL_RANK", 0))
-    torch.cuda.set_device(dev)
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     files = wl.molecule_files()
     mols = [Molecule(seq, var, libdir=DATA, itysol=wl.itysol) for seq, var in files]
     cm = wl.chain_mol()
     nch = len(cm)
     betas = [1.0 / (t * GAS) for t in wl.temperatures()]
     ens = Ensemble(mols, cm, wl.seeds(rank), betas, fp32=True)
-    stream = torch.cuda.Stream()
     ens.set_stream(stream.cuda_stream)
     ens.random_start()
     if wl.pt:
         ens.set_pt(betas, wrap=False, exchange_seed=4711 + rank)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     def step():
         if wl.pt:
@@ -337,18 +437,24 @@ def run_ours(args, rank, world):
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step()
-    # the autotuner picks the pair-work decomposition (state left unchanged)
+    # the autotuner picks the pair-work decomposition and the speculative
+    # window (state left unchanged)
     form, (ms_lists, ms_rows, ms_size) = ens.autotune()
-    tuned = {"pair_work": form, "sweep_ms_lists": ms_lists, "sweep_ms_rows": ms_rows,
-             "sweep_ms_rows_128plus": ms_size}
+    win, (w2, w4, w8) = ens.window()
+    tuned = {"pair_work": form, "window": win, "sweep_ms_lists": ms_lists,
+             "sweep_ms_rows": ms_rows, "sweep_ms_rows_128plus": ms_size,
+             "sweep_ms_rows_window2": w2, "sweep_ms_rows_window4": w4,
+             "sweep_ms_rows_window8": w8}
+    start = ens.checkpoint()
     # ---- device-timed region: K steps, each bracketed by events on the stream
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    pt0 = int(ens.pair_terms().sum())
     barrier()
     with Clocks(dev) as clk:
-        for k in range(args.steps):
+        for k in range(steps):
             with torch.cuda.stream(stream):
                 flush.zero_()
                 starts[k].record(stream)
@@ -356,11 +462,14 @@ def run_ours(args, rank, world):
             ends[k].record(stream)
         barrier()
     ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
-    # batched PT runs each step as one cooperative launch of spp (sweep,
-    # exchange) rounds when every chain is resident at once
+    pterms = int(ens.pair_terms().sum()) - pt0
     fused = bool(wl.pt and ens.pt_fused_last())
-    # ---- roofline: the sweep kernel alone, one launch per sweep, event-timed
-    n_roof = 50 if wl.name == "pt_enkefa64" else 8
+    errors = ens.errors()
+    if errors.any():
+        raise SystemExit("kernel error words: %s" % errors.tolist())
+    dE, nde = max_dE_vs_oracle(ens, files, wl, mols)
+    # ---- the sweep kernel alone, one launch per sweep, event-timed
+    n_roof = 50 if headline else 4
     rs = [torch.cuda.Event(enable_timing=True) for _ in range(n_roof)]
     re_ = [torch.cuda.Event(enable_timing=True) for _ in range(n_roof)]
     for k in range(n_roof):
@@ -371,15 +480,16 @@ def run_ours(args, rank, world):
         re_[k].record(stream)
     torch.cuda.synchronize()
     sweep_kernel_ms = statistics.mean(a.elapsed_time(b) for a, b in zip(rs, re_))
-    # ---- end-to-end through the C ABI with host buffers every step
+    # ---- end to end through the C ABI with host buffers every step, the same
+    # steps from the same starting state as the timed region
+    ens.restore(start)
     vl = torch.empty((nch, ens.vstride), dtype=torch.float64, pin_memory=True).numpy()
     vl[:] = ens.vlvr()
-    e2e_steps = max(10, args.steps // 4) if wl.name == "pt_enkefa64" else max(3, args.steps // 4)
     barrier()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     t0.record(stream)
-    for _ in range(e2e_steps):
+    for _ in range(steps):
         ens.set_vlvr(vl)                                   # H2D of the step's state
         step()
         ens.energies()                                     # D2H of the result
@@ -387,21 +497,17 @@ def run_ours(args, rank, world):
     t1.record(stream)
     barrier()
     e2e_ms = t0.elapsed_time(t1)
-    errors = ens.errors()
-    if errors.any():
-        raise SystemExit("kernel error words: %s" % errors.tolist())
-
-    # max over ranks
+    if ens.errors().any():
+        raise SystemExit("kernel error words: %s" % ens.errors().tolist())
     ms, e2e_ms, sweep_kernel_ms = max_over_ranks([ms, e2e_ms, sweep_kernel_ms], world, "cuda")
-    value = job_rate(nch * spp * args.steps, world, ms)
-    e2e_value = job_rate(nch * spp * e2e_steps, world, e2e_ms)
-
-    # roofline: algorithmic HBM bytes per launch of the sweep kernel
-    # (16 B coordinates per atom + 8 B per dihedral + 8 B energy, per
-    # evaluation; one evaluation per free dihedral per sweep; every chain)
+    value = job_rate(nch * spp * steps, world, ms)
+    e2e_value = job_rate(nch * spp * steps, world, e2e_ms)
+    # HBM roofline (north_star's figure): algorithmic bytes per launch of the
+    # sweep kernel (16 B coordinates per atom + 8 B per dihedral + 8 B energy,
+    # per evaluation; one evaluation per free dihedral per sweep; every chain)
     bytes_per_sweep = sum(mols[m].nvr * (16 * mols[m].natoms + 8 * mols[m].nvr + 8) for m in cm)
     if fused:   # the timed step is that one launch (and an 8-byte memset)
-        roof_kernel, roof_ms, bytes_per_launch = "k_sweep<true> (fused PT)", ms / args.steps, \
+        roof_kernel, roof_ms, bytes_per_launch = "k_sweep<true> (fused PT)", ms / steps, \
             bytes_per_sweep * spp
     else:
         roof_kernel, roof_ms, bytes_per_launch = "k_sweep<true>", sweep_kernel_ms, bytes_per_sweep
@@ -415,38 +521,83 @@ def run_ours(args, rank, world):
             pass
     traffic = None
     tf = os.path.join(ROOT, "profiles", "k_sweep_traffic.json")
-    if wl.name == "pt_enkefa64" and os.path.exists(tf):
+    if headline and os.path.exists(tf):
         try:
             traffic = json.load(open(tf)).get("fused_bytes_per_launch" if fused
                                               else "bytes_per_launch")
         except Exception:
             traffic = None
-    line = {
-        "metric": METRIC, "value": value, "unit": "sweeps/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32 pair terms / f64 rebuild+acceptance",
-        "data": ("synthetic (seeded random starts of the reference's Met-enkephalin deck)"
-                 if wl.name == "pt_enkefa64"
-                 else "synthetic (seeded sequences, seeded random starts)"),
+    # FP32 issue roofline (the pair terms the sweeps evaluated, 30 flops each)
+    tflops = pterms * 30.0 / (ms / 1000.0) / 1e12
+    fpeak = fp32_peak_tflops()
+    return {
+        "value": value, "unit": "sweeps/s", "ms_per_step": ms / steps,
         "config": config(wl, {"autotune": tuned}),
         "e2e": {"value": e2e_value, "unit": "sweeps/s",
                 "h2d_bytes_per_step": int(vl.nbytes),
                 "d2h_bytes_per_step": int(vl.nbytes + 8 * nch)},
-        "gpu_launches": args.steps * (1 if fused or not wl.pt else spp * 2),
+        "gpu_launches": steps * (1 if fused or not wl.pt else spp * 2),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_source": peak_src, "kernel": roof_kernel,
                      "kernel_ms_per_launch": roof_ms,
                      "bytes_per_launch": bytes_per_launch,
                      "single_sweep_launch_ms": sweep_kernel_ms},
-        "clocks": clk.summary(),
+        "roofline_fp32_issue": {"achieved": tflops, "peak": fpeak, "unit": "TFLOP/s",
+                                "frac": tflops / fpeak,
+                                "pair_terms_per_sweep": pterms / float(nch * spp * steps),
+                                "flops_per_pair_term": 30,
+                                "peak_source": "computed (148 SMs x 128 FP32 lanes x 2 x "
+                                               "measured max SM clock)"},
+        "max_abs_dE_vs_fp64_oracle_kcal": dE, "dE_sample_chains": nde,
+        "clocks": clk.summary(), "_ens": ens, "_mols": mols, "_files": files,
+        "_betas": betas,
     }
-    if wl.name == "pt_enkefa64" and not args.no_surrogate:
-        line["plain_single_replica"] = single_replica(mols[0], spp, stream)
-        line["surrogate"] = surrogate_leg(ens, mols[0], betas, spp, stream, flush)
+
+
+def run_ours(args, rank, world):
+    import torch
+    wl = WORKLOADS[args.workload]()
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    stream = torch.cuda.Stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    headline = wl.name == "pt_enkefa64"
+    r = measure(wl, args, rank, world, dev, stream, flush, args.steps, args.warmup, headline)
+    ens, mols, files, betas = r.pop("_ens"), r.pop("_mols"), r.pop("_files"), r.pop("_betas")
+    line = {
+        "metric": METRIC, "value": r["value"], "unit": "sweeps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 pair terms / f64 rebuild+acceptance",
+        "data": ("synthetic (seeded random starts of the reference's Met-enkephalin deck)"
+                 if headline else "synthetic (seeded sequences, seeded random starts)"),
+    }
+    line.update({k: v for k, v in r.items() if k not in line})
+    if headline and not args.no_surrogate:
+        line["plain_single_replica"] = single_replica(mols[0], wl.sweeps_per_step, stream)
+        line["surrogate"] = surrogate_leg(ens, mols[0], betas, wl.sweeps_per_step, stream, flush)
+    del ens
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(wl, files)
+    if headline and world == 1 and not args.no_extra:
+        # the other configurations, bounded: measured with the same rules
+        others = {}
+        for name in ("polyala256", "protein60_pt128"):
+            w2 = WORKLOADS[name]()
+            r2 = measure(w2, args, rank, world, dev, stream, flush, 3, 2, False)
+            for k in ("_ens", "_mols", "_betas"):
+                r2.pop(k)
+            f2 = r2.pop("_files")
+            if not args.no_cpu:
+                r2["cpu_baseline"] = cpu_baseline(w2, f2, target_seconds=8.0)
+                r2["e2e_vs_cpu"] = r2["e2e"]["value"] / r2["cpu_baseline"]["value"]
+            others[name] = r2
+        line["other_workloads"] = others
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
@@ -561,41 +712,45 @@ def surrogate_leg(ens, mol, betas, spp, stream, flush):
 
 
 def run_reference(args, rank, world):
+    """The reference algorithm on the host cores (the CPU oracle, FP64, built
+    for this CPU), on our arm's workload: the same chains, temperatures and
+    exchange schedule, every host thread busy.  A step is a bounded sample:
+    20 rounds of all 64 replicas for Met-enkephalin, one sample of
+    CpuChains otherwise.  The chains persist from step to step."""
     if rank != 0:
         return
     wl = WORKLOADS[args.workload]()
     files = wl.molecule_files()
-    oc = OracleChains(wl, files)
+    oc = CpuChains(wl, files)
     nch = len(wl.chain_mol())
     enk = wl.name == "pt_enkefa64"
-    # each step: a bounded sample of the workload (every replica 20 sweeps for
-    # Met-enkephalin; the per-molecule sample of OracleChains otherwise)
+    per = 20
     for _ in range(args.warmup if enk else 0):
-        oc.run(0, nch, 1)
-    total = 0.0
-    units = 0.0
+        oc.rounds(0, 1)
+    total = units = 0.0
     sample = ""
     for _ in range(args.steps):
         if enk:
-            per = 20
-            total += oc.run(0, nch, per)
+            total += oc.rounds(0, per)
             units += nch * per
-            sample = "%d replicas x %d sweeps per step, %d steps" % (nch, per, args.steps)
+            sample = ("%d replicas x %d rounds (sweep + exchange) per step, %d steps"
+                      % (nch, per, args.steps))
         else:
             rate, sample, t = oc.sample(5.0)
             total += t
             units += rate * t
+    oc.close()
     value = units / total
     extra = {"pair_precision": "fp64 (reference arithmetic)"}
     if enk:
-        extra["sweeps_per_step"] = 20
+        extra["sweeps_per_step"] = per
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "sweeps/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total * 1000.0 / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config(wl, extra),
         "cpu_baseline": {"value": value, "unit": "sweeps/s", "cores": oc.cores, "kind": "port",
-                         "sample": sample},
+                         "cpu": oc.cpu, "build": oc.build, "sample": sample},
         "e2e": {"value": value, "unit": "sweeps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0}}), flush=True)
 
@@ -610,6 +765,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-surrogate", action="store_true",
                     help="skip the surrogate training / delayed-acceptance leg")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the bounded legs of the other workloads")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", 0))

@@ -238,6 +238,16 @@ int smmp_ens_pt_sweeps(smmp_ens_t* e, int nsweeps, int serial, int graph_chunk);
 int smmp_ens_set_pt_fused(smmp_ens_t* e, int on, double timeout_s, int barrier_extra);
 int smmp_ens_pt_fused_last(smmp_ens_t* e, int* fused);   /* 1: last run was fused */
 int smmp_ens_pt_map(smmp_ens_t* e, int* temp_chain);   /* ipoi, 0-based chains */
+/* Exchange statistics since smmp_ens_set_pt: stats[2k] attempts and
+ * stats[2k+1] accepted exchanges of the label pair (k, k+1) (k = n-1: the
+ * periodic pair (n-1, 0)); partem_s.f:210-232. */
+int smmp_ens_pt_stats(smmp_ens_t* e, uint64_t* stats);
+/* Pair terms the sweeps of each chain have evaluated (no counterpart in the
+ * reference, which sums every pair at every energy() call): full sums at the
+ * sweep's opening and closing evaluations and re-sums, every pair of a
+ * proposal summed in full, and twice the pairs across a proposal's bond in
+ * the incremental mode.  Delayed-acceptance sweeps are not counted. */
+int smmp_ens_pair_terms(smmp_ens_t* e, uint64_t* terms);
 int smmp_ens_sizes(smmp_ens_t* e, int* nchains, int* vstride, int* tstride);
 int smmp_ens_get_energies(smmp_ens_t* e, double* eol);          /* [nchains] */
 int smmp_ens_get_terms(smmp_ens_t* e, double* terms);           /* [nchains*6] */

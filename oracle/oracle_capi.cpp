@@ -8,6 +8,9 @@
 #include <stdexcept>
 #include <string>
 #include <thread>
+#include <atomic>
+#include <condition_variable>
+#include <mutex>
 #include <vector>
 
 #include "smmp_oracle.hpp"
@@ -363,6 +366,189 @@ int orc_partem(void* h, int num_rep, const double* betas, int nequi, int nswp, d
       ipoi_out[k - 1] = ipoi[k];
       for (int i = 0; i < nvr; ++i) vl_out[(size_t)(k - 1) * nvr + i] = coor[(size_t)(k - 1) * nvr + i];
     }
+  });
+}
+
+}  // extern "C"
+
+namespace {
+
+// A reusable barrier for the chain threads of one PT ensemble.
+class RoundBarrier {
+ public:
+  explicit RoundBarrier(int n) : n_(n) {}
+  void wait() {
+    std::unique_lock<std::mutex> lk(m_);
+    const unsigned gen = gen_;
+    if (++count_ == n_) {
+      count_ = 0;
+      ++gen_;
+      cv_.notify_all();
+    } else {
+      cv_.wait(lk, [&] { return gen_ != gen; });
+    }
+  }
+
+ private:
+  std::mutex m_;
+  std::condition_variable cv_;
+  int n_, count_ = 0;
+  unsigned gen_ = 0;
+};
+
+// Batched parallel tempering as the product's batched mode defines it (no
+// counterpart routine in the reference; its exchange step is partem_s.f:
+// 210-232): chain c is a copy of the system with its own stream
+// sgrnd(seeds[c]) and a canonical random start (canon.f:60-67); a round is
+// one metropolis sweep of every chain at the inverse temperature of its
+// label, then one exchange step over the labels with alternating parity,
+// drawing from a separate stream sgrnd(exchange_seed) once per pair in pair
+// order, the periodic pair (n, 1) only when wrap.  Chains sweep on nthreads
+// host threads (they share nothing); the state persists between calls.
+struct BatchedPT {
+  std::vector<std::unique_ptr<Smmp>> ch;
+  std::unique_ptr<Smmp> ex;
+  std::vector<double> betas, eol, acz;
+  std::vector<int> ipoi;   // chain (0-based) at label k (1-based)
+  std::vector<unsigned long long> stats;
+  int n = 0, wrap = 0, iswitch = 1, nthreads = 1, exchanges = 1;
+
+  void exchange() {
+    if (n < 2 || !exchanges) return;
+    int num_rep1, nu;
+    if (iswitch == 1) {
+      num_rep1 = n - 1;
+      nu = 1;
+      iswitch = 2;
+    } else {
+      num_rep1 = n;
+      nu = 2;
+      iswitch = 1;
+    }
+    for (int i = nu; i <= num_rep1; i += 2) {
+      if (i == n && !wrap) continue;
+      const int j = (i == n) ? 1 : i + 1;
+      const int in = ipoi[i], jn = ipoi[j];
+      const double bi = betas[i - 1], bj = betas[j - 1];
+      const double delta = -bi * eol[jn] - bj * eol[in] + bi * eol[in] + bj * eol[jn];
+      const double ra = ex->grnd();
+      stats[2 * (i - 1)] += 1;
+      if (ra <= std::exp(delta)) {
+        ipoi[i] = jn;
+        ipoi[j] = in;
+        stats[2 * (i - 1) + 1] += 1;
+      }
+    }
+  }
+
+  // nrounds rounds; after each, `each(r)` on the calling thread's side.
+  template <class F>
+  void run(int nrounds, F each) {
+    const int nt = std::max(1, std::min(nthreads, n));
+    RoundBarrier bar(nt + 1);
+    std::vector<std::string> errs(nt);
+    std::atomic<bool> stop{false};
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; ++t)
+      th.emplace_back([&, t] {
+        Smmp::Weight w;
+        for (int r = 0; r < nrounds; ++r) {
+          bar.wait();   // betas set
+          if (!stop)
+            try {
+              for (int c = t; c < n; c += nt) ch[c]->metropolis(eol[c], acz[c], w);
+            } catch (const std::exception& e) {
+              errs[t] = e.what();
+              stop = true;
+            }
+          bar.wait();   // sweeps done
+        }
+      });
+    std::string err;
+    for (int r = 0; r < nrounds; ++r) {
+      for (int k = 1; k <= n; ++k) ch[ipoi[k]]->beta = betas[k - 1];
+      bar.wait();
+      bar.wait();
+      for (auto& e : errs)
+        if (!e.empty() && err.empty()) err = e;
+      if (!err.empty()) continue;
+      exchange();
+      each(r);
+    }
+    for (auto& x : th) x.join();
+    if (!err.empty()) throw std::runtime_error(err);
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+// exchange = 0: independent canonical chains (rounds are sweeps only).
+void* orc_pt_create(void* h, int n, const double* betas, const int* seeds, int exchange_seed,
+                    int wrap, int nthreads, int exchange) {
+  try {
+    auto* p = new BatchedPT;
+    p->exchanges = exchange;
+    p->n = n;
+    p->wrap = wrap;
+    p->nthreads = nthreads;
+    for (int c = 0; c < n; ++c) {
+      p->ch.emplace_back(new Smmp(*S(h)));
+      p->ch[c]->sgrnd(seeds[c]);
+      orc_random_start(p->ch[c].get());
+    }
+    p->ex.reset(new Smmp(*S(h)));
+    p->ex->sgrnd(exchange_seed);
+    p->betas.assign(betas, betas + n);
+    p->eol.assign(n, 0.0);
+    p->acz.assign(n, 0.0);
+    p->ipoi.assign(n + 1, 0);
+    for (int k = 1; k <= n; ++k) p->ipoi[k] = k - 1;
+    p->stats.assign(2 * n, 0);
+    return p;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return nullptr;
+  }
+}
+void orc_pt_free(void* p) { delete static_cast<BatchedPT*>(p); }
+
+// nrounds rounds of a batched PT ensemble; returns the wall time in seconds
+// (negative on error: orc_last_error).
+double orc_pt_run(void* p, int nrounds) {
+  auto* pt = static_cast<BatchedPT*>(p);
+  try {
+    auto t0 = std::chrono::steady_clock::now();
+    pt->run(nrounds, [](int) {});
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1.0;
+  }
+}
+
+// Per round r (0-based) of a fresh batched PT run: tc_hist[r*n+k] = chain at
+// label k (0-based) after the exchange, eol_hist[r*n+c] = energy of chain c,
+// vl_hist[(r*n+c)*nvr+i] = its free variables; stats[2k] / [2k+1] =
+// attempts / accepts of label pair (k, k+1).
+int orc_partem_batched(void* h, int n, const double* betas, const int* seeds, int exchange_seed,
+                       int wrap, int nrounds, int nthreads, int* tc_hist, double* eol_hist,
+                       double* vl_hist, unsigned long long* stats) {
+  return guard([&] {
+    std::unique_ptr<BatchedPT> pt(
+        static_cast<BatchedPT*>(orc_pt_create(h, n, betas, seeds, exchange_seed, wrap, nthreads, 1)));
+    if (!pt) throw std::runtime_error(g_err);
+    const int nvr = S(h)->nvr;
+    pt->run(nrounds, [&](int r) {
+      for (int k = 1; k <= n; ++k) tc_hist[(size_t)r * n + (k - 1)] = pt->ipoi[k];
+      for (int c = 0; c < n; ++c) {
+        eol_hist[(size_t)r * n + c] = pt->eol[c];
+        for (int i = 1; i <= nvr; ++i)
+          vl_hist[((size_t)r * n + c) * nvr + (i - 1)] = pt->ch[c]->vlvr[pt->ch[c]->idvr[i]];
+      }
+    });
+    for (int k = 0; k < 2 * n; ++k) stats[k] = pt->stats[k];
   });
 }
 

@@ -878,6 +878,24 @@ int smmp_ens_pt_map(smmp_ens_t* e, int* temp_chain) {
   });
 }
 
+int smmp_ens_pair_terms(smmp_ens_t* e, uint64_t* terms) {
+  return guard([&] {
+    need(e && terms, "NULL argument");
+    std::vector<unsigned long long> p;
+    e->e->get_pair_terms(p);
+    std::copy(p.begin(), p.end(), terms);
+  });
+}
+
+int smmp_ens_pt_stats(smmp_ens_t* e, uint64_t* stats) {
+  return guard([&] {
+    need(e && stats && e->e->has_pt(), "bad arguments");
+    std::vector<unsigned long long> st;
+    e->e->pt_stats(st);
+    std::copy(st.begin(), st.end(), stats);
+  });
+}
+
 int smmp_ens_sizes(smmp_ens_t* e, int* nchains, int* vstride, int* tstride) {
   return guard([&] {
     need(e != nullptr, "NULL ensemble");

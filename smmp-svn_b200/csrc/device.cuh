@@ -58,6 +58,8 @@ struct DMol {
   const unsigned long long* near_mask;   // row form of the pair set (rows != 0)
   const unsigned long long* near14;
   int rows;
+  int npairs;                            // pair terms of a full evaluation
+  const int* var_cross;                  // pair terms across each variable's bond
 };
 
 // Force field constants read by every chain (copied to shared memory).
@@ -133,6 +135,7 @@ struct DChains {
   double* terms;         // [chain*6]: eyel eyvw eyhb eyvr eysl eysm (last full evaluation)
   unsigned long long* nacc;
   unsigned long long* nprop;
+  unsigned long long* pterms;   // pair terms evaluated by the sweeps (FP32-issue roofline)
   int* err;              // first error of each chain (0 = none)
   double* coords;        // optional [chain * 3 * tstride] coordinates after the call
   // delayed acceptance (surrogate first stage), on when sur.w1 != nullptr

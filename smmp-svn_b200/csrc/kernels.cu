@@ -1589,7 +1589,8 @@ template <bool F32>
 __device__ __noinline__ void sweep_windows(const DMolSet& set, const DMol& m, Smem& s,
                                            const DWeight& w, double beta, int* err, bool rndord,
                                            double& eol, double& etor, double& ep, uint32_t& head,
-                                           unsigned long long& nacc, unsigned long long& nprop) {
+                                           unsigned long long& nacc, unsigned long long& nprop,
+                                           unsigned long long& pterms) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int spec_warp = kWarps - 1;
   const int n = m.natoms;
@@ -1625,6 +1626,7 @@ __device__ __noinline__ void sweep_windows(const DMolSet& set, const DMol& m, Sm
       split_hi_lo(ox, oy, oz, s.p4[a].w, s.l4[a].w, s.wp4[o], s.wl4[o]);
     }
     if (resum) {
+      pterms += (unsigned long long)m.npairs;
       double el = 0.0, vw = 0.0, hb = 0.0;
       pair_rows<F32, true>(set.f, m, s, kWarps, el, vw, hb);
       double v = el;
@@ -1719,6 +1721,7 @@ __device__ __noinline__ void sweep_windows(const DMolSet& set, const DMol& m, Sm
     }
     head += (uint32_t)(last * (u + 1) + u + drew_last);
     nprop += (unsigned long long)(last + 1);
+    for (int k = 0; k < wn; ++k) pterms += 2ull * (unsigned long long)m.var_cross[wp[k].jv];
     if (ks >= 0) {
       ++nacc;
       eol = enw_k;
@@ -1774,7 +1777,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
   load_chain(ch, m, c, s);
   double beta = ch.beta[c];
   int* err = &ch.err[c];
-  unsigned long long nacc = 0, nprop = 0;
+  unsigned long long nacc = 0, nprop = 0, pterms = 0;
   __syncthreads();
   // logs of the values already queued, then fill the queue
   if (warp == spec_warp) {
@@ -1807,6 +1810,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
     // ---- eol = energy() (metropolis.f:35)
     setvar_all(m, s);
     __syncthreads();
+    pterms += (unsigned long long)m.npairs;
     torsion_all(m, s);
     full_rebuild(m, s);
     evaluate_block<F32, ROWS, SASA>(set.f, m, s, err);
@@ -1829,7 +1833,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       // the incremental mode in speculative windows (same trajectory, fewer barriers)
       windowed = m.rows && !set.f.epsd && relaxed && set.window >= 2 && m.nfree > 0;
       if (windowed)
-        sweep_windows<F32>(set, m, s, w, beta, err, rndord, eol, etor, ep, head, nacc, nprop);
+        sweep_windows<F32>(set, m, s, w, beta, err, rndord, eol, etor, ep, head, nacc, nprop,
+                           pterms);
     }
     if (!windowed && m.nfree > 0 && threadIdx.x == 0) {
       make_proposal(m, s, 0, head, rndord, sc.cur);
@@ -1874,7 +1879,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       // afresh every 16 proposals (same coordinates; eol follows).
       const bool incr = ROWS && F32 && m.rows && !set.f.epsd && relaxed;
       double xold = 0.0;
+      pterms += incr ? 2ull * (unsigned long long)m.var_cross[cur.jv] : (unsigned long long)m.npairs;
       if (incr && p > 0 && (p & 15) == 0) {
+        pterms += (unsigned long long)m.npairs;
         double el = 0.0, vw = 0.0, hb = 0.0;
         pair_rows<F32, true>(set.f, m, s, kWarps, el, vw, hb);
         double v = el;
@@ -2010,6 +2017,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
     setvar_all(m, s);
     __syncthreads();
     if (sw + 1 == nsweeps) {
+      pterms += (unsigned long long)m.npairs;
       torsion_all(m, s);
       full_rebuild(m, s);
       evaluate_block<F32, ROWS, SASA>(set.f, m, s, err);
@@ -2042,6 +2050,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
     ch.eol[c] = eol;
     ch.nacc[c] += nacc;
     ch.nprop[c] += nprop;
+    ch.pterms[c] += pterms;
     s.mt[kQHead] = head;
   }
   __syncthreads();

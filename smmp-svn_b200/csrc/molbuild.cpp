@@ -1064,6 +1064,21 @@ MolTopo build_topology(const ResidueLibrary& lib, const ForceField& ff, const Bu
     const int i = int(w & 0x3fffu), j = int(w >> 14);
     cnt[(size_t)std::min(i, j) * n + std::max(i, j)] = 1;
   }
+  // pairs across each variable's bond (exactly one atom in its range): the
+  // pair terms an incremental proposal sums before and after the move
+  {
+    std::vector<std::pair<int, int>> pl;
+    pl.reserve((size_t)t.npairs);
+    for (int i = 0; i < n; ++i)
+      for (int j = i + 1; j < n; ++j)
+        if (cnt[(size_t)i * n + j]) pl.emplace_back(i, j);
+    for (int v = 0; v < nv; ++v) {
+      const int lo = t.var_lo[v], hi = t.var_hi[v];
+      int c = 0;
+      for (const auto& q : pl) c += ((q.first >= lo && q.first <= hi) != (q.second >= lo && q.second <= hi));
+      t.var_cross.push_back(c);
+    }
+  }
   // the same pair set by rows (every pair once, 1-4 pairs within the window)
   t.near_mask.assign(n, 0);
   t.near14.assign(n, 0);

@@ -134,6 +134,8 @@ DeviceSet::DeviceSet(const std::vector<std::shared_ptr<Molecule>>& mols) {
     d.var_base = upload(t.var_base);
     d.var_lo = upload(t.var_lo);
     d.var_hi = upload(t.var_hi);
+    d.var_cross = upload(t.var_cross);
+    d.npairs = (int)t.npairs;
     d.sib_off = upload(t.sib_off);
     d.sib = upload(t.sib.empty() ? std::vector<int>{0} : t.sib);
     d.var_e0 = upload(t.var_e0);
@@ -285,6 +287,7 @@ Ensemble::Ensemble(std::vector<std::shared_ptr<Molecule>> mols, std::vector<int>
   ch_.terms = dalloc<double>(allocs_, (size_t)n_ * 6);
   ch_.nacc = dalloc<unsigned long long>(allocs_, n_);
   ch_.nprop = dalloc<unsigned long long>(allocs_, n_);
+  ch_.pterms = dalloc<unsigned long long>(allocs_, n_);
   ch_.err = dalloc<int>(allocs_, n_);
   ch_.coords = nullptr;
   ch_.sur = DSurrogate{};
@@ -391,7 +394,7 @@ int Ensemble::autotune(int flags, double* ms_out) {
                nm = (size_t)nmt_ * kMTWords;
   std::vector<double> v, t, e, tr;
   std::vector<uint32_t> mt;
-  std::vector<unsigned long long> a, p, d1, d2;
+  std::vector<unsigned long long> a, p, d1, d2, pt;
   std::vector<int> er;
   d2h(v, ch_.vlvr, nv);
   d2h(t, ch_.toat, nt);
@@ -400,6 +403,7 @@ int Ensemble::autotune(int flags, double* ms_out) {
   d2h(tr, ch_.terms, (size_t)n_ * 6);
   d2h(a, ch_.nacc, n_);
   d2h(p, ch_.nprop, n_);
+  d2h(pt, ch_.pterms, n_);
   d2h(d1, ch_.da_n1, n_);
   d2h(d2, ch_.da_n2, n_);
   d2h(er, ch_.err, n_);
@@ -411,6 +415,7 @@ int Ensemble::autotune(int flags, double* ms_out) {
     h2d(ch_.terms, tr);
     h2d(ch_.nacc, a);
     h2d(ch_.nprop, p);
+    h2d(ch_.pterms, pt);
     h2d(ch_.da_n1, d1);
     h2d(ch_.da_n2, d2);
     h2d(ch_.err, er);
@@ -760,6 +765,7 @@ void Ensemble::get_acceptance(std::vector<unsigned long long>& a,
   d2h(p, ch_.nprop, n_);
 }
 void Ensemble::get_errors(std::vector<int>& e) const { d2h(e, ch_.err, n_); }
+void Ensemble::get_pair_terms(std::vector<unsigned long long>& p) const { d2h(p, ch_.pterms, n_); }
 void Ensemble::set_acceptance(const std::vector<unsigned long long>& acc,
                               const std::vector<unsigned long long>& prop) {
   if ((int)acc.size() != n_ || (int)prop.size() != n_) throw std::runtime_error("set_acceptance: size");

@@ -150,6 +150,9 @@ class Ensemble {
   void get_acceptance(std::vector<unsigned long long>& acc,
                       std::vector<unsigned long long>& prop) const;
   void get_errors(std::vector<int>& e) const;
+  // pair terms the sweeps evaluated per chain (full sums and the pairs across
+  // each incremental proposal's bond, before and after the move)
+  void get_pair_terms(std::vector<unsigned long long>& p) const;
   void set_acceptance(const std::vector<unsigned long long>& acc,
                       const std::vector<unsigned long long>& prop);
   void get_coords(std::vector<double>& xyz);       // [chain*3*tstride]

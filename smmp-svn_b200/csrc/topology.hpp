@@ -74,6 +74,7 @@ struct MolTopo {
   std::vector<uint32_t> chunks;        // i | j0<<14 | (len-1)<<28
   std::vector<uint32_t> pairs14;       // i | j<<14
   long long npairs = 0;                // pair terms per full evaluation
+  std::vector<int> var_cross;          // pairs across each variable's bond (one atom in its range)
   // The same pair set by rows: for atom i, bit k of near_mask[i] / near14[i]
   // marks pair (i, i+1+k) as a normal / 1-4 pair.  rows_ok is set when every
   // pair more than kNearWindow apart is a normal pair and no pair is listed

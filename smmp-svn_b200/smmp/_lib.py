@@ -111,6 +111,8 @@ _SIGS = {
     "smmp_ens_set_window": (c_int, [c_void_p, c_int, P(c_int)]),
     "smmp_ens_window": (c_int, [c_void_p, P(c_int), P(c_double)]),
     "smmp_ens_set_pair_work": (c_int, [c_void_p, c_int]),
+    "smmp_ens_pt_stats": (c_int, [c_void_p, P(ctypes.c_uint64)]),
+    "smmp_ens_pair_terms": (c_int, [c_void_p, P(ctypes.c_uint64)]),
     "smmp_ens_da_stats": (c_int, [c_void_p, P(ctypes.c_uint64), P(ctypes.c_uint64)]),
     "smmp_sur_get_params": (c_int, [c_void_p, P(ctypes.c_float), P(ctypes.c_float)]),
     "smmp_sur_set_params": (c_int, [c_void_p, P(ctypes.c_float), P(ctypes.c_float)]),

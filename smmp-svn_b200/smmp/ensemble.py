@@ -208,6 +208,18 @@ class Ensemble:
         check(lib.smmp_ens_pt_map(self._h, out.ctypes.data_as(_I)))
         return out
 
+    def pair_terms(self):
+        """Pair terms each chain's sweeps have evaluated so far."""
+        out = np.zeros(self.nchains, dtype=np.uint64)
+        check(lib.smmp_ens_pair_terms(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))))
+        return out
+
+    def pt_stats(self):
+        """(attempts, accepts) of each label pair (k, k+1) since set_pt."""
+        out = np.zeros(2 * self.nchains, dtype=np.uint64)
+        check(lib.smmp_ens_pt_stats(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))))
+        return out[0::2], out[1::2]
+
     # ---------------------------------------------------------------- state
     def energies(self):
         out = np.zeros(self.nchains)

@@ -217,6 +217,28 @@ class Oracle:
         self.lib().orc_get_topology(self.h, P(ai), P(ad), P(vi), P(ms), P(vw), P(l14))
         return ai
 
+    def partem_batched(self, betas, seeds, exchange_seed, wrap, nrounds, nthreads=8):
+        """Batched parallel tempering (oracle/oracle_capi.cpp orc_partem_batched):
+        per-round histories (chain at each label, energies, free variables)
+        and the per-pair (attempts, accepts)."""
+        n = len(betas)
+        L = self.lib()
+        L.orc_partem_batched.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                         ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        b = np.ascontiguousarray(betas, dtype=np.float64)
+        sd = np.ascontiguousarray(seeds, dtype=np.int32)
+        tc = np.zeros((nrounds, n), np.int32)
+        eo = np.zeros((nrounds, n))
+        vl = np.zeros((nrounds, n, self.nvr))
+        st = np.zeros(2 * n, np.uint64)
+        rc = L.orc_partem_batched(self.h, n, b.ctypes.data, sd.ctypes.data, int(exchange_seed),
+                                  int(bool(wrap)), int(nrounds), int(nthreads), tc.ctypes.data,
+                                  eo.ctypes.data, vl.ctypes.data, st.ctypes.data)
+        assert rc == 0, L.orc_last_error()
+        return tc, eo, vl, (st[0::2], st[1::2])
+
     def topology(self):
         """All of orc_get_topology: (atom_i [n,11], atom_d [n,4], var_i [nv,9],
         moving sets [nms,2], vdW domains [nvw,3], 1-4 entries [n14,2]);
