@@ -102,6 +102,14 @@ int smmp_energy(double* e_out);
  * (COMMON /eny_r/, INCL.H:343-349). */
 int smmp_energy_terms(double terms[6]);
 
+/* enysol(nmol=0): smmp.pyf:664-665, enysol.f:13.  The numerical solvation
+ * energy eysl of the current conformation (nmol 0 or 1: the one molecule).
+ * The reference sums it over the coordinates of the last rebuild; here the
+ * conformation is rebuilt from the current variables (as energy() does) and
+ * its eysl returned; the energy terms are updated as by smmp_energy.  Needs a
+ * numerical SASA model (itysol 1..9), else SMMP_ERR_ARG. */
+int smmp_enysol(int nmol, double* eysl);
+
 /* setvar(nml, vlvrx): smmp.pyf:949-950, setvar.f:13.  Sets the variables of
  * molecule nml (1-based) and rebuilds its coordinates. */
 int smmp_setvar(int nml, const double* vlvrx);

@@ -623,6 +623,98 @@ int orc_gradient_by_sums(void* h, double* grad) {
 }
 
 // mulcan_par_mod.f90 weight recursion (see muca_update / muca_finish).
+// canon.f:12-132 (without its output files): beta from temp, a random
+// start when lrand, nequi sweeps, then sweeps nsw = 0..nswp with the energy
+// recorded when mod(nsw, nmes) == 0.  out = [energy after equilibration,
+// acceptance rate, last energy].
+int orc_canon(void* h, int nequi, int nswp, int nmes, double temp, int lrand, double* trace,
+              double* out) {
+  Smmp* s = S(h);
+  return guard([&] {
+    Smmp::Weight w;
+    s->beta = 1.0 / (temp * 1.98773e-3);
+    if (lrand) orc_random_start(h);
+    double eol = s->energy(), acz = 0.0;
+    for (int k = 1; k <= nequi; ++k) s->metropolis(eol, acz, w);
+    out[0] = eol;
+    acz = 0.0;
+    int m = 0, nsw = 0;
+    for (nsw = 0; nsw <= nswp; ++nsw) {
+      s->metropolis(eol, acz, w);
+      if (nsw % nmes == 0) trace[m++] = eol;
+    }
+    out[1] = acz / (double)(nsw * s->nvr);
+    out[2] = eol;
+  });
+}
+
+// nsweeps metropolis sweeps with a multicanonical weight (kind 1:
+// muca_weight, 2: muca_weight2; mulcan_par_mod.f90:380-410) over the bins
+// kmin..kmax of width ebin; eol and acz in/out as metropolis's arguments.
+int orc_sweeps_muca(void* h, int nsweeps, int kind, int kmin, int kmax, double ebin,
+                    const double* b, const double* alpha, double* eol, double* acz) {
+  Smmp* s = S(h);
+  return guard([&] {
+    Smmp::Weight w;
+    w.kind = kind == 1 ? Smmp::W_MUCA : Smmp::W_MUCA2;
+    w.kmin = kmin;
+    w.kmax = kmax;
+    w.ebin = ebin;
+    w.b = b;
+    w.alpha = alpha;
+    for (int k = 0; k < nsweeps; ++k) s->metropolis(*eol, *acz, w);
+  });
+}
+
+// mulcan_par (mulcan_par_mod.f90:23-190, without its files): beta from temp,
+// random start, nsweep sweeps with muca_weight, the histogram of each sweep's
+// energy bin, the weights updated every nup sweeps, and at the end beta
+// folded into b (muca_weight2's table).  b_out, alpha_out: [kmax-kmin+1];
+// out = [acceptance, last energy].
+int orc_mulcan_par(void* h, int nsweep, int nup, double temp, int kmin, int kmax, double ebin,
+                   double* b_out, double* alpha_out, double* out) {
+  Smmp* s = S(h);
+  return guard([&] {
+    const int nb = kmax - kmin + 1;
+    const double beta = 1.0 / (temp * 1.98773e-3);
+    s->beta = beta;
+    std::vector<double> xhist(nb, 0.0), g1(nb, 0.0), b(nb, 0.0), alpha(nb, 0.0), ent(nb, 0.0);
+    std::vector<int> ihist(nb, 0);
+    orc_random_start(h);
+    double eol = s->energy(), acz = 0.0;
+    Smmp::Weight w;
+    w.kind = Smmp::W_MUCA;
+    w.kmin = kmin;
+    w.kmax = kmax;
+    w.ebin = ebin;
+    w.b = b.data();
+    w.alpha = alpha.data();
+    for (int nsw = 1; nsw <= nsweep; ++nsw) {
+      s->metropolis(eol, acz, w);
+      const double x = eol / ebin + std::copysign(0.5, eol);
+      const int muold = (int)std::min((double)kmax, std::max((double)kmin, x));
+      ihist[muold - kmin] += 1;
+      if (nsw % nup == 0)
+        oracle::muca_update(kmin, kmax, ebin, beta, ihist.data(), xhist.data(), g1.data(),
+                            b.data(), alpha.data(), ent.data());
+    }
+    out[0] = acz / (double)((nsweep + 1) * s->nvr);
+    out[1] = eol;
+    oracle::muca_finish(kmin, kmax, ebin, beta, b.data(), alpha.data());
+    for (int k = 0; k < nb; ++k) {
+      b_out[k] = b[k];
+      alpha_out[k] = alpha[k];
+    }
+  });
+}
+
+// enysol.f:13-339: the numerical solvation energy of the current coordinates
+// (after an energy() call), molecule nmol (0: all).
+int orc_enysol(void* h, int nmol, double* eysl) {
+  Smmp* s = S(h);
+  return guard([&] { *eysl = s->enysol(nmol); });
+}
+
 int orc_muca_update(int kmin, int kmax, double ebin, double beta, int* ihist, double* xhist,
                     double* g1, double* b, double* alpha, double* ent) {
   return guard([&] { oracle::muca_update(kmin, kmax, ebin, beta, ihist, xhist, g1, b, alpha, ent); });

@@ -342,6 +342,16 @@ int smmp_energy(double* e_out) {
   });
 }
 
+int smmp_enysol(int nmol, double* eysl) {
+  return guard([&] {
+    require_molecule();
+    need(nmol == 0 || nmol == 1, "molecule index out of range");
+    need(U().cfg.itysol > 0, "enysol needs a numerical SASA model (itysol 1..9)");
+    universe_energy();
+    if (eysl) *eysl = U().terms[4];
+  });
+}
+
 int smmp_energy_terms(double terms[6]) {
   return guard([&] {
     need(terms != nullptr, "terms is NULL");

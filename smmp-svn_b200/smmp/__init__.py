@@ -257,6 +257,14 @@ def energy():
     return e.value
 
 
+def enysol(nmol=0):
+    """enysol(nmol=0) -- smmp.pyf:664, enysol.f:13: the numerical solvation
+    energy of the current conformation (rebuilt from the current variables)."""
+    e = ctypes.c_double()
+    check(lib.smmp_enysol(int(nmol), ctypes.byref(e)))
+    return e.value
+
+
 def setvar(nml, vlvrx):
     """setvar(nml, vlvrx) -- smmp.pyf:949, setvar.f:13."""
     a = np.ascontiguousarray(vlvrx, dtype=np.float64)

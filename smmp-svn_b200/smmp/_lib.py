@@ -41,6 +41,7 @@ _SIGS = {
     "smmp_init_molecule": (c_int, [c_int, c_char_p, c_char_p, c_char_p, c_char_p]),
     "smmp_energy": (c_int, [P(c_double)]),
     "smmp_energy_terms": (c_int, [P(c_double)]),
+    "smmp_enysol": (c_int, [c_int, P(c_double)]),
     "smmp_setvar": (c_int, [c_int, P(c_double)]),
     "smmp_metropolis": (c_int, [P(c_double), P(c_double), P(Weight)]),
     "smmp_sgrnd": (c_int, [ctypes.c_int32]),
