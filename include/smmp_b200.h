@@ -135,6 +135,22 @@ int smmp_outvar(int nml, const char* fileName);
  * from the variables) in PDB format; fileName "" (or blanks): standard output. */
 int smmp_outpdb(int nml, const char* fileName);
 
+/* gradient(): gradient.f:13 (opeshe.f:12-317), vacuum energy (itysol 0).
+ * Sets the variables and rebuilds (as setvar), then gdeyvr[ntlvr] = dE/dv of
+ * every variable (COMMON /eny_r/ gdeyvr) and *eysm the energy; the terms as
+ * smmp_energy_terms gives them.  FP64 on the GPU. */
+int smmp_gradient(double* gdeyvr, double* eysm);
+/* minim(imin, maxit, eps): smmp.pyf:1234, minim.f:13.  Minimises the energy
+ * over the free variables with the GPU gradient: imin 1 quasi-Newton (BFGS),
+ * 2 conjugate gradients (Polak-Ribiere+), each with a strong-Wolfe line
+ * search; stops when the squared gradient is below eps, after maxit energy
+ * and gradient evaluations, or when a line search makes no progress.  The
+ * variables are left at the minimum (wrapped into (-pi, pi]) and the energy
+ * re-evaluated; *nop (if not NULL) = evaluations used.  The search path is
+ * this library's own, not minqsn.f's: the same minimum, not the same steps.
+ * Vacuum energy (itysol 0) only. */
+int smmp_minim(int imin, int maxit, double eps, int* nop);
+
 /* sgrnd(seed) / grnd(): smmp.pyf:5620, twister.f:64 and :104. */
 int smmp_sgrnd(int32_t seed);
 double smmp_grnd(void);
@@ -256,6 +272,10 @@ int smmp_ens_pt_stats(smmp_ens_t* e, uint64_t* stats);
  * proposal summed in full, and twice the pairs across a proposal's bond in
  * the incremental mode.  Delayed-acceptance sweeps are not counted. */
 int smmp_ens_pair_terms(smmp_ens_t* e, uint64_t* terms);
+/* gradient.f (vacuum) for every chain: grad[chain * vstride + v] = dE/dv of
+ * every variable (FP64), energies[chain] the energy (may be NULL).  The chains'
+ * dihedral states go through setvar as in the reference. */
+int smmp_ens_gradient(smmp_ens_t* e, double* grad, double* energies);
 int smmp_ens_sizes(smmp_ens_t* e, int* nchains, int* vstride, int* tstride);
 int smmp_ens_get_energies(smmp_ens_t* e, double* eol);          /* [nchains] */
 int smmp_ens_get_terms(smmp_ens_t* e, double* terms);           /* [nchains*6] */

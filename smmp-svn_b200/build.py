@@ -27,7 +27,7 @@ CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I" + SRC, "-I" 
 CUDA_SOURCES = ["kernels.cu", "runtime.cu", "capi.cu", "surrogate.cu", "esolan.cu"]
 # the analytic SASA keeps the reference's separately rounded FP64 arithmetic
 CUDA_EXTRA = {"esolan.cu": ["-fmad=false"]}
-CXX_SOURCES = ["molbuild.cpp", "ecepp.cpp", "topology.cpp", "muca.cpp"]
+CXX_SOURCES = ["molbuild.cpp", "ecepp.cpp", "topology.cpp", "muca.cpp", "minimize.cpp"]
 
 
 def _headers():

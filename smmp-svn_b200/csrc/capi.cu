@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "../../include/smmp_b200.h"
+#include "minimize.hpp"
 #include "molbuild.hpp"
 #include "muca.hpp"
 #include "runtime.hpp"
@@ -477,6 +478,56 @@ double smmp_grnd(void) {
   return st == SMMP_OK ? r : NAN;
 }
 
+// gradient() of the global system: energies and gdeyvr of chain 0.
+double universe_gradient(std::vector<double>& g) {
+  Universe& u = U();
+  u.ens->gradient(g);
+  raise_kernel_errors(*u.ens);
+  std::vector<double> e, t;
+  u.ens->get_eol(e);
+  u.ens->get_terms(t);
+  for (int k = 0; k < 6; ++k) u.terms[k] = t[k];
+  return e[0];
+}
+
+int smmp_gradient(double* gdeyvr, double* eysm) {
+  return guard([&] {
+    require_molecule();
+    need(U().cfg.itysol == 0, "the GPU gradient is for the vacuum energy (itysol 0)");
+    std::vector<double> g;
+    const double e = universe_gradient(g);
+    if (gdeyvr) std::copy(g.begin(), g.begin() + U().mol->topo.nvar, gdeyvr);
+    if (eysm) *eysm = e;
+  });
+}
+
+int smmp_minim(int imin, int maxit, double eps, int* nop) {
+  return guard([&] {
+    require_molecule();
+    need(imin == 1 || imin == 2, "imin must be 1 (quasi-Newton) or 2 (conjugate gradients)");
+    need(maxit > 0 && eps >= 0.0, "bad minim arguments");
+    Universe& u = U();
+    need(u.cfg.itysol == 0, "the GPU gradient is for the vacuum energy (itysol 0)");
+    const MolTopo& t = u.mol->topo;
+    std::vector<double> vl, g;
+    u.ens->get_vlvr(vl);
+    std::vector<double> x(t.nfree);
+    for (int k = 0; k < t.nfree; ++k) x[k] = vl[t.idvr[k]];
+    auto fg = [&](const double* xv, double* gv) {
+      for (int k = 0; k < t.nfree; ++k) vl[t.idvr[k]] = xv[k];
+      u.ens->set_vlvr(vl);
+      const double e = universe_gradient(g);
+      for (int k = 0; k < t.nfree; ++k) gv[k] = g[t.idvr[k]];
+      return e;
+    };
+    const MinimizeResult r = minimize(imin, x, fg, maxit, eps);
+    for (int k = 0; k < t.nfree; ++k) vl[t.idvr[k]] = h_wrap(x[k]);   // minim.f: into (-pi, pi]
+    u.ens->set_vlvr(vl);
+    universe_energy();
+    if (nop) *nop = r.calls;
+  });
+}
+
 int smmp_canon(int nequi, int nswp, int nmes, double temp, int lrand, double* trace, double* out) {
   return guard([&] {
     require_molecule();
@@ -894,6 +945,21 @@ int smmp_ens_pair_terms(smmp_ens_t* e, uint64_t* terms) {
     std::vector<unsigned long long> p;
     e->e->get_pair_terms(p);
     std::copy(p.begin(), p.end(), terms);
+  });
+}
+
+int smmp_ens_gradient(smmp_ens_t* e, double* grad, double* energies) {
+  return guard([&] {
+    need(e && grad, "NULL argument");
+    std::vector<double> g;
+    e->e->gradient(g);
+    std::copy(g.begin(), g.end(), grad);
+    if (energies) {
+      std::vector<double> en;
+      e->e->get_eol(en);
+      std::copy(en.begin(), en.end(), energies);
+    }
+    raise_kernel_errors(*e->e);
   });
 }
 

@@ -31,6 +31,7 @@
 #include <cstdint>
 
 #include "device.cuh"
+#include "gradient_core.cuh"
 #include "kernels.hpp"
 #include "mt.cuh"
 
@@ -1351,6 +1352,94 @@ __global__ void __launch_bounds__(kThreads, 1) k_energy(DMolSet set, DChains ch,
   store_chain(ch, m, c, s);
 }
 
+// dE/dvlvr of every variable and the energy (gradient.f:13 with opeshe.f:12-317,
+// vacuum) for chains [first, first + gridDim.x), in the order-free form of
+// gradient_core.cuh: setvar and a full FP64 rebuild of the chain's variables,
+// the force on every atom from all of its pairs of the mklist lists
+// (shared-memory atomics), then one warp per variable sums the forces and
+// torques over the atoms it moves, its contiguous range [var_lo, var_hi].
+// grad[c * vstride + v]; the energy to ch.eol and its terms to ch.terms.
+__global__ void __launch_bounds__(kThreads, 1) k_gradient(DMolSet set, DChains ch, int first,
+                                                          double* grad) {
+  const int c = first + blockIdx.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  Smem s = carve(set, false);
+  const DMol& m = stage_mol(set, ch, c, s);
+  load_static(*set.ff, m, s, false);
+  load_chain(ch, m, c, s);
+  __syncthreads();
+  setvar_all(m, s);
+  __syncthreads();
+  torsion_all(m, s);
+  full_rebuild(m, s);
+  // forces in the rebuild frames' region, free after the rebuild
+  double *Fx = s.bx, *Fy = s.by, *Fz = s.bz;
+  for (int k = threadIdx.x; k < m.natoms; k += blockDim.x) Fx[k] = Fy[k] = Fz[k] = 0.0;
+  __syncthreads();
+  const GradTables tab{s.ta, s.ta14, s.tc, s.thb, set.f.conv, set.f.plt, set.f.slp, set.f.epsd};
+  double e[3] = {0.0, 0.0, 0.0};
+  auto pair = [&](int i, int j, bool is14) {
+    const double dx = s.x[j] - s.x[i], dy = s.y[j] - s.y[i], dz = s.z[j] - s.z[i];
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    const double f = gradient_pair(tab, s.type[i], s.type[j], s.cq[i], s.cq[j], r2, is14, e);
+    atomicAdd(&Fx[i], f * dx);
+    atomicAdd(&Fy[i], f * dy);
+    atomicAdd(&Fz[i], f * dz);
+    atomicAdd(&Fx[j], -f * dx);
+    atomicAdd(&Fy[j], -f * dy);
+    atomicAdd(&Fz[j], -f * dz);
+  };
+  for (int t = threadIdx.x; t < m.nchunks * 8; t += blockDim.x) {
+    int i, j;
+    if (gradient_chunk_pair(m.chunks, t, i, j)) pair(i, j, false);
+  }
+  for (int t = threadIdx.x; t < m.n14; t += blockDim.x) {
+    const uint32_t w = m.pairs14[t];
+    pair(int(w & 0x3fffu), int(w >> 14), true);
+  }
+  double vr = 0.0;
+  for (int v = threadIdx.x; v < m.nvar; v += blockDim.x) vr += s.et[v];
+  warp_partials(s, e[0], e[1], e[2], vr, 0.0);
+  __syncthreads();
+  for (int v = warp; v < m.nvar; v += kWarps) {
+    double S[6] = {0, 0, 0, 0, 0, 0};
+    for (int a = m.var_lo[v] + lane; a <= m.var_hi[v]; a += 32) {
+      const double fx = Fx[a], fy = Fy[a], fz = Fz[a], x = s.x[a], y = s.y[a], z = s.z[a];
+      S[0] += fx;
+      S[1] += fy;
+      S[2] += fz;
+      S[3] += fy * z - fz * y;
+      S[4] += fz * x - fx * z;
+      S[5] += fx * y - fy * x;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+      for (int k = 0; k < 6; ++k) S[k] += __shfl_xor_sync(0xffffffffu, S[k], o);
+    if (lane == 0) {
+      const int b = m.var_base[v], o = m.iow[b];
+      double ev[3] = {s.x[b] - s.x[o], s.y[b] - s.y[o], s.z[b] - s.z[o]};
+      const double inv = 1.0 / sqrt(ev[0] * ev[0] + ev[1] * ev[1] + ev[2] * ev[2]);
+      ev[0] *= inv;
+      ev[1] *= inv;
+      ev[2] *= inv;
+      const double rb[3] = {s.x[b], s.y[b], s.z[b]};
+      const double fvr = gradient_torsion_force(m.var_e0[v], m.var_sg[v], m.var_rn[v],
+                                                s.toat[m.var_atom[v]]);
+      grad[(size_t)c * ch.vstride + v] = gradient_variable(ev, rb, S, S + 3, fvr);
+    }
+  }
+  double sum[5];
+  all_sums(s, sum);
+  if (threadIdx.x == 0) {
+    const double en = total_of(sum);
+    ch.eol[c] = en;
+    write_terms(ch, c, sum);
+    if (!isfinite(en)) set_err(&ch.err[c], kErrNonFinite);
+  }
+  store_chain(ch, m, c, s);
+}
+
 // Replica exchange (partem_s.f:210-232): alternate even/odd neighbour pairs,
 // replica num_rep pairs with 1 when `wrap` is set.  temp_chain[k] is the chain
 // at temperature label k (ipoi); betas[k] the inverse temperature of label k.
@@ -2614,6 +2703,15 @@ cudaError_t launch_sweep_pt(const DMolSet& set, const DChains& ch, const DWeight
     default: return SMMP_SWEEP(true, true, true);
   }
 #undef SMMP_SWEEP
+}
+
+cudaError_t launch_gradient(const DMolSet& set, const DChains& ch, int first, int count,
+                            double* grad, cudaStream_t st) {
+  const size_t sm = sweep_smem_bytes(set);
+  cudaError_t e = prep_smem((const void*)k_gradient, sm);
+  if (e != cudaSuccess || count <= 0) return e;
+  k_gradient<<<count, kThreads, sm, st>>>(set, ch, first, grad);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_exchange(const DChains& ch, int* temp_chain, const double* betas, int n,

@@ -42,6 +42,10 @@ constexpr int kEsolanBatch = 16;
 size_t esolan_scratch_bytes(int count);
 cudaError_t launch_esolan(const DMolSet& set, const DChains& ch, int first, int count,
                           double* scratch, double* area, cudaStream_t st);
+// gradient.f / opeshe.f: dE/dv of every variable of chains [first,
+// first+count) into grad[chain * vstride + v], energies into ch.eol/terms.
+cudaError_t launch_gradient(const DMolSet& set, const DChains& ch, int first, int count,
+                            double* grad, cudaStream_t st);
 cudaError_t launch_exchange(const DChains& ch, int* temp_chain, const double* betas, int n,
                             uint32_t* mt, int* iswitch, int wrap, unsigned long long* stats,
                             cudaStream_t st);

@@ -359,6 +359,15 @@ void Ensemble::set_surrogate(const DSurrogate* view, float floor, int min_stage1
   graph_len_ = 0;
 }
 
+void Ensemble::gradient(std::vector<double>& g) {
+  if (set().f.itysol != 0)
+    throw std::invalid_argument("the GPU gradient is for the vacuum energy (itysol 0)");
+  if (!grad_buf_) grad_buf_ = dalloc<double>(allocs_, (size_t)n_ * ch_.vstride);
+  check_cuda(launch_gradient(set(), ch_, 0, n_, grad_buf_, stream_), "gradient launch");
+  check_cuda(cudaStreamSynchronize(stream_), "gradient sync");
+  d2h(g, grad_buf_, (size_t)n_ * ch_.vstride);
+}
+
 void Ensemble::set_pair_work(int form) {
   if (form < 0 || form > 2) throw std::invalid_argument("pair-work form must be 0, 1 or 2");
   const int rows_mode[3] = {0, 1, -1};

@@ -118,6 +118,9 @@ class Ensemble {
 
   void random_start();                       // canon.f:60-67 for every chain
   void energy(bool fp32);                    // energy() of every chain
+  // gradient.f (vacuum): dE/dv of every variable of every chain into
+  // g[chain * vstride + v] (FP64), energies as energy() leaves them
+  void gradient(std::vector<double>& g);
   void sweeps(int nsweeps, int flags, const DWeight& w);   // metropolis, no exchange
   void sweeps_chain(int c, int nsweeps, int flags, const DWeight& w);
   void energy_chain(int c, bool fp32);
@@ -186,6 +189,7 @@ class Ensemble {
   bool pt_fused_last_ = false;   // the last batched pt_sweeps ran the fused launch
   double window_ms_[3] = {0.0, 0.0, 0.0};
   double* coords_buf_ = nullptr;
+  double* grad_buf_ = nullptr;
   // analytic SASA (itysol < 0): per-thread scratch of k_esolan for
   // kEsolanBatch chains, the per-atom areas of every chain
   double* esolan_scratch_ = nullptr;

@@ -28,7 +28,7 @@ __all__ = ["init_energy", "init_molecule", "energy", "setvar", "metropolis", "ou
            "grnd", "canon", "anneal", "can_weight", "MucaWeight", "SmmpError",
            "epar_l", "isolty", "updchois", "bet", "mol_par", "var_r", "var_i", "eny_r",
            "updstats", "gpu_available", "reset", "coordinates", "MucaState",
-           "mulcan_par"]
+           "mulcan_par", "enysol", "gradient", "minim"]
 
 
 def gpu_available():
@@ -263,6 +263,26 @@ def enysol(nmol=0):
     e = ctypes.c_double()
     check(lib.smmp_enysol(int(nmol), ctypes.byref(e)))
     return e.value
+
+
+def gradient():
+    """gradient() -- gradient.f:13 (vacuum): (energy, dE/dv of every
+    variable); the derivatives are also /eny_r/ gdeyvr of the reference."""
+    n = _sizes()[1]
+    g = np.zeros(max(n, 1))
+    e = ctypes.c_double()
+    check(lib.smmp_gradient(g.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(e)))
+    return e.value, g[:n]
+
+
+def minim(imin, maxit, eps):
+    """minim(imin, maxit, eps) -- smmp.pyf:1234, minim.f:13: minimise over the
+    free variables (1 quasi-Newton, 2 conjugate gradients) with the GPU
+    gradient; the variables are left at the minimum.  Returns the number of
+    energy+gradient evaluations."""
+    nop = ctypes.c_int()
+    check(lib.smmp_minim(int(imin), int(maxit), float(eps), ctypes.byref(nop)))
+    return nop.value
 
 
 def setvar(nml, vlvrx):

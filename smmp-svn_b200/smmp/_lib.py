@@ -42,6 +42,9 @@ _SIGS = {
     "smmp_energy": (c_int, [P(c_double)]),
     "smmp_energy_terms": (c_int, [P(c_double)]),
     "smmp_enysol": (c_int, [c_int, P(c_double)]),
+    "smmp_gradient": (c_int, [P(c_double), P(c_double)]),
+    "smmp_minim": (c_int, [c_int, c_int, c_double, P(c_int)]),
+    "smmp_ens_gradient": (c_int, [c_void_p, P(c_double), P(c_double)]),
     "smmp_setvar": (c_int, [c_int, P(c_double)]),
     "smmp_metropolis": (c_int, [P(c_double), P(c_double), P(Weight)]),
     "smmp_sgrnd": (c_int, [ctypes.c_int32]),

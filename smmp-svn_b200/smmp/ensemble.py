@@ -208,6 +208,14 @@ class Ensemble:
         check(lib.smmp_ens_pt_map(self._h, out.ctypes.data_as(_I)))
         return out
 
+    def gradient(self):
+        """(nchains, vstride) dE/dv of every variable (vacuum, FP64) and the
+        energies (gradient.f)."""
+        g = np.zeros(self.nchains * self.vstride)
+        e = np.zeros(self.nchains)
+        check(lib.smmp_ens_gradient(self._h, g.ctypes.data_as(_D), e.ctypes.data_as(_D)))
+        return g.reshape(self.nchains, self.vstride), e
+
     def pair_terms(self):
         """Pair terms each chain's sweeps have evaluated so far."""
         out = np.zeros(self.nchains, dtype=np.uint64)
