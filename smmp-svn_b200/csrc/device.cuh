@@ -59,6 +59,7 @@ struct DMol {
   const unsigned long long* near14;
   int rows;
   int npairs;                            // pair terms of a full evaluation
+  const uint32_t* flat;                  // every pair once: i | j<<14 | is14<<28
   const int* var_cross;                  // pair terms across each variable's bond
 };
 

@@ -243,8 +243,7 @@ __device__ Smem carve(const DMolSet& set, bool sasa) {
 // array, in the order stage_mol copies them (host sizing and device staging
 // must agree exactly).
 __host__ __device__ inline size_t stage_size(int natoms, int nvar, int nsib, int nlevels, int nfree,
-                                             int nchunks, int n14, int nheavy, bool rows,
-                                             bool lists) {
+                                             int nflat, int nheavy, bool rows, bool lists) {
   size_t b = 0;
   auto a = [&](size_t elem, int n) { b += align16(elem * (size_t)(n > 0 ? n : 1)); };
   a(4, nvar);          // var_atom
@@ -271,10 +270,7 @@ __host__ __device__ inline size_t stage_size(int natoms, int nvar, int nsib, int
   a(8, natoms);        // blen
   a(8, natoms);        // cba
   a(8, natoms);        // sba
-  if (lists) {
-    a(4, nchunks);     // chunks
-    a(4, n14);         // pairs14
-  }
+  if (lists) a(4, nflat);   // flat pair list
   return b;
 }
 
@@ -338,10 +334,7 @@ __device__ const DMol& stage_mol(const DMolSet& set, const DChains& ch, int c, S
   m.blen = stage_array(g.blen, g.natoms, pool, end, ok);
   m.cba = stage_array(g.cba, g.natoms, pool, end, ok);
   m.sba = stage_array(g.sba, g.natoms, pool, end, ok);
-  if (set.stage_lists) {
-    m.chunks = stage_array(g.chunks, g.nchunks, pool, end, ok);
-    m.pairs14 = stage_array(g.pairs14, g.n14, pool, end, ok);
-  }
+  if (set.stage_lists) m.flat = stage_array(g.flat, g.npairs, pool, end, ok);
   __syncthreads();
   if (threadIdx.x == 0) *s.mol = m;
   __syncthreads();
@@ -824,17 +817,13 @@ __device__ void pair_energy(const FFScalars& ff, const DMol& m, const Smem& s, i
     pair_rows<F32, false>(ff, m, s, nthr >> 5, el, vw, hb);
     return;
   }
-  const int nwork = m.nchunks * 8;
+  // the dense pair list: thread tid takes pairs tid, tid + nthr, ...
+  const int np = m.npairs;
   if (!F32) {
-    for (int t = tid; t < nwork; t += nthr) {
-      uint32_t w = m.chunks[t >> 3];
-      int l = t & 7;
-      int len = int((w >> 28) & 7u) + 1;
-      if (l < len) pair_term<false>(ff, s, int(w & 0x3fffu), int((w >> 14) & 0x3fffu) + l, false, el, vw, hb);
-    }
-    for (int t = tid; t < m.n14; t += nthr) {
-      uint32_t w = m.pairs14[t];
-      pair_term<false>(ff, s, int(w & 0x3fffu), int(w >> 14), true, el, vw, hb);
+    for (int t = tid; t < np; t += nthr) {
+      const uint32_t w = m.flat[t];
+      pair_term<false>(ff, s, int(w & 0x3fffu), int((w >> 14) & 0x3fffu), (w >> 28) != 0u, el, vw,
+                       hb);
     }
     return;
   }
@@ -845,23 +834,17 @@ __device__ void pair_energy(const FFScalars& ff, const DMol& m, const Smem& s, i
   KSum ke, kv, kh;
   double e64 = 0.0, v64 = 0.0, h64 = 0.0;
   int t = tid;
-  for (; t + nthr < nwork; t += 2 * nthr) {
-    uint32_t w0 = m.chunks[t >> 3], w1 = m.chunks[(t + nthr) >> 3];
-    int l0 = t & 7, l1 = (t + nthr) & 7;
-    if (l0 <= int((w0 >> 28) & 7u))
-      pair32(ff, s, int(w0 & 0x3fffu), int((w0 >> 14) & 0x3fffu) + l0, false, ke, kv, kh, e64, v64, h64);
-    if (l1 <= int((w1 >> 28) & 7u))
-      pair32(ff, s, int(w1 & 0x3fffu), int((w1 >> 14) & 0x3fffu) + l1, false, ke, kv, kh, e64, v64, h64);
+  for (; t + nthr < np; t += 2 * nthr) {   // two pairs in flight per thread
+    const uint32_t w0 = m.flat[t], w1 = m.flat[t + nthr];
+    pair32(ff, s, int(w0 & 0x3fffu), int((w0 >> 14) & 0x3fffu), (w0 >> 28) != 0u, ke, kv, kh, e64,
+           v64, h64);
+    pair32(ff, s, int(w1 & 0x3fffu), int((w1 >> 14) & 0x3fffu), (w1 >> 28) != 0u, ke, kv, kh, e64,
+           v64, h64);
   }
-  for (; t < nwork; t += nthr) {
-    uint32_t w = m.chunks[t >> 3];
-    int l = t & 7;
-    if (l <= int((w >> 28) & 7u))
-      pair32(ff, s, int(w & 0x3fffu), int((w >> 14) & 0x3fffu) + l, false, ke, kv, kh, e64, v64, h64);
-  }
-  for (int u = tid; u < m.n14; u += nthr) {
-    uint32_t w = m.pairs14[u];
-    pair32(ff, s, int(w & 0x3fffu), int(w >> 14), true, ke, kv, kh, e64, v64, h64);
+  for (; t < np; t += nthr) {
+    const uint32_t w = m.flat[t];
+    pair32(ff, s, int(w & 0x3fffu), int((w >> 14) & 0x3fffu), (w >> 28) != 0u, ke, kv, kh, e64,
+           v64, h64);
   }
   el += ff.conv * ke.value() + e64;
   vw += kv.value() + v64;
@@ -1107,6 +1090,24 @@ __device__ __forceinline__ void all_sums(const Smem& s, double* out) {
     for (int k = 0; k < 5; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
 #pragma unroll
   for (int k = 0; k < 5; ++k) out[k] = v[k];
+}
+// Sum of nw <= 16 warp partials in the order of a 32-lane xor butterfly whose
+// lanes nw..31 hold zero: warp_tree_sum over a warp and tree_sum16 in one
+// thread give the same bits (lane 0's tree; every lane ends with its bits).
+__device__ __forceinline__ double warp_tree_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double tree_sum16(const double* p, int stride, int nw) {
+  double t[16];
+#pragma unroll
+  for (int l = 0; l < 16; ++l) t[l] = (l < nw ? p[l * stride] : 0.0) + 0.0;
+#pragma unroll
+  for (int o = 8; o > 0; o >>= 1)
+#pragma unroll
+    for (int l = 0; l < o; ++l) t[l] = t[l] + t[l + o];
+  return t[0];
 }
 __device__ __forceinline__ double total_of(const double* sum) {
   // energy.f: eysm = eyel + eyvw + eyhb + eyvr, then + eysl
@@ -1757,7 +1758,7 @@ __device__ __noinline__ void sweep_windows(const DMolSet& set, const DMol& m, Sm
     int up = 0, drew = 1;
     if (lane < wn) {
       const Proposal& P = wp[lane];
-      for (int k = 0; k < kWarps - 1; ++k) dpair += s.wred[k * kMaxWindow + lane];
+      dpair = tree_sum16(s.wred + lane, kMaxWindow, kWarps - 1);
       const double epair = (ep + dpair) + 0.0;
       etn = (etor - P.eold) + P.enew;
       enw = epair + etn;
@@ -2034,11 +2035,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       }
       __syncthreads();
       // ---- phase C: every warp sums and decides (metropolis.f:72-87)
-      double dpair = 0.0, esl = 0.0;
-      for (int k = 0; k < kWarps - 1; ++k) {
-        dpair += s.red[k * 8];
-        esl += s.red[k * 8 + 1];
-      }
+      double dpair = warp_tree_sum(lane < kWarps - 1 ? s.red[lane * 8] : 0.0), esl = 0.0;
+      if (sasa) esl = warp_tree_sum(lane < kWarps - 1 ? s.red[lane * 8 + 1] : 0.0);
       // pair energy of the proposal: the state's plus the change (row form),
       // or the full sum
       const double epair = (incr ? ep + dpair : dpair) + esl;
@@ -2540,7 +2538,7 @@ size_t sweep_smem_bytes(const DMolSet& set) {
 }
 
 size_t stage_bytes_of(const DMol& d, bool lists) {
-  return stage_size(d.natoms, d.nvar, d.nsib, d.nlevels, d.nfree, d.nchunks, d.n14, d.nheavy,
+  return stage_size(d.natoms, d.nvar, d.nsib, d.nlevels, d.nfree, d.npairs, d.nheavy,
                     d.rows != 0, lists);
 }
 

@@ -1053,6 +1053,22 @@ MolTopo build_topology(const ResidueLibrary& lib, const ForceField& ff, const Bu
   auto by_atom = [](uint32_t x, uint32_t y) { return (x & 0x3fffu) < (y & 0x3fffu); };
   std::stable_sort(t.chunks.begin(), t.chunks.end(), by_atom);
   std::stable_sort(t.pairs14.begin(), t.pairs14.end(), by_atom);
+  // the dense list: every pair once, by listing atom, then partner
+  {
+    std::vector<uint64_t> keyed;
+    keyed.reserve((size_t)t.npairs);
+    for (uint32_t w : t.chunks) {
+      const uint32_t i = w & 0x3fffu, j0 = (w >> 14) & 0x3fffu, len = ((w >> 28) & 7u) + 1;
+      for (uint32_t j = j0; j < j0 + len; ++j) keyed.push_back(((uint64_t)i << 32) | (j << 1));
+    }
+    for (uint32_t w : t.pairs14)
+      keyed.push_back(((uint64_t)(w & 0x3fffu) << 32) | ((w >> 14) << 1) | 1u);
+    std::sort(keyed.begin(), keyed.end());
+    t.flat.reserve(keyed.size());
+    for (uint64_t k : keyed)
+      t.flat.push_back(uint32_t(k >> 32) | (uint32_t((k & 0xffffffffu) >> 1) << 14) |
+                       (uint32_t(k & 1u) << 28));
+  }
   // pair kind per unordered pair: 0 none, 1 one-four, 2 normal
   if ((long long)n * n > (1ll << 26)) fail("build_molecule: molecule too large for the pair table");
   std::vector<uint8_t> cnt((size_t)n * n, 0);

@@ -135,6 +135,7 @@ DeviceSet::DeviceSet(const std::vector<std::shared_ptr<Molecule>>& mols) {
     d.var_lo = upload(t.var_lo);
     d.var_hi = upload(t.var_hi);
     d.var_cross = upload(t.var_cross);
+    d.flat = upload(t.flat.empty() ? std::vector<uint32_t>{0} : t.flat);
     d.npairs = (int)t.npairs;
     d.sib_off = upload(t.sib_off);
     d.sib = upload(t.sib.empty() ? std::vector<int>{0} : t.sib);

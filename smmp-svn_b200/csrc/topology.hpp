@@ -73,6 +73,9 @@ struct MolTopo {
   // pair work
   std::vector<uint32_t> chunks;        // i | j0<<14 | (len-1)<<28
   std::vector<uint32_t> pairs14;       // i | j<<14
+  // every pair of the lists once, by listing atom then partner:
+  // i | j<<14 | is14<<28 (the sweep's dense pair loop)
+  std::vector<uint32_t> flat;
   long long npairs = 0;                // pair terms per full evaluation
   std::vector<int> var_cross;          // pairs across each variable's bond (one atom in its range)
   // The same pair set by rows: for atom i, bit k of near_mask[i] / near14[i]
