@@ -715,6 +715,45 @@ int orc_enysol(void* h, int nmol, double* eysl) {
   return guard([&] { *eysl = s->enysol(nmol); });
 }
 
+// enysol.f:107-330 over n arbitrary spheres (xyz[3n], radii r[n], sigma[n]),
+// with the unit-sphere points of the file tes (tessel, enysol.f:341-365):
+// counts[k] = exposed points of sphere k (-1 for r <= 0), areas[k], and
+// eysl = sum sigma_k areas_k in the reference's order; returns asa.
+int orc_enysol_spheres(int n, const double* xyz, const double* r, const double* sigma,
+                       const char* tes, int* counts, double* areas, double* eysl, double* asa) {
+  return guard([&] {
+    Smmp pts;
+    pts.tessel(tes);
+    std::vector<double> x(n + 1), y(n + 1), z(n + 1), rv(n + 1);
+    for (int k = 1; k <= n; ++k) {
+      x[k] = xyz[3 * (k - 1)];
+      y[k] = xyz[3 * (k - 1) + 1];
+      z[k] = xyz[3 * (k - 1) + 2];
+      rv[k] = r[k - 1];
+      counts[k - 1] = -1;
+      areas[k - 1] = 0.0;
+    }
+    double e = 0.0, vol = 0.0;
+    oracle::enysol_spheres(n, x.data(), y.data(), z.data(), rv.data(), pts.spoint.data(), pts.npnt,
+                           *asa, vol, [&](int k, double area, int icount) {
+                             counts[k - 1] = icount;
+                             areas[k - 1] = area;
+                             e = e + area * sigma[k - 1];
+                           });
+    *eysl = e;
+  });
+}
+
+// Solvation radii (rvdw, probe included) and coefficients of every atom.
+void orc_get_solvation(void* h, double* rvdw, double* sigma) {
+  Smmp* s = S(h);
+  int na = s->iatrs2[s->irsml2[s->ntlml]];
+  for (int i = 1; i <= na; ++i) {
+    rvdw[i - 1] = s->rvdw[i];
+    sigma[i - 1] = s->sigma[i];
+  }
+}
+
 int orc_muca_update(int kmin, int kmax, double ebin, double beta, int* ihist, double* xhist,
                     double* g1, double* b, double* alpha, double* ent) {
   return guard([&] { oracle::muca_update(kmin, kmax, ebin, beta, ihist, xhist, g1, b, alpha, ent); });

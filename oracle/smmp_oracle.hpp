@@ -203,6 +203,13 @@ double esolan_areas(int numat, const double* x, const double* y, const double* z
                     const double* rvdw, const double* sigma, const std::function<double()>& grnd,
                     double* As_out, double* gradan = nullptr);
 
+// enysol.f:107-330 over the spheres 1..numat (1-based arrays, radii > 0 take
+// part): asa and vdvol of the numerical surface; per_atom(k, area, icount)
+// for each sphere in the reference's box order.
+void enysol_spheres(int numat, const double* x, const double* y, const double* z,
+                    const double* rv, const double* spoint, int npnt, double& asa, double& vdvol,
+                    const std::function<void(int, double, int)>& per_atom);
+
 // mulcan_par_mod.f90:93-145 and :163-168: the multicanonical weight
 // recursion (arrays indexed k - kmin; ihist zeroed by the update).
 void muca_update(int kmin, int kmax, double ebin, double beta, int* ihist, double* xhist,

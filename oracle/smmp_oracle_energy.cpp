@@ -360,36 +360,33 @@ double Smmp::enyshe(int nml) {
   return eysm;
 }
 
-// enysol.f:13-339: solvation energy from the numerical SASA (point test).
-double Smmp::enysol(int nmol) {
-  eyslh = eyslp = 0.0;
-  int nrslow, nrshi;
-  if (nmol == 0) {
-    nrslow = irsml1[1];
-    nrshi = irsml2[ntlml];
-  } else {
-    nrslow = irsml1[nmol];
-    nrshi = irsml2[nmol];
-  }
-  int nlow = iatrs1[nrslow], nup = iatrs2[nrshi];
-  for (int i = nrslow; i <= nrshi; ++i) surfres[i] = 0.0;
-  int numat = nup - nlow + 1;
-  asa = vdvol = eysl = 0.0;
-  double avr_x = xat(nlow), avr_y = yat(nlow), avr_z = zat(nlow);
-  double xmin = xat(nlow), ymin = yat(nlow), zmin = zat(nlow);
+// enysol.f:107-330 over the spheres 1..numat (1-based arrays; x[1] is the
+// first sphere): cubic boxes of the largest diameter, each sphere tested
+// against the spheres of its own and the 26 adjacent boxes, then the npnt
+// unit-sphere points scaled to its radius counted as exposed when outside
+// every neighbour.  Spheres with radius <= 0 take no part.  per_atom(k, area,
+// icount) is called for each sphere in the reference's box order; asa and
+// vdvol are summed in that order.
+void enysol_spheres(int numat, const double* x, const double* y, const double* z,
+                    const double* rv, const double* spoint, int npnt, double& asa, double& vdvol,
+                    const std::function<void(int, double, int)>& per_atom) {
+  asa = vdvol = 0.0;
+  if (numat <= 0) return;
+  double avr_x = x[1], avr_y = y[1], avr_z = z[1];
+  double xmin = x[1], ymin = y[1], zmin = z[1];
   double xmax = xmin, ymax = ymin, zmax = zmin;
-  double rmax = rvdw[nlow];
-  for (int j = nlow + 1; j <= nup; ++j) {
-    if (xat(j) <= xmin) xmin = xat(j);
-    else if (xat(j) >= xmax) xmax = xat(j);
-    avr_x = avr_x + xat(j);
-    if (yat(j) <= ymin) ymin = yat(j);
-    else if (yat(j) >= ymax) ymax = yat(j);
-    avr_y = avr_y + yat(j);
-    if (zat(j) <= zmin) zmin = zat(j);
-    else if (zat(j) >= zmax) zmax = zat(j);
-    avr_z = avr_z + zat(j);
-    if (rvdw[j] >= rmax) rmax = rvdw[j];
+  double rmax = rv[1];
+  for (int j = 2; j <= numat; ++j) {
+    if (x[j] <= xmin) xmin = x[j];
+    else if (x[j] >= xmax) xmax = x[j];
+    avr_x = avr_x + x[j];
+    if (y[j] <= ymin) ymin = y[j];
+    else if (y[j] >= ymax) ymax = y[j];
+    avr_y = avr_y + y[j];
+    if (z[j] <= zmin) zmin = z[j];
+    else if (z[j] >= zmax) zmax = z[j];
+    avr_z = avr_z + z[j];
+    if (rv[j] >= rmax) rmax = rv[j];
   }
   avr_x = avr_x / double(numat);
   avr_y = avr_y / double(numat);
@@ -404,24 +401,23 @@ double Smmp::enysol(int nmol) {
   xmin = xmin - shiftx;
   ymin = ymin - shifty;
   zmin = zmin - shiftz;
-  std::vector<int> inbox(ncbox + 2, 0), numbox(nup + 1, 0), indsort(numat + 2, 0);
-  for (int j = nlow; j <= nup; ++j) {
-    int mx = std::min(int(std::max((xat(j) - xmin) / diamax, 0.0)), ndx - 1);
-    int my = std::min(int(std::max((yat(j) - ymin) / diamax, 0.0)), ndy - 1);
-    int mz = std::min(int(std::max((zat(j) - zmin) / diamax, 0.0)), ndz - 1);
+  std::vector<int> inbox(ncbox + 2, 0), numbox(numat + 1, 0), indsort(numat + 2, 0);
+  for (int j = 1; j <= numat; ++j) {
+    int mx = std::min(int(std::max((x[j] - xmin) / diamax, 0.0)), ndx - 1);
+    int my = std::min(int(std::max((y[j] - ymin) / diamax, 0.0)), ndy - 1);
+    int mz = std::min(int(std::max((z[j] - zmin) / diamax, 0.0)), ndz - 1);
     int nboxj = mx + my * ndx + mz * nqxy + 1;
     numbox[j] = nboxj;
     inbox[nboxj] = inbox[nboxj] + 1;
   }
   for (int i = 1; i <= ncbox; ++i) inbox[i + 1] = inbox[i + 1] + inbox[i];
-  for (int i = nlow; i <= nup; ++i) {
+  for (int i = 1; i <= numat; ++i) {
     int j = numbox[i], jj = inbox[j];
     indsort[jj] = i;
     inbox[j] = jj - 1;
   }
   std::vector<int> look(numat + 2);
   std::vector<double> xyz(3 * (numat + 2)), radb2(numat + 2);
-  std::vector<char> surfc(npnt + 1);
   for (int iz = 0; iz <= ndz - 1; ++iz)
     for (int iy = 0; iy <= ndy - 1; ++iy)
       for (int ix = 0; ix <= ndx - 1; ++ix) {
@@ -437,21 +433,21 @@ double Smmp::enysol(int nmol) {
             for (int jx = nsx; jx <= nex; ++jx) {
               int jbox = jx + jy * ndx + jz * nqxy + 1;
               for (int ii = inbox[jbox] + 1; ii <= inbox[jbox + 1]; ++ii)
-                if (rvdw[indsort[ii]] > 0.0) look[jcnt++] = indsort[ii];
+                if (rv[indsort[ii]] > 0.0) look[jcnt++] = indsort[ii];
             }
         for (int ia = inbox[ibox] + 1; ia <= inbox[ibox + 1]; ++ia) {
           int jbi = indsort[ia];
-          double trad = rvdw[jbi];
+          double trad = rv[jbi];
           if (!(trad > 0.0)) continue;
           int nnei = 0;
           for (int ib = 1; ib <= jcnt - 1; ++ib) {
             int jtk = look[ib];
             if (jtk == jbi) continue;
-            double dx = (xat(jbi) - xat(jtk)) / trad;
-            double dy = (yat(jbi) - yat(jtk)) / trad;
-            double dz = (zat(jbi) - zat(jtk)) / trad;
+            double dx = (x[jbi] - x[jtk]) / trad;
+            double dy = (y[jbi] - y[jtk]) / trad;
+            double dz = (z[jbi] - z[jtk]) / trad;
             double dd = dx * dx + dy * dy + dz * dz;
-            double akrad = rvdw[jtk] / trad;
+            double akrad = rv[jtk] / trad;
             double dr = 1.0 + akrad;
             dr = dr * dr;
             if (dd <= dr) {
@@ -468,12 +464,12 @@ double Smmp::enysol(int nmol) {
           int icount = 0;
           double sx = 0.0, sy = 0.0, sz = 0.0;
           for (int il = 1; il <= npnt; ++il) {
-            const double* s = &spoint[(il - 1) * 3];
+            const double* sp = &spoint[(il - 1) * 3];
             bool exposed = true;
             for (int ik = 1; ik <= nnei; ++ik) {
               double sdd = 0.0;
               for (int k = 0; k < 3; ++k) {
-                double t = xyz[3 * ik + k] + s[k];
+                double t = xyz[3 * ik + k] + sp[k];
                 sdd = sdd + t * t;
               }
               if (sdd <= radb2[ik]) {
@@ -481,34 +477,56 @@ double Smmp::enysol(int nmol) {
                 break;
               }
             }
-            surfc[il] = exposed;
             if (exposed) {
               ++icount;
-              sx = sx + s[0];
-              sy = sy + s[1];
-              sz = sz + s[2];
+              sx = sx + sp[0];
+              sy = sy + sp[1];
+              sz = sz + sp[2];
             }
           }
           double sdr = 4.0 * pi * trad * trad / double(npnt);
           double area = sdr * double(icount);
           double volume = sdr / 3.0 *
-                          (trad * double(icount) + (xat(jbi) - avr_x) * sx +
-                           (yat(jbi) - avr_y) * sy + (zat(jbi) - avr_z) * sz);
+                          (trad * double(icount) + (x[jbi] - avr_x) * sx +
+                           (y[jbi] - avr_y) * sy + (z[jbi] - avr_z) * sz);
           asa = asa + area;
           vdvol = vdvol + volume;
-          eysl = eysl + area * sigma[jbi];
-          if (sigma[jbi] < 0) {
-            eyslp = eyslp + area * sigma[jbi];
-            asap = asap + area;
-          }
-          if (sigma[jbi] > 0) {
-            eyslh = eyslh + area * sigma[jbi];
-            asah = asah + area;
-          }
-          int jres = nursat(jbi);
-          surfres[jres] = surfres[jres] + area;
+          per_atom(jbi, area, icount);
         }
       }
+}
+
+// enysol.f:13-339: solvation energy from the numerical SASA (point test) of
+// the atoms of molecule nmol (0: all molecules).
+double Smmp::enysol(int nmol) {
+  eyslh = eyslp = 0.0;
+  int nrslow, nrshi;
+  if (nmol == 0) {
+    nrslow = irsml1[1];
+    nrshi = irsml2[ntlml];
+  } else {
+    nrslow = irsml1[nmol];
+    nrshi = irsml2[nmol];
+  }
+  int nlow = iatrs1[nrslow], nup = iatrs2[nrshi];
+  for (int i = nrslow; i <= nrshi; ++i) surfres[i] = 0.0;
+  eysl = 0.0;
+  const int off = nlow - 1;   // sphere k is atom off + k
+  enysol_spheres(nup - nlow + 1, &xat(off), &yat(off), &zat(off), rvdw.data() + off,
+                 spoint.data(), npnt, asa, vdvol, [&](int k, double area, int) {
+                   const int jbi = off + k;
+                   eysl = eysl + area * sigma[jbi];
+                   if (sigma[jbi] < 0) {
+                     eyslp = eyslp + area * sigma[jbi];
+                     asap = asap + area;
+                   }
+                   if (sigma[jbi] > 0) {
+                     eyslh = eyslh + area * sigma[jbi];
+                     asah = asah + area;
+                   }
+                   int jres = nursat(jbi);
+                   surfres[jres] = surfres[jres] + area;
+                 });
   return eysl;
 }
 

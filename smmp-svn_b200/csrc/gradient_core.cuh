@@ -6,10 +6,12 @@
 // recursion over moving sets gives the same sums (to rounding); which atoms
 // a variable moves is the same set in both (checked on the host topology).
 //
-// Host and device share this arithmetic: a kernel runs the pair loop over
-// threads (forces accumulated with atomics) and one thread per variable for
-// the derivatives; a host build of the same functions is checked against
-// the reference's gradient.
+// Host and device share this arithmetic.  k_gradient (kernels.cu) runs the
+// pair loop over the block's threads (forces accumulated with FP64 atomics)
+// and the force and torque sums of each variable over one warp; a host build
+// of the same functions over the product's topology is checked against the
+// oracle's gradient to 1e-12 of the largest derivative (ECEPP/3, ECEPP/2 and
+// the sigmoidal dielectric).
 #pragma once
 #include <cmath>
 #include <cstdint>

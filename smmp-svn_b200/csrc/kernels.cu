@@ -808,8 +808,8 @@ __device__ double cross_rows(const FFScalars& ff, const DMol& m, const Smem& s, 
 }
 
 // Pair sums of the threads [0, nthr): by rows when the molecule has the row
-// form (kernels built with ROWS), else vdW chunks (8 partners each) and 1-4
-// pairs from the mklist lists.
+// form (kernels built with ROWS), else the dense pair list (the mklist pairs,
+// 1-4 pairs flagged).
 template <bool F32, bool ROWS>
 __device__ void pair_energy(const FFScalars& ff, const DMol& m, const Smem& s, int tid, int nthr,
                             double& el, double& vw, double& hb) {

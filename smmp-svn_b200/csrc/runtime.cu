@@ -156,7 +156,7 @@ DeviceSet::DeviceSet(const std::vector<std::shared_ptr<Molecule>>& mols) {
     }
     // Default pair-work form before any autotuning: rows from about a
     // hundred atoms on (measured: Met-enkephalin, 75 atoms, is faster with
-    // the chunk lists; Ace-Ala40-NMe, 412 atoms, with rows).
+    // the pair lists; Ace-Ala40-NMe, 412 atoms, with rows).
     d.rows = (t.rows_ok && t.natoms >= 128) ? 1 : 0;
     rows_ok_.push_back(t.rows_ok ? 1 : 0);
     dm.push_back(d);
@@ -387,7 +387,7 @@ int Ensemble::set_window(int k) {
 }
 
 // Autotuner: time one sweep of every chain with each pair-work form (0:
-// chunk lists; 1: 32-partner row passes; 2: row passes for molecules of 128
+// pair lists; 1: 32-partner row passes; 2: row passes for molecules of 128
 // atoms or more, lists for the rest), then the row form with speculative
 // windows of 2, 4 and 8 proposals, each from the same saved state (best of
 // three timed sweeps after a warm-up), keep the fastest, and put the state

@@ -40,7 +40,7 @@ class DeviceSet {
   const DMolSet& set() const { return set_; }
   // reserve shared memory for the surrogate's first stage (re-sizes staging)
   void set_da(bool on);
-  // pair-work form of the molecules that allow rows: 0 chunk lists, 1 rows,
+  // pair-work form of the molecules that allow rows: 0 pair lists, 1 rows,
   // -1 the size-based default
   void set_rows(int mode);
   int any_rows_possible() const;
@@ -97,7 +97,7 @@ class Ensemble {
   // device memory must outlive its use here.
   void set_surrogate(const DSurrogate* view, float floor, int min_stage1);
   void da_stats(std::vector<unsigned long long>& n1, std::vector<unsigned long long>& n2) const;
-  // Autotuner: times one sweep of all chains with each pair-work form (0 chunk
+  // Autotuner: times one sweep of all chains with each pair-work form (0 pair
   // lists, 1 row passes, 2 rows for molecules of 128+ atoms) from the same
   // saved state, keeps the fastest and restores the state.  Returns the
   // winner; ms_out[3] the three times.
@@ -108,7 +108,7 @@ class Ensemble {
   int window() const { return dev_->window(); }
   int set_window(int k);
   const double* window_ms() const { return window_ms_; }
-  // pair-work form by hand (as autotune's choice: 0 chunk lists, 1 rows,
+  // pair-work form by hand (as autotune's choice: 0 pair lists, 1 rows,
   // 2 rows for molecules of 128+ atoms)
   void set_pair_work(int form);
   cudaStream_t stream() const { return stream_; }

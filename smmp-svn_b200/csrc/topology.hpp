@@ -8,8 +8,11 @@
 //    variable shifts (setvar.f:40-56), the contiguous atom range that rotates
 //    with it (setmvs.f:168-199, the range before overlaps are removed), and the
 //    torsion-potential constants (enyshe.f:79-80);
-//  * pair work: every (atom, vdW domain) of mklist.f cut into chunks of at
-//    most 8 consecutive partners, and the 1-4 partners as explicit pairs;
+//  * pair work: the dense pair list (every mklist.f pair once, ordered by
+//    listing atom then partner, 1-4 pairs flagged), used by the sweep; and
+//    the same pairs as every (atom, vdW domain) cut into chunks of at most 8
+//    consecutive partners plus the 1-4 partners as explicit pairs, used by
+//    the gradient kernel and the host checks;
 //  * solvation radii and coefficients (init_molecule.f:194-210).
 #pragma once
 #include <cstdint>

@@ -287,10 +287,10 @@ class Ensemble:
         check(lib.smmp_ens_set_surrogate(self._h, surrogate._h if surrogate else None,
                                          float(floor), int(min_stage1)))
 
-    AUTOTUNE_FORMS = ("chunk lists", "rows", "rows for 128+ atoms")
+    AUTOTUNE_FORMS = ("pair lists", "rows", "rows for 128+ atoms")
 
     def autotune(self):
-        """Pick the fastest pair-work decomposition (chunk lists, row passes,
+        """Pick the fastest pair-work decomposition (pair lists, row passes,
         or row passes for molecules of 128 atoms or more) by timing one sweep
         of each from the same saved state; the state is restored.  Returns
         (form, (ms_lists, ms_rows, ms_by_size)), form one of AUTOTUNE_FORMS."""

@@ -6,7 +6,10 @@ Met-enkephalin input decks into tests/golden/smmp_data/, and records the
 reference's published numbers (README and EXAMPLES/annealing.out) with their
 sources in tests/golden/golden.json.
 
-    python tests/golden/make_fixtures.py /root/reference/trunk
+    python tests/golden/make_fixtures.py <SMMP trunk directory>
+
+The argument is the reference's trunk/ directory (the one holding README,
+EXAMPLES/ and SMMP/).
 """
 import json
 import os
@@ -98,4 +101,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/trunk")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_fixtures.py <SMMP trunk directory>")
+    main(sys.argv[1])

@@ -5,13 +5,15 @@
 // coordinates, bond frames and dihedral state, against the oracle's
 // gradient (gradient.f / opeshe.f).
 //
-//   gradient_host_check <libdir/> <seqfile> [varfile]
+//   gradient_host_check <libdir/> <seqfile> [varfile|-] [ecepp2 0|1] [epsd 0|1]
 //
 // Prints the largest difference relative to the largest derivative for six
 // conformations and exits 1 above 1e-12.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
+#include <string>
 #include <vector>
 
 #include "gradient_core.cuh"
@@ -31,13 +33,17 @@ using namespace smmpb200;
 
 int main(int argc, char** argv) {
   if (argc < 3) return 2;
-  const std::string var = argc > 3 ? argv[3] : " ";
-  const ForceField ff = ecepp_forcefield(argv[1], false, false, 0);
-  const ResidueLibrary lib(library_path(argv[1], false));
-  const MolTopo t = build_topology(lib, ff, BuildOptions{}, argv[2], var);
+  const std::string var = (argc > 3 && std::string(argv[3]) != "-") ? argv[3] : " ";
+  const bool sh2 = argc > 4 && std::atoi(argv[4]) != 0;
+  const bool epsd = argc > 5 && std::atoi(argv[5]) != 0;
+  const ForceField ff = ecepp_forcefield(argv[1], sh2, epsd, 0);
+  const ResidueLibrary lib(library_path(argv[1], sh2));
+  BuildOptions opt;
+  opt.sh2 = sh2;
+  const MolTopo t = build_topology(lib, ff, opt, argv[2], var);
   const GradTables tab{ff.pair.a, ff.pair.a14, ff.pair.c, ff.pair.hb, ff.conv, ff.plt, ff.slp,
                        ff.epsd};
-  void* h = orc_create(argv[1], 0, 0, 0);
+  void* h = orc_create(argv[1], sh2 ? 1 : 0, epsd ? 1 : 0, 0);
   if (!h || orc_init_molecule(h, argv[2], var.c_str(), "nh2", "cooh")) return 2;
   const int n = t.natoms, nv = t.nvar;
   std::vector<double> v0(nv);

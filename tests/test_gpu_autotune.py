@@ -1,4 +1,4 @@
-"""The autotuner: it times the pair-work decompositions (chunk lists, rows,
+"""The autotuner: it times the pair-work decompositions (pair lists, rows,
 rows for molecules of 128+ atoms, rows with speculative windows of 2, 4 and 8
 proposals) from a saved state, keeps the fastest, and
 leaves the ensemble's state (variables, energies, random streams, counters)

@@ -44,6 +44,16 @@ def test_gradient_core_enkefa(harness):
     _run(harness, DATA + "enkefa.seq", DATA + "enkefa.var")
 
 
+def test_gradient_core_ecepp2(harness):
+    """ECEPP/2 tables and charges (lib.sh2)."""
+    _run(harness, DATA + "enkefa.seq", DATA + "enkefa.var", "1", "0")
+
+
+def test_gradient_core_sigmoidal_dielectric(harness):
+    """The distance-dependent dielectric (gradient_pair's epsd branch)."""
+    _run(harness, DATA + "enkefa.seq", DATA + "enkefa.var", "0", "1")
+
+
 def test_gradient_core_protein60(harness, tmp_path):
     from smmp.sequences import natural_protein
     _run(harness, seqfile(tmp_path, natural_protein(60), "p60"))
