@@ -126,6 +126,7 @@ MinimizeResult minimize(int imin, std::vector<double>& x, const EnergyGradient& 
   LineSearch ls{fg, x, p, std::vector<double>(n), std::vector<double>(n), r.calls, maxit};
   double g2 = dot(g, g);
   std::vector<double> gprev;
+  double fprev = f;
   int since_restart = 0;
   bool first = true;
   while (g2 > eps && r.calls < maxit && n > 0) {
@@ -161,10 +162,20 @@ MinimizeResult minimize(int imin, std::vector<double>& x, const EnergyGradient& 
     double pmax = 0.0;
     for (size_t k = 0; k < n; ++k) pmax = std::max(pmax, std::fabs(p[k]));
     const double amax = pmax > 0.0 ? 0.5 / pmax : 1.0;
+    // first trial step.  Quasi-Newton: at most a unit gradient step on the
+    // first iteration, then 1.  Conjugate gradients: the step that would
+    // lower the energy by 10 kcal/mol (mincjg.f's expected first decrease,
+    // AMF), then the one that repeats the last decrease; a steep start then
+    // moves by a short step instead of to the line minimum far downhill.
     double a1 = 1.0;
-    if (first) a1 = std::min(1.0, 1.0 / std::sqrt(g2));
+    if (bfgs) {
+      if (first) a1 = std::min(1.0, 1.0 / std::sqrt(g2));
+    } else {
+      a1 = first ? 10.0 / -d0 : std::min(1.0, 2.02 * (f - fprev) / -d0);
+    }
+    if (!(a1 > 0.0)) a1 = 1.0;
     double fnew = f;
-    const double a = wolfe(ls, f, d0, a1, amax, bfgs ? 0.9 : 0.1, fnew);
+    const double a = wolfe(ls, f, d0, a1, amax, bfgs ? 0.9 : 0.3, fnew);
     if (a <= 0.0 || !(fnew <= f)) break;   // no progress
     for (size_t k = 0; k < n; ++k) {
       s[k] = a * p[k];
@@ -191,6 +202,7 @@ MinimizeResult minimize(int imin, std::vector<double>& x, const EnergyGradient& 
       }
     }
     x = ls.xt;
+    fprev = f;
     gprev = g;
     g = gnew;
     f = fnew;
