@@ -457,9 +457,10 @@ __device__ void first_frame(const DMol& m, Smem& s) {
 }
 
 // Eyring step (bldmol.f:175-242): atom i from the frame of its parent ia.
+// The sin and cos of atom i's dihedral wait in its own x and y slots (see
+// full_rebuild); the step reads them, then writes the coordinates there.
 __device__ __forceinline__ void eyring(const DMol& m, Smem& s, int i, int ia) {
-  double st, ct;
-  sincos(s.toat[i], &st, &ct);
+  const double st = s.x[i], ct = s.y[i];
   double ca = m.cba[i], sa = m.sba[i], bl = m.blen[i];
   double x1 = s.fx[3 * ia], x2 = s.fx[3 * ia + 1], x3 = s.fx[3 * ia + 2];
   double z1 = s.fz[3 * ia], z2 = s.fz[3 * ia + 1], z3 = s.fz[3 * ia + 2];
@@ -483,20 +484,29 @@ __device__ __forceinline__ void eyring(const DMol& m, Smem& s, int i, int ia) {
   s.z[i] = s.z[ia] + nx3 * bl;
 }
 
-// Full rebuild of all coordinates from the dihedral state (bldmol.f:13-93):
-// the first frame, then one Eyring step per depth level (each step takes the
-// sin/cos of its own dihedral).
+// Full rebuild of all coordinates from the dihedral state (bldmol.f:13-93).
+// The transcendental work is off the chain of dependent steps: while thread 0
+// sets up the first frame, every thread takes the sin/cos of the dihedrals
+// (parked in the x/y slots of the atoms, none of which is placed yet); then
+// the first warp alone runs one Eyring step per depth level with warp
+// syncs between levels (levels are a few atoms wide: 7 in Met-enkephalin, 12
+// in a 60-residue protein), and the block refreshes the FP32 copies.
 __device__ void full_rebuild(const DMol& m, Smem& s) {
   if (threadIdx.x == 0) first_frame(m, s);
+  for (int k = threadIdx.x; k < m.natoms; k += blockDim.x)
+    if (k != m.i1) sincos(s.toat[k], &s.x[k], &s.y[k]);
   __syncthreads();
-  for (int L = 1; L < m.nlevels; ++L) {
-    int b = m.level_off[L], e = m.level_off[L + 1];
-    for (int k = b + threadIdx.x; k < e; k += blockDim.x) {
-      int a = m.level_atoms[k];
-      eyring(m, s, a, m.iow[a]);
+  if (threadIdx.x < 32) {
+    for (int L = 1; L < m.nlevels; ++L) {
+      const int b = m.level_off[L], e = m.level_off[L + 1];
+      for (int k = b + (int)threadIdx.x; k < e; k += 32) {
+        const int a = m.level_atoms[k];
+        eyring(m, s, a, m.iow[a]);
+      }
+      __syncwarp();
     }
-    __syncthreads();
   }
+  __syncthreads();
   for (int k = threadIdx.x; k < m.natoms; k += blockDim.x) f32_copy(s, k);
   __syncthreads();
 }
@@ -849,6 +859,51 @@ __device__ void pair_energy(const FFScalars& ff, const DMol& m, const Smem& s, i
   el += ff.conv * ke.value() + e64;
   vw += kv.value() + v64;
   hb += kh.value() + h64;
+}
+
+// One pair of the dense list in FP32 for a total: Coulomb (conv folded into
+// the charge product, as in the row form's totals) plus the 12-6 or 12-10
+// term; a pair inside its types' guard distance adds its FP64 term to a64
+// instead and gives 0.
+__device__ __forceinline__ float list_term(const FFScalars& ff, const Smem& s, uint32_t w,
+                                           float convf, double* a64) {
+  const int i = int(w & 0x3fffu), j = int((w >> 14) & 0x3fffu);
+  const bool is14 = (w >> 28) != 0u;
+  const float4 pi = s.p4[i], pj = s.p4[j], li = s.l4[i], lj = s.l4[j];
+  const float dx = (pj.x - pi.x) + (lj.x - li.x);
+  const float dy = (pj.y - pi.y) + (lj.y - li.y);
+  const float dz = (pj.z - pi.z) + (lj.z - li.z);
+  const float r2 = dx * dx + dy * dy + dz * dz;
+  const float4 pr = s.tab4[__float_as_int(li.w) * kTypes + __float_as_int(lj.w)];
+  if (r2 < fabsf(pr.w)) {
+    pair_term_clash(ff, s, i, j, is14, a64);
+    return 0.f;
+  }
+  const float ri = rsqrtf(r2);
+  const float r2i = ri * ri;
+  const float r6i = r2i * r2i * r2i;
+  const float rc = pr.w < 0.f ? r6i * r2i * r2i : r6i;
+  return convf * pi.w * pj.w * ri + ((is14 ? pr.y : pr.x) * r6i * r6i - pr.z * rc);
+}
+
+// Total pair energy (Coulomb + van der Waals + H-bond) of the dense list,
+// this thread's share, FP32 terms in one compensated sum (a proposal of the
+// sweep needs only the total).
+__device__ double pair_total_list(const FFScalars& ff, const DMol& m, const Smem& s, int tid,
+                                  int nthr) {
+  KSum k;
+  double a64[3] = {0.0, 0.0, 0.0};
+  const float convf = (float)ff.conv;
+  const int np = m.npairs;
+  int t = tid;
+  for (; t + nthr < np; t += 2 * nthr) {   // two pairs in flight per thread
+    const float e0 = list_term(ff, s, m.flat[t], convf, a64);
+    const float e1 = list_term(ff, s, m.flat[t + nthr], convf, a64);
+    k.add(e0);
+    k.add(e1);
+  }
+  for (; t < np; t += nthr) k.add(list_term(ff, s, m.flat[t], convf, a64));
+  return ((k.value() + a64[0]) + a64[1]) + a64[2];
 }
 
 // ---------------------------------------------------------------- SASA
@@ -1542,6 +1597,12 @@ __device__ bool grid_barrier(unsigned* bar, unsigned expected, unsigned long lon
   return *flag != 0;
 }
 
+// Barrier of the pair warps 0 .. kWarps-2 of k_sweep (named barrier 1; the
+// last warp does not take part).
+__device__ __forceinline__ void pair_warps_sync() {
+  asm volatile("bar.sync 1, %0;" ::"r"((kWarps - 1) * 32) : "memory");
+}
+
 // Atom t of the set a proposal moves: the subtree [lo, lo+span) or, when
 // `flip`, every other atom.
 __device__ __forceinline__ int moved_atom(int t, int lo, int span, bool flip) {
@@ -1985,14 +2046,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
         ep = fresh_ep;
         __syncthreads();
       }
-      if (incr) {
-        if (warp != spec_warp) xold = cross_rows<F32>(set.f, m, s, kWarps - 1, lo, hi);
-        __syncthreads();
-      }
-      // ---- phase A: rotate the subtree of cur.jv about its bond (+theta)
-      {
+      // ---- phase A: rotate the subtree of cur.jv about its bond (+theta),
+      // by the pair warps alone (they sync among themselves); the last warp,
+      // which reads no coordinates, goes straight on to its phase B work
+      if (warp != spec_warp) {
+        if (incr) {
+          xold = cross_rows<F32>(set.f, m, s, kWarps - 1, lo, hi);
+          pair_warps_sync();
+        }
         const Axis ax = proposal_axis(s, cur, flip);
-        for (int t = threadIdx.x; t < nmoved; t += blockDim.x) {
+        for (int t = threadIdx.x; t < nmoved; t += nthr_pairs) {
           const int k = moved_atom(t, lo, span, flip);
           if (flip && (k == cur.a || k == cur.b)) continue;   // on the axis
           s.bx[k] = s.x[k];
@@ -2001,8 +2064,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
           rotate_point(ax, s.bx[k], s.by[k], s.bz[k], s.x[k], s.y[k], s.z[k]);
           if (F32) f32_copy(s, k);
         }
+        pair_warps_sync();
       }
-      __syncthreads();
       // ---- phase B: pair energy; the last warp replays this proposal's
       // setvar call on the dihedral state and prepares proposal p+1
       if (warp != spec_warp) {
@@ -2011,6 +2074,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
           el = cross_rows<F32>(set.f, m, s, kWarps - 1, lo, hi) - xold;   // the change
         else if (ROWS && m.rows)
           pair_rows<F32, true>(set.f, m, s, kWarps - 1, el, vw, hb);
+        else if (F32 && !set.f.epsd)
+          el = pair_total_list(set.f, m, s, threadIdx.x, nthr_pairs);
         else
           pair_energy<F32, false>(set.f, m, s, threadIdx.x, nthr_pairs, el, vw, hb);
         if (sasa)
