@@ -581,7 +581,7 @@ __device__ __forceinline__ void pair32(const FFScalars& ff, const Smem& s, int i
   float dy = (pj.y - pi.y) + (lj.y - li.y);
   float dz = (pj.z - pi.z) + (lj.z - li.z);
   float r2 = dx * dx + dy * dy + dz * dz;
-  const float4 pr = s.tab4[s.type[i] * kTypes + s.type[j]];
+  const float4 pr = s.tab4[__float_as_int(li.w) * kTypes + __float_as_int(lj.w)];
   if (r2 < fabsf(pr.w)) {
     double e, v, h;
     e = v = h = 0.0;
@@ -859,51 +859,6 @@ __device__ void pair_energy(const FFScalars& ff, const DMol& m, const Smem& s, i
   el += ff.conv * ke.value() + e64;
   vw += kv.value() + v64;
   hb += kh.value() + h64;
-}
-
-// One pair of the dense list in FP32 for a total: Coulomb (conv folded into
-// the charge product, as in the row form's totals) plus the 12-6 or 12-10
-// term; a pair inside its types' guard distance adds its FP64 term to a64
-// instead and gives 0.
-__device__ __forceinline__ float list_term(const FFScalars& ff, const Smem& s, uint32_t w,
-                                           float convf, double* a64) {
-  const int i = int(w & 0x3fffu), j = int((w >> 14) & 0x3fffu);
-  const bool is14 = (w >> 28) != 0u;
-  const float4 pi = s.p4[i], pj = s.p4[j], li = s.l4[i], lj = s.l4[j];
-  const float dx = (pj.x - pi.x) + (lj.x - li.x);
-  const float dy = (pj.y - pi.y) + (lj.y - li.y);
-  const float dz = (pj.z - pi.z) + (lj.z - li.z);
-  const float r2 = dx * dx + dy * dy + dz * dz;
-  const float4 pr = s.tab4[__float_as_int(li.w) * kTypes + __float_as_int(lj.w)];
-  if (r2 < fabsf(pr.w)) {
-    pair_term_clash(ff, s, i, j, is14, a64);
-    return 0.f;
-  }
-  const float ri = rsqrtf(r2);
-  const float r2i = ri * ri;
-  const float r6i = r2i * r2i * r2i;
-  const float rc = pr.w < 0.f ? r6i * r2i * r2i : r6i;
-  return convf * pi.w * pj.w * ri + ((is14 ? pr.y : pr.x) * r6i * r6i - pr.z * rc);
-}
-
-// Total pair energy (Coulomb + van der Waals + H-bond) of the dense list,
-// this thread's share, FP32 terms in one compensated sum (a proposal of the
-// sweep needs only the total).
-__device__ double pair_total_list(const FFScalars& ff, const DMol& m, const Smem& s, int tid,
-                                  int nthr) {
-  KSum k;
-  double a64[3] = {0.0, 0.0, 0.0};
-  const float convf = (float)ff.conv;
-  const int np = m.npairs;
-  int t = tid;
-  for (; t + nthr < np; t += 2 * nthr) {   // two pairs in flight per thread
-    const float e0 = list_term(ff, s, m.flat[t], convf, a64);
-    const float e1 = list_term(ff, s, m.flat[t + nthr], convf, a64);
-    k.add(e0);
-    k.add(e1);
-  }
-  for (; t < np; t += nthr) k.add(list_term(ff, s, m.flat[t], convf, a64));
-  return ((k.value() + a64[0]) + a64[1]) + a64[2];
 }
 
 // ---------------------------------------------------------------- SASA
@@ -2074,8 +2029,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
           el = cross_rows<F32>(set.f, m, s, kWarps - 1, lo, hi) - xold;   // the change
         else if (ROWS && m.rows)
           pair_rows<F32, true>(set.f, m, s, kWarps - 1, el, vw, hb);
-        else if (F32 && !set.f.epsd)
-          el = pair_total_list(set.f, m, s, threadIdx.x, nthr_pairs);
         else
           pair_energy<F32, false>(set.f, m, s, threadIdx.x, nthr_pairs, el, vw, hb);
         if (sasa)
