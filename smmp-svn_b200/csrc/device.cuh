@@ -165,6 +165,8 @@ struct DPTFused {
   unsigned long long timeout_ns;   // a barrier wait longer than this sets kErrTimeout
   unsigned extra;              // arrivals beyond the launch's blocks (0; >0 only in tests:
                                // the barrier then never opens and every wait runs out)
+  int master;                  // 1: the launch's last block runs no chain but the
+                               // exchanges (set by the launcher)
 };
 
 enum SweepFlags : int {

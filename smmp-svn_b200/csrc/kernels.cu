@@ -116,6 +116,7 @@ struct Scalars {
   int refill;
   int hlo, hhi;          // heavy-atom indices of the proposal's subtree range
   int gsync;             // result of the last grid barrier
+  unsigned gen;          // barrier generation seen at the last grid_arrive
   int wn;                // proposals of the current speculative window
 };
 
@@ -1460,17 +1461,24 @@ __global__ void __launch_bounds__(kThreads, 1) k_gradient(DMolSet set, DChains c
 // (shared or global memory, used by this warp only); `lq` receives the logs
 // the refill computes.  Energies are read past L1: in the fused sweep other
 // blocks wrote them.
+// Pairs of an exchange step of parity sw: i = nu, nu+2, ..., num_rep1
+// (1-based); i == n is the wrap pair.
+__device__ __forceinline__ int exchange_pairs(int n, int sw, int wrap) {
+  const int num_rep1 = sw == 1 ? n - 1 : n, nu = sw == 1 ? 1 : 2;
+  int npairs = 0;
+  for (int i = nu; i <= num_rep1; i += 2)
+    if (i != n || wrap) ++npairs;
+  return npairs;
+}
+
 __device__ void exchange_core(const DChains& ch, int* temp_chain, const double* betas, int n,
                               uint32_t* slot, double* lq, int* iswitch, int wrap,
                               unsigned long long* stats) {
   const int lane = threadIdx.x & 31;
   if (n > 1) {
     const int sw = *iswitch;
-    const int num_rep1 = sw == 1 ? n - 1 : n, nu = sw == 1 ? 1 : 2;
-    // pairs i = nu, nu+2, ..., num_rep1 (1-based); i == n is the wrap pair
-    int npairs = 0;
-    for (int i = nu; i <= num_rep1; i += 2)
-      if (i != n || wrap) ++npairs;
+    const int nu = sw == 1 ? 1 : 2;
+    const int npairs = exchange_pairs(n, sw, wrap);
     uint32_t head = slot[kQHead];
     for (int base = 0; base < npairs; base += 32) {
       const int cnt = min(32, npairs - base);
@@ -1542,7 +1550,7 @@ __device__ bool grid_barrier(unsigned* bar, unsigned expected, unsigned long lon
           if (*err == 0) *err = kErrTimeout;
           break;
         }
-        __nanosleep(256);
+        __nanosleep(64);
       }
     }
     __threadfence();
@@ -1556,6 +1564,96 @@ __device__ bool grid_barrier(unsigned* bar, unsigned expected, unsigned long lon
 // last warp does not take part).
 __device__ __forceinline__ void pair_warps_sync() {
   asm volatile("bar.sync 1, %0;" ::"r"((kWarps - 1) * 32) : "memory");
+}
+
+// The same barrier in two halves: grid_arrive counts this block in and
+// returns the generation it saw (the barrier opens when the count reaches
+// `expected`); grid_wait waits, bounded as above, for the generation to move
+// on.  The block may work in between.
+// With release false the block whose arrival completes the count leaves the
+// barrier shut: the master block of the fused exchange opens it.
+__device__ unsigned grid_arrive(unsigned* bar, unsigned expected, bool release,
+                                unsigned* gen_seen) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    volatile unsigned* gen = bar + 1;
+    const unsigned g = *gen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(bar, 1u) + 1u;
+    if (release && arrived == expected) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    }
+    *gen_seen = g;
+  }
+  __syncthreads();
+  return *gen_seen;
+}
+__device__ bool grid_wait(unsigned* bar, unsigned g, unsigned long long timeout_ns, int* err,
+                          int* flag) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    volatile unsigned* gen = bar + 1;
+    const unsigned long long t0 = global_ns();
+    while (*gen == g) {
+      if (global_ns() - t0 > timeout_ns) {
+        ok = 0;
+        if (*err == 0) *err = kErrTimeout;
+        break;
+      }
+      __nanosleep(64);
+    }
+    __threadfence();
+    *flag = ok;
+  }
+  __syncthreads();
+  return *flag != 0;
+}
+
+// The master block of a fused parallel-tempering launch (the launch's extra
+// last block, on an SM no chain uses): for each of the nsweeps rounds it
+// waits, bounded, until all `expected` chains have arrived, runs the
+// exchange with its first warp, shuts the count and opens the barrier; then
+// it tops up the exchange stream's queue for the next round while the
+// chains sweep.  It alone touches the exchange stream during the launch.  A
+// wait that runs out ends it (the chains' own waits then run out too and
+// record the timeout).
+__device__ void pt_master(const DChains& ch, const DPTFused& pt, int nsweeps, unsigned expected) {
+  if (threadIdx.x >= 32) return;
+  const int lane = threadIdx.x;
+  volatile unsigned* cnt = pt.bar;
+  for (int r = 0; r < nsweeps; ++r) {
+    int ok = 1;
+    if (lane == 0) {
+      const unsigned long long t0 = global_ns();
+      while (*cnt != expected) {
+        if (global_ns() - t0 > pt.timeout_ns) {
+          ok = 0;
+          break;
+        }
+        __nanosleep(32);
+      }
+      __threadfence();
+    }
+    if (!__shfl_sync(0xffffffffu, ok, 0)) return;
+    exchange_core(ch, pt.temp_chain, pt.betas, pt.n, pt.mt, pt.lq, pt.iswitch, pt.wrap, pt.stats);
+    if (lane == 0) {
+      atomicExch(pt.bar, 0u);
+      __threadfence();
+      atomicAdd(pt.bar + 1, 1u);
+    }
+    __syncwarp();
+    // the refill the next exchange would start with, done now (the same
+    // values at the same points of the stream)
+    if (r + 1 < nsweeps && pt.n > 1) {
+      const int need = min(32, exchange_pairs(pt.n, *pt.iswitch, pt.wrap));
+      while ((int)(pt.mt[kQTail] - pt.mt[kQHead]) < need) rng_refill_warp(pt.mt, pt.lq);
+    }
+    __syncwarp();
+  }
 }
 
 // Atom t of the set a proposal moves: the subtree [lo, lo+span) or, when
@@ -1870,6 +1968,10 @@ template <bool F32, bool ROWS, bool SASA>
 __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, DWeight w, int first,
                                                        int nsweeps, int flags, double check_tol,
                                                        DPTFused pt) {
+  if (pt.on && pt.master && blockIdx.x == gridDim.x - 1) {
+    pt_master(ch, pt, nsweeps, gridDim.x - 1 + pt.extra);
+    return;
+  }
   const int c = first + blockIdx.x;
   const bool sasa = SASA;
   const bool rndord = (flags & kFlagRndOrd) != 0;
@@ -1907,8 +2009,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
   // and setvar is not idempotent to the last bit, so it is the opening
   // evaluation that the trajectory must start from.
   bool check_pending = false;
-
-  for (int sw = 0; sw < nsweeps; ++sw) {
+  // The opening energy() of a sweep reads nothing of the temperature, so with
+  // the fused exchange it is evaluated while the chain waits for the other
+  // chains to arrive at the exchange (opened: done ahead).
+  bool opened = false;
+  auto opening = [&]() {
     if (flags & kFlagExtraSetvar) {   // partem_s.f:194-198: setvar(i, vlvr) first
       setvar_all(m, s);
       __syncthreads();
@@ -1921,13 +2026,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
     full_rebuild(m, s);
     evaluate_block<F32, ROWS, SASA>(set.f, m, s, err);
     __syncthreads();
-    {
-      double sum[5];
-      all_sums(s, sum);
-      enew = total_of(sum);
-      etor = sum[3];
-      ep = (sum[0] + sum[1]) + sum[2];
-    }
+    double sum[5];
+    all_sums(s, sum);
+    enew = total_of(sum);
+    etor = sum[3];
+    ep = (sum[0] + sum[1]) + sum[2];
+  };
+
+  for (int sw = 0; sw < nsweeps; ++sw) {
+    if (!opened) opening();
+    opened = false;
     if (check_pending && threadIdx.x == 0 && !(flags & kFlagNoCheck) &&
         fabs(eol - enew) > check_tol && eol < 100000.0)
       set_err(err, kErrConsistency);
@@ -2140,14 +2248,25 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       check_pending = true;
     }
     if (pt.on) {
-      // fused parallel tempering: every chain's energy is in place, block 0's
-      // first warp exchanges, then every chain takes up its new temperature
+      // fused parallel tempering: every chain's energy is in place, the
+      // exchange runs (in the master block, or else in block 0's first warp
+      // between two barriers), then every chain takes up its new
+      // temperature; between its arrival and its wait, a chain evaluates the
+      // opening energy of its next sweep
       if (threadIdx.x == 0) ch.eol[c] = eol;
-      if (!grid_barrier(pt.bar, gridDim.x + pt.extra, pt.timeout_ns, err, &sc.gsync)) break;
-      if (blockIdx.x == 0 && warp == 0)
-        exchange_core(ch, pt.temp_chain, pt.betas, pt.n, pt.mt, pt.lq, pt.iswitch, pt.wrap,
-                      pt.stats);
-      if (!grid_barrier(pt.bar, gridDim.x + pt.extra, pt.timeout_ns, err, &sc.gsync)) break;
+      const unsigned nchain = gridDim.x - (pt.master ? 1u : 0u) + pt.extra;
+      const unsigned gen = grid_arrive(pt.bar, nchain, !pt.master, &sc.gen);
+      if (sw + 1 < nsweeps) {
+        opening();
+        opened = true;
+      }
+      if (!grid_wait(pt.bar, gen, pt.timeout_ns, err, &sc.gsync)) break;
+      if (!pt.master) {
+        if (blockIdx.x == 0 && warp == 0)
+          exchange_core(ch, pt.temp_chain, pt.betas, pt.n, pt.mt, pt.lq, pt.iswitch, pt.wrap,
+                        pt.stats);
+        if (!grid_barrier(pt.bar, nchain, pt.timeout_ns, err, &sc.gsync)) break;
+      }
       beta = __ldcg(&ch.beta[c]);
     }
   }
@@ -2659,9 +2778,11 @@ static cudaError_t launch_sweep_pt_t(DMolSet set, DChains ch, DWeight w, int cou
     return e;
   if (!coop) return cudaErrorNotSupported;
   if ((long long)per * nsm < count) return cudaErrorCooperativeLaunchTooLarge;
+  // one more block, when it fits, to run the exchanges (pt_master)
+  pt.master = (long long)per * nsm >= (long long)count + 1 ? 1 : 0;
   int first = 0;
   void* args[] = {&set, &ch, &w, &first, &nsweeps, &flags, &check_tol, &pt};
-  return cudaLaunchCooperativeKernel(fn, dim3(count), dim3(kThreads), args, sm, st);
+  return cudaLaunchCooperativeKernel(fn, dim3(count + pt.master), dim3(kThreads), args, sm, st);
 }
 
 static int variant(const DMolSet& set, bool fp32) {
