@@ -28,6 +28,7 @@ struct DMol {
   int natoms, nvar, nfree, nchunks, n14, nheavy, nlevels, nres, nsib;
   int i1, i2, i3;
   double gbpr[6];
+  double ag[9];        // global axes of the first frame from gbpr[3..5], [row * 3 + col]
   const int* iow;
   const uint8_t* type;
   const double* charge;

@@ -408,26 +408,17 @@ __device__ void torsion_all(const DMol& m, Smem& s) {
 }
 
 // ---------------------------------------------------------------- rebuild
-// Frame of the first backbone atom from the global parameters (setgbl,
-// bldmol.f:303-420).  Single thread.
+// Frame of the first backbone atom (setgbl, bldmol.f:303-420) from the
+// molecule's global axes (m.ag) and the dihedrals of i2 and i3, whose sin
+// and cos wait in the x/y slots of those atoms (full_rebuild).  Single
+// thread.
 __device__ void first_frame(const DMol& m, Smem& s) {
-  int i1 = m.i1, i2 = m.i2, i3 = m.i3;
-  double ca = cos(m.gbpr[3]), sa = sin(m.gbpr[3]);
-  double cb = cos(m.gbpr[4]), sb = sin(m.gbpr[4]);
-  double cg = cos(m.gbpr[5]), sg = sin(m.gbpr[5]);
+  const int i1 = m.i1, i2 = m.i2, i3 = m.i3;
   double ag[3][3];
-  double x1 = ca * cg - sa * sb * sg, x2 = sa * cg + ca * sb * sg, x3 = -cb * sg;
-  double d = sqrt(x1 * x1 + x2 * x2 + x3 * x3);
-  ag[0][0] = x1 / d; ag[1][0] = x2 / d; ag[2][0] = x3 / d;
-  double y1 = -sa * cb, y2 = ca * cb, y3 = sb;
-  d = sqrt(y1 * y1 + y2 * y2 + y3 * y3);
-  ag[0][1] = y1 / d; ag[1][1] = y2 / d; ag[2][1] = y3 / d;
-  double z1 = ca * sg + sa * sb * cg, z2 = sa * sg - ca * sb * cg, z3 = cb * cg;
-  d = sqrt(z1 * z1 + z2 * z2 + z3 * z3);
-  ag[0][2] = z1 / d; ag[1][2] = z2 / d; ag[2][2] = z3 / d;
-  double st2, ct2, st3, ct3;
-  sincos(s.toat[i2], &st2, &ct2);
-  sincos(s.toat[i3], &st3, &ct3);
+  for (int r = 0; r < 3; ++r)
+    for (int q = 0; q < 3; ++q) ag[r][q] = m.ag[r * 3 + q];
+  const double st2 = s.x[i2], ct2 = s.y[i2], st3 = s.x[i3], ct3 = s.y[i3];
+  double x1, x2, x3, y1, y3, z1, z2, z3;
   double sa2 = m.sba[i2];
   x1 = -m.cba[i2];
   x2 = -sa2 * ct2;
@@ -460,9 +451,11 @@ __device__ void first_frame(const DMol& m, Smem& s) {
 // Eyring step (bldmol.f:175-242): atom i from the frame of its parent ia.
 // The sin and cos of atom i's dihedral wait in its own x and y slots (see
 // full_rebuild); the step reads them, then writes the coordinates there.
-__device__ __forceinline__ void eyring(const DMol& m, Smem& s, int i, int ia) {
+__device__ __forceinline__ void eyring(const double* __restrict__ cba,
+                                       const double* __restrict__ sba,
+                                       const double* __restrict__ blen, Smem& s, int i, int ia) {
   const double st = s.x[i], ct = s.y[i];
-  double ca = m.cba[i], sa = m.sba[i], bl = m.blen[i];
+  double ca = cba[i], sa = sba[i], bl = blen[i];
   double x1 = s.fx[3 * ia], x2 = s.fx[3 * ia + 1], x3 = s.fx[3 * ia + 2];
   double z1 = s.fz[3 * ia], z2 = s.fz[3 * ia + 1], z3 = s.fz[3 * ia + 2];
   double y1 = z2 * x3 - z3 * x2, y2 = z3 * x1 - z1 * x3, y3 = z1 * x2 - z2 * x1;
@@ -493,16 +486,27 @@ __device__ __forceinline__ void eyring(const DMol& m, Smem& s, int i, int ia) {
 // syncs between levels (levels are a few atoms wide: 7 in Met-enkephalin, 12
 // in a 60-residue protein), and the block refreshes the FP32 copies.
 __device__ void full_rebuild(const DMol& m, Smem& s) {
-  if (threadIdx.x == 0) first_frame(m, s);
-  for (int k = threadIdx.x; k < m.natoms; k += blockDim.x)
-    if (k != m.i1) sincos(s.toat[k], &s.x[k], &s.y[k]);
+  // the molecule's arrays in registers before the first shared store
+  const int* __restrict__ lvl_off = m.level_off;
+  const int* __restrict__ lvl_at = m.level_atoms;
+  const int* __restrict__ iow = m.iow;
+  const double* __restrict__ cba = m.cba;
+  const double* __restrict__ sba = m.sba;
+  const double* __restrict__ blen = m.blen;
+  const int nlev = m.nlevels, n = m.natoms, i1 = m.i1;
+  for (int k = threadIdx.x; k < n; k += blockDim.x)
+    if (k != i1) sincos(s.toat[k], &s.x[k], &s.y[k]);
   __syncthreads();
   if (threadIdx.x < 32) {
-    for (int L = 1; L < m.nlevels; ++L) {
-      const int b = m.level_off[L], e = m.level_off[L + 1];
+    if (threadIdx.x == 0) first_frame(m, s);
+    __syncwarp();
+    int e = lvl_off[1];
+    for (int L = 1; L < nlev; ++L) {
+      const int b = e;
+      e = lvl_off[L + 1];
       for (int k = b + (int)threadIdx.x; k < e; k += 32) {
-        const int a = m.level_atoms[k];
-        eyring(m, s, a, m.iow[a]);
+        const int a = lvl_at[k];
+        eyring(cba, sba, blen, s, a, iow[a]);
       }
       __syncwarp();
     }

@@ -2,6 +2,7 @@
 #include "runtime.hpp"
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <numeric>
 #include <stdexcept>
@@ -11,6 +12,30 @@
 #include "molbuild.hpp"
 
 namespace smmpb200 {
+
+// The part of the first frame (setgbl, bldmol.f:303-420) that depends only
+// on the molecule's global angles gbpr[3..5]: three normalised axes, column
+// c of ag[r * 3 + c].  A constant of the molecule, so computed here once.
+static void global_axes(const double* gbpr, double* ag) {
+  const double ca = std::cos(gbpr[3]), sa = std::sin(gbpr[3]);
+  const double cb = std::cos(gbpr[4]), sb = std::sin(gbpr[4]);
+  const double cg = std::cos(gbpr[5]), sg = std::sin(gbpr[5]);
+  const double x1 = ca * cg - sa * sb * sg, x2 = sa * cg + ca * sb * sg, x3 = -cb * sg;
+  double d = std::sqrt(x1 * x1 + x2 * x2 + x3 * x3);
+  ag[0] = x1 / d;
+  ag[3] = x2 / d;
+  ag[6] = x3 / d;
+  const double y1 = -sa * cb, y2 = ca * cb, y3 = sb;
+  d = std::sqrt(y1 * y1 + y2 * y2 + y3 * y3);
+  ag[1] = y1 / d;
+  ag[4] = y2 / d;
+  ag[7] = y3 / d;
+  const double z1 = ca * sg + sa * sb * cg, z2 = sa * sg - ca * sb * cg, z3 = cb * cg;
+  d = std::sqrt(z1 * z1 + z2 * z2 + z3 * z3);
+  ag[2] = z1 / d;
+  ag[5] = z2 / d;
+  ag[8] = z3 / d;
+}
 
 void check_cuda(cudaError_t e, const char* what) {
   if (e != cudaSuccess)
@@ -119,6 +144,7 @@ DeviceSet::DeviceSet(const std::vector<std::shared_ptr<Molecule>>& mols) {
     d.i2 = t.i2;
     d.i3 = t.i3;
     for (int k = 0; k < 6; ++k) d.gbpr[k] = t.gbpr[k];
+    global_axes(t.gbpr, d.ag);
     d.iow = upload(t.iow);
     d.type = upload(t.type);
     d.charge = upload(t.charge);
