@@ -62,6 +62,12 @@ struct DMol {
   int npairs;                            // pair terms of a full evaluation
   const uint32_t* flat;                  // every pair once: i | j<<14 | is14<<28
   const int* var_cross;                  // pair terms across each variable's bond
+  // pairs each free variable's turn changes, as indices into flat (CSR by
+  // variable; cache = 0 when the molecule has none: over 65,535 pairs)
+  const int* cross_off;
+  const uint16_t* cross_idx;
+  int ncross, cross_max;
+  int cache;
 };
 
 // Force field constants read by every chain (copied to shared memory).
@@ -89,6 +95,8 @@ struct DMolSet {
   int any_rows;              // 1: some molecule evaluates its pairs by rows
   int da;                    // 1: shared memory for the surrogate's first stage
   int window;                // proposals per speculative window (<= 1: one at a time)
+  int cache_pairs;           // > 0: shared memory for the cached pair terms of this many
+  int cache_cross;           //      pairs and the new terms of this many crossing pairs
   const DForceField* ff;     // device
   FFScalars f;
 };

@@ -157,6 +157,8 @@ struct Smem {
   float4 *wp4, *wl4;
   double* wred;
   Proposal* wprop;
+  float* ecache;         // cached FP32 pair terms of the state, one per pair of the dense list
+  float* tnew;           // the proposal's new terms of its crossing pairs
   DMol* mol;
   char* pool;            // staged topology (see stage_mol)
 };
@@ -164,7 +166,7 @@ struct Smem {
 __host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~size_t(15); }
 
 __host__ __device__ inline size_t smem_layout(int n, int v, int npnt, bool sasa, bool da, int win,
-                                              Smem* s, char* base) {
+                                              int cpairs, int ccross, Smem* s, char* base) {
   size_t off = 0;
   auto take = [&](size_t bytes) -> char* {
     char* p = base ? base + off : nullptr;
@@ -225,6 +227,8 @@ __host__ __device__ inline size_t smem_layout(int n, int v, int npnt, bool sasa,
   t.wl4 = (float4*)take(16 * wn);
   t.wred = (double*)take(win >= 2 ? 8 * kWarps * kMaxWindow : 8);
   t.wprop = (Proposal*)take(win >= 2 ? sizeof(Proposal) * 2 * kMaxWindow : 16);
+  t.ecache = (float*)take(cpairs > 0 ? 4 * (size_t)cpairs : 4);
+  t.tnew = (float*)take(ccross > 0 ? 4 * (size_t)ccross : 4);
   t.sc = (Scalars*)take(sizeof(Scalars));
   t.mol = (DMol*)take(sizeof(DMol));
   t.pool = take(0);
@@ -236,7 +240,7 @@ __device__ Smem carve(const DMolSet& set, bool sasa) {
   extern __shared__ __align__(16) char smem_raw[];
   Smem s;
   smem_layout(set.max_atoms, set.max_vars, set.f.npnt, sasa, set.da != 0, sasa ? 0 : set.window,
-              &s, smem_raw);
+              sasa ? 0 : set.cache_pairs, sasa ? 0 : set.cache_cross, &s, smem_raw);
   return s;
 }
 
@@ -244,7 +248,8 @@ __device__ Smem carve(const DMolSet& set, bool sasa) {
 // array, in the order stage_mol copies them (host sizing and device staging
 // must agree exactly).
 __host__ __device__ inline size_t stage_size(int natoms, int nvar, int nsib, int nlevels, int nfree,
-                                             int nflat, int nheavy, bool rows, bool lists) {
+                                             int nflat, int nheavy, bool rows, bool lists,
+                                             int ncross) {
   size_t b = 0;
   auto a = [&](size_t elem, int n) { b += align16(elem * (size_t)(n > 0 ? n : 1)); };
   a(4, nvar);          // var_atom
@@ -271,7 +276,13 @@ __host__ __device__ inline size_t stage_size(int natoms, int nvar, int nsib, int
   a(8, natoms);        // blen
   a(8, natoms);        // cba
   a(8, natoms);        // sba
-  if (lists) a(4, nflat);   // flat pair list
+  if (lists) {
+    a(4, nflat);   // flat pair list
+    if (ncross > 0) {
+      a(4, nvar + 1);   // cross_off
+      a(2, ncross);     // cross_idx
+    }
+  }
   return b;
 }
 
@@ -335,7 +346,13 @@ __device__ const DMol& stage_mol(const DMolSet& set, const DChains& ch, int c, S
   m.blen = stage_array(g.blen, g.natoms, pool, end, ok);
   m.cba = stage_array(g.cba, g.natoms, pool, end, ok);
   m.sba = stage_array(g.sba, g.natoms, pool, end, ok);
-  if (set.stage_lists) m.flat = stage_array(g.flat, g.npairs, pool, end, ok);
+  if (set.stage_lists) {
+    m.flat = stage_array(g.flat, g.npairs, pool, end, ok);
+    if (set.cache_pairs > 0 && g.cache) {
+      m.cross_off = stage_array(g.cross_off, g.nvar + 1, pool, end, ok);
+      m.cross_idx = stage_array(g.cross_idx, g.ncross, pool, end, ok);
+    }
+  }
   __syncthreads();
   if (threadIdx.x == 0) *s.mol = m;
   __syncthreads();
@@ -864,6 +881,82 @@ __device__ void pair_energy(const FFScalars& ff, const DMol& m, const Smem& s, i
   el += ff.conv * ke.value() + e64;
   vw += kv.value() + v64;
   hb += kh.value() + h64;
+}
+
+// ---------------------------------------------------------------- cached pair terms
+// For molecules with per-variable crossing lists (m.cache), a sweep keeps
+// the FP32 total term of every pair of the state in s.ecache, filled after
+// each opening energy().  A proposal then evaluates only the pairs its turn
+// changes and sums (new - cached) for the change of the pair energy; an
+// accepted proposal writes its new terms into the cache.  A pair closer than
+// its types' guard distance is summed in FP64 (as everywhere in the FP32
+// mode) and makes the cache unusable once such a pair enters the state (the
+// rest of the sweep then sums every pair in full, as without the cache).
+
+// Total term of pair word w from the FP32 copies: Coulomb (conv folded into
+// the charge product) plus the 12-6 or 12-10 term.  Returns true for a pair
+// inside its guard distance, whose FP64 total is then in t64.
+__device__ __forceinline__ bool cache_term(const FFScalars& ff, const Smem& s, uint32_t w,
+                                           float convf, float& term, double& t64) {
+  const int i = int(w & 0x3fffu), j = int((w >> 14) & 0x3fffu);
+  const bool is14 = (w >> 28) != 0u;
+  const float4 pi = s.p4[i], pj = s.p4[j], li = s.l4[i], lj = s.l4[j];
+  const float dx = (pj.x - pi.x) + (lj.x - li.x);
+  const float dy = (pj.y - pi.y) + (lj.y - li.y);
+  const float dz = (pj.z - pi.z) + (lj.z - li.z);
+  const float r2 = dx * dx + dy * dy + dz * dz;
+  const float4 pr = s.tab4[__float_as_int(li.w) * kTypes + __float_as_int(lj.w)];
+  if (r2 < fabsf(pr.w)) {
+    double e = 0.0, v = 0.0, h = 0.0;
+    pair_term<false>(ff, s, i, j, is14, e, v, h);
+    t64 = (e + v) + h;
+    term = 0.f;
+    return true;
+  }
+  const float ri = rsqrtf(r2);
+  const float r2i = ri * ri;
+  const float r6i = r2i * r2i * r2i;
+  const float rc = pr.w < 0.f ? r6i * r2i * r2i : r6i;
+  term = convf * pi.w * pj.w * ri + ((is14 ? pr.y : pr.x) * r6i * r6i - pr.z * rc);
+  return false;
+}
+
+// Fill the cache from the current coordinates (whole block); returns, in
+// every thread, whether some pair of the state is inside its guard distance.
+__device__ bool fill_pair_cache(const FFScalars& ff, const DMol& m, Smem& s) {
+  const float convf = (float)ff.conv;
+  int clash = 0;
+  for (int t = threadIdx.x; t < m.npairs; t += blockDim.x) {
+    float term;
+    double t64;
+    if (cache_term(ff, s, m.flat[t], convf, term, t64)) clash = 1;
+    s.ecache[t] = term;
+  }
+  return __syncthreads_or(clash) != 0;
+}
+
+// The proposal's change of the pair energy over the crossing pairs of
+// variable v, this thread's share (threads [0, nthr)); its new terms go to
+// s.tnew, and nclash counts its pairs inside their guard distance.
+__device__ double cached_delta(const FFScalars& ff, const DMol& m, Smem& s, int v, int tid,
+                               int nthr, int& nclash) {
+  const int b = m.cross_off[v], e = m.cross_off[v + 1];
+  const float convf = (float)ff.conv;
+  KSum k;
+  double d64 = 0.0;
+  for (int q = b + tid; q < e; q += nthr) {
+    const int t = m.cross_idx[q];
+    float term;
+    double t64;
+    if (cache_term(ff, s, m.flat[t], convf, term, t64)) {
+      d64 += t64 - (double)s.ecache[t];
+      ++nclash;
+    } else {
+      k.add(term - s.ecache[t]);
+    }
+    s.tnew[q - b] = term;
+  }
+  return k.value() + d64;
 }
 
 // ---------------------------------------------------------------- SASA
@@ -2017,6 +2110,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
   // the fused exchange it is evaluated while the chain waits for the other
   // chains to arrive at the exchange (opened: done ahead).
   bool opened = false;
+  // proposals sum only the pairs their turn changes against the cached terms
+  // (cok: the cache holds the state, which has no pair inside its guard)
+  const bool cmode = F32 && !SASA && set.cache_pairs > 0 && m.cache && !m.rows && !set.f.epsd;
+  bool cok = false;
   auto opening = [&]() {
     if (flags & kFlagExtraSetvar) {   // partem_s.f:194-198: setvar(i, vlvr) first
       setvar_all(m, s);
@@ -2035,6 +2132,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
     enew = total_of(sum);
     etor = sum[3];
     ep = (sum[0] + sum[1]) + sum[2];
+    if (cmode) {
+      pterms += (unsigned long long)m.npairs;
+      cok = !fill_pair_cache(set.f, m, s);
+    }
   };
 
   for (int sw = 0; sw < nsweeps; ++sw) {
@@ -2096,8 +2197,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       // sweep's start: no clash terms) and the state's pair energy is summed
       // afresh every 16 proposals (same coordinates; eol follows).
       const bool incr = ROWS && F32 && m.rows && !set.f.epsd && relaxed;
+      const bool cached = cmode && cok;
       double xold = 0.0;
-      pterms += incr ? 2ull * (unsigned long long)m.var_cross[cur.jv] : (unsigned long long)m.npairs;
+      pterms += incr     ? 2ull * (unsigned long long)m.var_cross[cur.jv]
+                : cached ? (unsigned long long)(m.cross_off[cur.jv + 1] - m.cross_off[cur.jv])
+                         : (unsigned long long)m.npairs;
       if (incr && p > 0 && (p & 15) == 0) {
         pterms += (unsigned long long)m.npairs;
         double el = 0.0, vw = 0.0, hb = 0.0;
@@ -2137,12 +2241,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       // setvar call on the dihedral state and prepares proposal p+1
       if (warp != spec_warp) {
         double el = 0.0, vw = 0.0, hb = 0.0, sl = 0.0;
-        if (incr)
+        if (incr) {
           el = cross_rows<F32>(set.f, m, s, kWarps - 1, lo, hi) - xold;   // the change
-        else if (ROWS && m.rows)
+        } else if (cached) {   // the change, and in sl the count of guarded pairs
+          int nc = 0;
+          el = cached_delta(set.f, m, s, cur.jv, threadIdx.x, nthr_pairs, nc);
+          sl = (double)nc;
+        } else if (ROWS && m.rows) {
           pair_rows<F32, true>(set.f, m, s, kWarps - 1, el, vw, hb);
-        else
+        } else {
           pair_energy<F32, false>(set.f, m, s, threadIdx.x, nthr_pairs, el, vw, hb);
+        }
         if (sasa)
           sl = sasa_energy(set.f, m, s, 0, kWarps - 1, err,
                            SasaInc{s.sae, s.san, lo, span, cur.a, cur.b, flip, sc.hlo, sc.hhi});
@@ -2167,9 +2276,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       // ---- phase C: every warp sums and decides (metropolis.f:72-87)
       double dpair = warp_tree_sum(lane < kWarps - 1 ? s.red[lane * 8] : 0.0), esl = 0.0;
       if (sasa) esl = warp_tree_sum(lane < kWarps - 1 ? s.red[lane * 8 + 1] : 0.0);
-      // pair energy of the proposal: the state's plus the change (row form),
-      // or the full sum
-      const double epair = (incr ? ep + dpair : dpair) + esl;
+      const bool pclash =
+          cached && warp_tree_sum(lane < kWarps - 1 ? s.red[lane * 8 + 1] : 0.0) > 0.0;
+      // pair energy of the proposal: the state's plus the change (row form,
+      // cached terms), or the full sum
+      const double epair = ((incr || cached) ? ep + dpair : dpair) + esl;
       // every value read here was written before the last barrier
       const double etor_new = (etor - cur.eold) + cur.enew;
       const double enw = epair + etor_new;
@@ -2194,9 +2305,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       if (up) {
         eol = enw;
         etor = etor_new;
-        if (incr) ep += dpair;
+        if (incr || cached) ep += dpair;
         if (sasa)   // the proposal's SASA terms become the state's
           for (int h = threadIdx.x; h < m.nheavy; h += blockDim.x) s.sae[h] = s.san[h];
+        if (cached) {   // the new terms become the state's (a guarded pair: full sums from here)
+          if (pclash) {
+            cok = false;
+          } else {
+            const int cb = m.cross_off[cur.jv], ce = m.cross_off[cur.jv + 1];
+            for (int q = cb + (int)threadIdx.x; q < ce; q += blockDim.x)
+              s.ecache[m.cross_idx[q]] = s.tnew[q - cb];
+          }
+        }
       } else {
         for (int t = threadIdx.x; t < nmoved; t += blockDim.x) {
           const int k = moved_atom(t, lo, span, flip);
@@ -2674,13 +2794,14 @@ __global__ void __launch_bounds__(32) k_exchange(DChains ch, int* temp_chain, co
 size_t sweep_smem_bytes(const DMolSet& set) {
   const bool sasa = set.f.itysol > 0;
   return smem_layout(set.max_atoms, set.max_vars, set.f.npnt, sasa, set.da != 0,
-                     sasa ? 0 : set.window, nullptr, nullptr) +
+                     sasa ? 0 : set.window, sasa ? 0 : set.cache_pairs,
+                     sasa ? 0 : set.cache_cross, nullptr, nullptr) +
          (size_t)set.stage_bytes;
 }
 
 size_t stage_bytes_of(const DMol& d, bool lists) {
   return stage_size(d.natoms, d.nvar, d.nsib, d.nlevels, d.nfree, d.npairs, d.nheavy,
-                    d.rows != 0, lists);
+                    d.rows != 0, lists, d.cache ? d.ncross : 0);
 }
 
 cudaError_t launch_seed(uint32_t* mt, const int* seeds, int nslots, cudaStream_t st) {

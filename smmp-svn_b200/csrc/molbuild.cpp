@@ -1095,6 +1095,25 @@ MolTopo build_topology(const ResidueLibrary& lib, const ForceField& ff, const Bu
       t.var_cross.push_back(c);
     }
   }
+  // the same, as indices into the dense list, for each free variable, less
+  // the pairs with an atom on the variable's axis (their distance does not
+  // change when the range turns about that axis)
+  t.cross_off.assign(nv + 1, 0);
+  if (t.flat.size() <= 65535) {
+    std::vector<char> is_free(nv, 0);
+    for (int v : t.idvr) is_free[v] = 1;
+    for (int v = 0; v < nv; ++v) {
+      t.cross_off[v] = (int)t.cross_idx.size();
+      if (!is_free[v]) continue;
+      const int lo = t.var_lo[v], hi = t.var_hi[v], b = t.var_base[v], a = t.iow[b];
+      for (size_t k = 0; k < t.flat.size(); ++k) {
+        const int i = int(t.flat[k] & 0x3fffu), j = int((t.flat[k] >> 14) & 0x3fffu);
+        if (i == a || i == b || j == a || j == b) continue;
+        if ((i >= lo && i <= hi) != (j >= lo && j <= hi)) t.cross_idx.push_back((uint16_t)k);
+      }
+    }
+    t.cross_off[nv] = (int)t.cross_idx.size();
+  }
   // the same pair set by rows (every pair once, 1-4 pairs within the window)
   t.near_mask.assign(n, 0);
   t.near14.assign(n, 0);

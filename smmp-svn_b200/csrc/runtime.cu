@@ -161,6 +161,13 @@ DeviceSet::DeviceSet(const std::vector<std::shared_ptr<Molecule>>& mols) {
     d.var_lo = upload(t.var_lo);
     d.var_hi = upload(t.var_hi);
     d.var_cross = upload(t.var_cross);
+    d.cross_off = upload(t.cross_off);
+    d.cross_idx = upload(t.cross_idx.empty() ? std::vector<uint16_t>{0} : t.cross_idx);
+    d.ncross = (int)t.cross_idx.size();
+    d.cross_max = 0;
+    for (int v = 0; v < t.nvar; ++v)
+      d.cross_max = std::max(d.cross_max, t.cross_off[v + 1] - t.cross_off[v]);
+    d.cache = t.cross_idx.empty() ? 0 : 1;
     d.flat = upload(t.flat.empty() ? std::vector<uint32_t>{0} : t.flat);
     d.npairs = (int)t.npairs;
     d.sib_off = upload(t.sib_off);
@@ -202,6 +209,12 @@ DeviceSet::DeviceSet(const std::vector<std::shared_ptr<Molecule>>& mols) {
   set_.any_rows = 0;
   for (const DMol& d : dm) set_.any_rows |= d.rows;
   set_.da = 0;
+  cache_pairs_ = cache_cross_ = 0;
+  for (const DMol& d : dm)
+    if (d.cache) {
+      cache_pairs_ = std::max(cache_pairs_, d.npairs);
+      cache_cross_ = std::max(cache_cross_, d.cross_max);
+    }
   with_lists_ = without_ = 0;
   for (const DMol& d : dm) {
     with_lists_ = std::max(with_lists_, stage_bytes_of(d, true));
@@ -250,9 +263,13 @@ void DeviceSet::set_da(bool on) {
 void DeviceSet::size_staging() {
   const size_t with_lists = with_lists_, without = without_;
   // stage the pair lists too when the largest molecule's copy fits
+  // (and keep the cached pair terms of list-form molecules when that fits too)
   const size_t budget = 200 * 1024;
   set_.stage_lists = 1;
   set_.stage_bytes = (int)with_lists;
+  set_.cache_pairs = cache_pairs_;
+  set_.cache_cross = cache_cross_;
+  if (sweep_smem_bytes(set_) > budget) set_.cache_pairs = set_.cache_cross = 0;
   if (sweep_smem_bytes(set_) > budget) {
     set_.stage_lists = 0;
     set_.stage_bytes = (int)without;

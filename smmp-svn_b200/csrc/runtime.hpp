@@ -53,6 +53,7 @@ class DeviceSet {
  private:
   void size_staging();
   size_t with_lists_ = 0, without_ = 0;
+  int cache_pairs_ = 0, cache_cross_ = 0;   // cached pair terms, when they fit
   std::vector<DMol> dm_;
   std::vector<int> rows_ok_;
   DMol* dmols_ = nullptr;

@@ -81,6 +81,11 @@ struct MolTopo {
   std::vector<uint32_t> flat;
   long long npairs = 0;                // pair terms per full evaluation
   std::vector<int> var_cross;          // pairs across each variable's bond (one atom in its range)
+  // For molecules of at most 65,535 pairs: per free variable, the indices
+  // into `flat` of the pairs whose distance its turn changes (one atom in
+  // its range, neither on its axis), CSR by variable (empty for fixed ones).
+  std::vector<int> cross_off;
+  std::vector<uint16_t> cross_idx;
   // The same pair set by rows: for atom i, bit k of near_mask[i] / near14[i]
   // marks pair (i, i+1+k) as a normal / 1-4 pair.  rows_ok is set when every
   // pair more than kNearWindow apart is a normal pair and no pair is listed
