@@ -111,8 +111,11 @@ struct Proposal {
 };
 
 struct Scalars {
-  Proposal cur;
-  Proposal spec[2];      // next proposal if this one draws 1 (spec[0]) or 2 (spec[1]) numbers
+  // next proposal if this one draws 1 (spec[2 * par]) or 2 (spec[2 * par + 1])
+  // numbers, in two slots by the parity par of the proposal; spec[4] holds a
+  // proposal made after the decision (the first of a sweep, or the same
+  // variable again)
+  Proposal spec[5];
   int refill;
   int hlo, hhi;          // heavy-atom indices of the proposal's subtree range
   int gsync;             // result of the last grid barrier
@@ -1251,8 +1254,12 @@ __device__ __forceinline__ void set_err(int* err, int code) {
 
 // Prepare a proposal (metropolis.f:42-66) from queue position `pos`:
 // variable, new value and the cos/sin of the rotation it implies.
+// part 0 fills every field but enew, part 1 only enew; the two parts run
+// on two lanes through one sincos call (of the step and of the torsion
+// argument), so that neither waits for the other.  part < 0: both, one
+// after the other.
 __device__ void make_proposal(const DMol& m, const Smem& s, int p, uint32_t pos, bool rndord,
-                              Proposal& out) {
+                              Proposal& out, int part = -1) {
   const double* q = qbuf(s.mt);
   uint32_t k = pos;
   int ivar = p;
@@ -1266,24 +1273,57 @@ __device__ void make_proposal(const DMol& m, const Smem& s, int p, uint32_t pos,
   double dv = __dmul_rn(m.axvr[jv], __dsub_rn(q[k & (kQueue - 1)], 0.5));
   ++k;
   double vnew = addang(vold, dv);
-  double sv, cv;
-  sincos(difang(vold, vnew), &sv, &cv);
-  // dihedral of the primary atom after this proposal's setvar (setvar.f:40-53)
-  int iat = m.var_atom[jv];
-  double t0 = s.toat[iat];
-  double to = __dadd_rn(t0, difang(t0, vnew));
-  if (fabs(to) > kPi) to = __dsub_rn(to, copysign(kPi2, to));
-  out.jv = jv;
-  out.ivar = ivar;
-  out.used = (int)(k - pos);
-  out.b = m.var_base[jv];
-  out.a = m.iow[out.b];
-  out.vold = vold;
-  out.vnew = vnew;
-  out.cth = cv;
-  out.sth = sv;
-  out.enew = torsion_term(m, jv, to);
-  out.eold = s.et[jv];
+  if (part >= 0) {
+    double x;
+    if (part == 0) {
+      x = difang(vold, vnew);
+    } else {   // dihedral of the primary atom after this proposal's setvar (setvar.f:40-53)
+      const double t0 = s.toat[m.var_atom[jv]];
+      double to = __dadd_rn(t0, difang(t0, vnew));
+      if (fabs(to) > kPi) to = __dsub_rn(to, copysign(kPi2, to));
+      x = to * m.var_rn[jv];
+    }
+    double sv, cv;
+    sincos(x, &sv, &cv);
+    if (part == 0) {
+      out.jv = jv;
+      out.ivar = ivar;
+      out.used = (int)(k - pos);
+      out.b = m.var_base[jv];
+      out.a = m.iow[out.b];
+      out.vold = vold;
+      out.vnew = vnew;
+      out.cth = cv;
+      out.sth = sv;
+      out.eold = s.et[jv];
+    } else {
+      const double e0 = m.var_e0[jv];
+      out.enew = e0 != 0.0 ? e0 * (1.0 + m.var_sg[jv] * cv) : 0.0;
+    }
+    return;
+  }
+  {
+    double sv, cv;
+    sincos(difang(vold, vnew), &sv, &cv);
+    out.jv = jv;
+    out.ivar = ivar;
+    out.used = (int)(k - pos);
+    out.b = m.var_base[jv];
+    out.a = m.iow[out.b];
+    out.vold = vold;
+    out.vnew = vnew;
+    out.cth = cv;
+    out.sth = sv;
+    out.eold = s.et[jv];
+  }
+  {
+    // dihedral of the primary atom after this proposal's setvar (setvar.f:40-53)
+    int iat = m.var_atom[jv];
+    double t0 = s.toat[iat];
+    double to = __dadd_rn(t0, difang(t0, vnew));
+    if (fabs(to) > kPi) to = __dsub_rn(to, copysign(kPi2, to));
+    out.enew = torsion_term(m, jv, to);
+  }
 }
 
 // Load the chain's state into shared memory.
@@ -2156,14 +2196,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
                            pterms);
     }
     if (!windowed && m.nfree > 0 && threadIdx.x == 0) {
-      make_proposal(m, s, 0, head, rndord, sc.cur);
-      s.vlvr[sc.cur.jv] = sc.cur.vnew;
+      make_proposal(m, s, 0, head, rndord, sc.spec[4]);
+      s.vlvr[sc.spec[4].jv] = sc.spec[4].vnew;
       sc.refill = 0;
     }
     __syncthreads();
 
-    for (int p = 0; p < (windowed ? 0 : m.nfree); ++p) {
-      const Proposal cur = sc.cur;
+    int cur_slot = 4;   // sc.spec slot of the current proposal
+    for (int p = 0, par = 0; p < (windowed ? 0 : m.nfree); ++p, par ^= 1) {
+      const Proposal cur = sc.spec[cur_slot];
       const int lo = m.var_lo[cur.jv], hi = m.var_hi[cur.jv];
       // The rebuild holds the first three backbone atoms in place (setgbl):
       // when the subtree holds i3 (the dihedral about i1-i2), the rest of the
@@ -2269,15 +2310,21 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
         setvar_warp(m, s);
         __syncwarp();
         if (sc.refill) rng_refill_warp(s.mt, s.lq);
-        if (lane < 2 && p + 1 < m.nfree)
-          make_proposal(m, s, p + 1, head + cur.used + lane, rndord, sc.spec[lane]);
+        if (lane < 4 && p + 1 < m.nfree)   // two proposals, each on two lanes
+          make_proposal(m, s, p + 1, head + cur.used + (lane & 1), rndord,
+                        sc.spec[2 * par + (lane & 1)], lane >> 1);
       }
       __syncthreads();
       // ---- phase C: every warp sums and decides (metropolis.f:72-87)
-      double dpair = warp_tree_sum(lane < kWarps - 1 ? s.red[lane * 8] : 0.0), esl = 0.0;
-      if (sasa) esl = warp_tree_sum(lane < kWarps - 1 ? s.red[lane * 8 + 1] : 0.0);
-      const bool pclash =
-          cached && warp_tree_sum(lane < kWarps - 1 ? s.red[lane * 8 + 1] : 0.0) > 0.0;
+      double dpair = lane < kWarps - 1 ? s.red[lane * 8] : 0.0;
+      double sum1 = lane < kWarps - 1 ? s.red[lane * 8 + 1] : 0.0;   // SASA, or guarded pairs
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {   // warp_tree_sum of both, interleaved
+        dpair += __shfl_xor_sync(0xffffffffu, dpair, o);
+        sum1 += __shfl_xor_sync(0xffffffffu, sum1, o);
+      }
+      const double esl = sasa ? sum1 : 0.0;
+      const bool pclash = cached && sum1 > 0.0;
       // pair energy of the proposal: the state's plus the change (row form,
       // cached terms), or the full sum
       const double epair = ((incr || cached) ? ep + dpair : dpair) + esl;
@@ -2337,14 +2384,19 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
           s.vlvr[cur.jv] = cur.vold;
         if (!isfinite(enw)) set_err(err, kErrNonFinite);
         if (p + 1 < m.nfree) {
-          Proposal nx = sc.spec[drew];
-          if (nx.jv == cur.jv) make_proposal(m, s, p + 1, head, rndord, nx);   // same variable again
-          sc.cur = nx;
-          s.vlvr[nx.jv] = nx.vnew;
+          Proposal& nx = sc.spec[2 * par + drew];
+          if (nx.jv == cur.jv) {   // same variable again: from the state after this decision
+            make_proposal(m, s, p + 1, head, rndord, sc.spec[4]);
+            s.vlvr[cur.jv] = sc.spec[4].vnew;
+          } else {
+            s.vlvr[nx.jv] = nx.vnew;
+          }
         }
         sc.refill = (s.mt[kQTail] - head) < 24 ? 1 : 0;
       }
       __syncthreads();
+      // the next proposal's slot (every thread reads the same words)
+      if (p + 1 < m.nfree) cur_slot = sc.spec[2 * par + drew].jv == cur.jv ? 4 : 2 * par + drew;
     }
     // ---- closing energy() and consistency check (metropolis.f:172-179)
     if (warp == spec_warp) {
