@@ -2091,9 +2091,12 @@ __device__ __noinline__ void sweep_windows(const DMolSet& set, const DMol& m, Sm
 
 // nsweeps Metropolis sweeps (metropolis.f:13-184) of chains
 // [first, first+gridDim.x).  Per sweep the reference calls energy() nvr+2
-// times; here the start of every sweep does a full setvar+rebuild+evaluation,
-// each proposal updates the dihedral state with the same setvar arithmetic,
-// rotates the moving subtree in place and evaluates every pair of the lists,
+// times; here the start of every sweep does a full setvar and evaluation
+// (with a rebuild: every sweep with FP64 pair terms, the first of the launch
+// with FP32 ones), each proposal updates the dihedral state with the same
+// setvar arithmetic, rotates the moving subtree in place and evaluates the
+// pairs it changes (all of the lists, the crossing rows, or the crossing
+// pairs against cached terms),
 // and the closing consistency check of the launch's last sweep does a full
 // evaluation (earlier sweeps are checked against the next opening one).
 // With pt.on every sweep is followed by a replica exchange of all chains of
@@ -2154,7 +2157,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
   // (cok: the cache holds the state, which has no pair inside its guard)
   const bool cmode = F32 && !SASA && set.cache_pairs > 0 && m.cache && !m.rows && !set.f.epsd;
   bool cok = false;
-  auto opening = [&]() {
+  // With FP32 pair terms only the launch's first sweep rebuilds the
+  // coordinates from the dihedrals: later sweeps start from the coordinates
+  // their predecessor's accepted rotations left, which differ from a rebuild
+  // by FP64 rounding alone, far below what FP32 terms resolve.  FP64 pair
+  // terms rebuild every sweep, as energy() does (metropolis.f:35).
+  auto opening = [&](bool rebuild) {
     if (flags & kFlagExtraSetvar) {   // partem_s.f:194-198: setvar(i, vlvr) first
       setvar_all(m, s);
       __syncthreads();
@@ -2164,7 +2172,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
     __syncthreads();
     pterms += (unsigned long long)m.npairs;
     torsion_all(m, s);
-    full_rebuild(m, s);
+    if (rebuild)
+      full_rebuild(m, s);
+    else
+      __syncthreads();
     evaluate_block<F32, ROWS, SASA>(set.f, m, s, err);
     __syncthreads();
     double sum[5];
@@ -2179,7 +2190,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
   };
 
   for (int sw = 0; sw < nsweeps; ++sw) {
-    if (!opened) opening();
+    if (!opened) opening(!F32 || sw == 0);
     opened = false;
     if (check_pending && threadIdx.x == 0 && !(flags & kFlagNoCheck) &&
         fabs(eol - enew) > check_tol && eol < 100000.0)
@@ -2433,7 +2444,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       const unsigned nchain = gridDim.x - (pt.master ? 1u : 0u) + pt.extra;
       const unsigned gen = grid_arrive(pt.bar, nchain, !pt.master, &sc.gen);
       if (sw + 1 < nsweeps) {
-        opening();
+        opening(!F32);
         opened = true;
       }
       if (!grid_wait(pt.bar, gen, pt.timeout_ns, err, &sc.gsync)) break;
