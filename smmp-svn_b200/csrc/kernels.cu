@@ -2388,7 +2388,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       head += cur.used + drew;
       ++nprop;
       nacc += up;
-      if (threadIdx.x == 0) {
+      // the state's bookkeeping on the last warp, which restores no atoms
+      // (it moves none) and so reaches this point first
+      if (threadIdx.x == spec_warp * 32) {
         if (up)
           s.et[cur.jv] = cur.enew;
         else
