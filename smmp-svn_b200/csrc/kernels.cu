@@ -1202,14 +1202,10 @@ __device__ __forceinline__ void all_sums(const Smem& s, double* out) {
 #pragma unroll
   for (int k = 0; k < 5; ++k) out[k] = v[k];
 }
-// Sum of nw <= 16 warp partials in the order of a 32-lane xor butterfly whose
-// lanes nw..31 hold zero: warp_tree_sum over a warp and tree_sum16 in one
-// thread give the same bits (lane 0's tree; every lane ends with its bits).
-__device__ __forceinline__ double warp_tree_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
+// Sum of nw <= 16 warp partials in the order of a 32-lane xor butterfly
+// (v += shfl_xor(v, o) for o = 16 .. 1) whose lanes nw..31 hold zero: the
+// decision phase's butterfly over a warp and tree_sum16 in one thread give
+// the same bits (lane 0's tree; every lane ends with its bits).
 __device__ __forceinline__ double tree_sum16(const double* p, int stride, int nw) {
   double t[16];
 #pragma unroll
@@ -2206,10 +2202,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
         sweep_windows<F32>(set, m, s, w, beta, err, rndord, eol, etor, ep, head, nacc, nprop,
                            pterms);
     }
-    if (!windowed && m.nfree > 0 && threadIdx.x == 0) {
-      make_proposal(m, s, 0, head, rndord, sc.spec[4]);
-      s.vlvr[sc.spec[4].jv] = sc.spec[4].vnew;
-      sc.refill = 0;
+    if (!windowed && m.nfree > 0 && warp == spec_warp) {   // the sweep's first proposal
+      if (lane < 2) make_proposal(m, s, 0, head, rndord, sc.spec[4], lane);
+      __syncwarp();
+      if (lane == 0) {
+        s.vlvr[sc.spec[4].jv] = sc.spec[4].vnew;
+        sc.refill = 0;
+      }
     }
     __syncthreads();
 
@@ -2309,9 +2308,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
                            SasaInc{s.sae, s.san, lo, span, cur.a, cur.b, flip, sc.hlo, sc.hhi});
         double v = (el + vw) + hb;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          v += __shfl_xor_sync(0xffffffffu, v, o);
-          sl += __shfl_xor_sync(0xffffffffu, sl, o);
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (sasa) {
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) sl += __shfl_xor_sync(0xffffffffu, sl, o);
+        } else {   // the cached terms need only whether some pair was guarded
+          sl = __any_sync(0xffffffffu, sl > 0.0) ? 1.0 : 0.0;
         }
         if (lane == 0) {
           s.red[warp * 8] = v;
@@ -2328,14 +2330,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       __syncthreads();
       // ---- phase C: every warp sums and decides (metropolis.f:72-87)
       double dpair = lane < kWarps - 1 ? s.red[lane * 8] : 0.0;
-      double sum1 = lane < kWarps - 1 ? s.red[lane * 8 + 1] : 0.0;   // SASA, or guarded pairs
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {   // warp_tree_sum of both, interleaved
+      for (int o = 16; o > 0; o >>= 1)   // the butterfly of tree_sum16
         dpair += __shfl_xor_sync(0xffffffffu, dpair, o);
-        sum1 += __shfl_xor_sync(0xffffffffu, sum1, o);
+      double esl = 0.0;
+      if (sasa) {
+        esl = lane < kWarps - 1 ? s.red[lane * 8 + 1] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) esl += __shfl_xor_sync(0xffffffffu, esl, o);
       }
-      const double esl = sasa ? sum1 : 0.0;
-      const bool pclash = cached && sum1 > 0.0;
+      // some warp met a guarded pair (cached terms)
+      const bool pclash =
+          cached && __any_sync(0xffffffffu, lane < kWarps - 1 && s.red[lane * 8 + 1] > 0.0);
       // pair energy of the proposal: the state's plus the change (row form,
       // cached terms), or the full sum
       const double epair = ((incr || cached) ? ep + dpair : dpair) + esl;
