@@ -119,6 +119,10 @@ struct Scalars {
   int refill;
   int hlo, hhi;          // heavy-atom indices of the proposal's subtree range
   int gsync;             // result of the last grid barrier
+  // a proposal's sums over the pair warps, formed once by the last of them
+  unsigned nred;         // pair warps done with the current proposal
+  int dclash;            // some pair was guarded (cached terms)
+  double dsum, dsl;      // pair energy (change), SASA energy
   unsigned gen;          // barrier generation seen at the last grid_arrive
   int wn;                // proposals of the current speculative window
 };
@@ -2122,6 +2126,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
   double beta = ch.beta[c];
   int* err = &ch.err[c];
   unsigned long long nacc = 0, nprop = 0, pterms = 0;
+  if (threadIdx.x == 0) sc.nred = 0;
   __syncthreads();
   // logs of the values already queued, then fill the queue
   if (warp == spec_warp) {
@@ -2319,6 +2324,32 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
           s.red[warp * 8] = v;
           s.red[warp * 8 + 1] = sl;
         }
+        // the last pair warp to get here sums the warps' partials once, in
+        // a fixed order (the butterfly of tree_sum16), for every warp to read
+        unsigned last = 0;
+        if (lane == 0) {
+          __threadfence_block();
+          last = atomicAdd(&sc.nred, 1u) == (unsigned)(kWarps - 2) ? 1u : 0u;
+        }
+        if (__shfl_sync(0xffffffffu, last, 0)) {
+          __threadfence_block();
+          double t = lane < kWarps - 1 ? s.red[lane * 8] : 0.0;
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+          double e1 = 0.0;
+          if (sasa) {
+            e1 = lane < kWarps - 1 ? s.red[lane * 8 + 1] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) e1 += __shfl_xor_sync(0xffffffffu, e1, o);
+          }
+          const bool anyc = __any_sync(0xffffffffu, lane < kWarps - 1 && s.red[lane * 8 + 1] > 0.0);
+          if (lane == 0) {
+            sc.dsum = t;
+            sc.dsl = e1;
+            sc.dclash = anyc ? 1 : 0;
+            sc.nred = 0;
+          }
+        }
       } else {
         setvar_warp(m, s);
         __syncwarp();
@@ -2329,19 +2360,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       }
       __syncthreads();
       // ---- phase C: every warp sums and decides (metropolis.f:72-87)
-      double dpair = lane < kWarps - 1 ? s.red[lane * 8] : 0.0;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1)   // the butterfly of tree_sum16
-        dpair += __shfl_xor_sync(0xffffffffu, dpair, o);
-      double esl = 0.0;
-      if (sasa) {
-        esl = lane < kWarps - 1 ? s.red[lane * 8 + 1] : 0.0;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) esl += __shfl_xor_sync(0xffffffffu, esl, o);
-      }
-      // some warp met a guarded pair (cached terms)
-      const bool pclash =
-          cached && __any_sync(0xffffffffu, lane < kWarps - 1 && s.red[lane * 8 + 1] > 0.0);
+      const double dpair = sc.dsum;
+      const double esl = sasa ? sc.dsl : 0.0;
+      const bool pclash = cached && sc.dclash != 0;   // some warp met a guarded pair
       // pair energy of the proposal: the state's plus the change (row form,
       // cached terms), or the full sum
       const double epair = ((incr || cached) ? ep + dpair : dpair) + esl;
