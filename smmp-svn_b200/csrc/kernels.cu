@@ -559,12 +559,13 @@ __device__ __forceinline__ void pair_term_at(const FFScalars& ff, const Smem& s,
     double ri = rsqrt(r2);
     double r2i = ri * ri;
     double r6i = r2i * r2i * r2i;
-    double ep = 1.0;
     if (ff.epsd) {
       double sr = ff.slp * (r2 * ri);
-      ep = ff.plt - (sr * sr + 2.0 * sr + 2.0) * (ff.plt - 1.0) * exp(-sr) / 2.0;
+      const double ep = ff.plt - (sr * sr + 2.0 * sr + 2.0) * (ff.plt - 1.0) * exp(-sr) / 2.0;
+      el += qq * ri / ep;
+    } else {
+      el += __dmul_rn(qq, ri);   // the same bits as dividing the product by a dielectric of 1
     }
-    el += qq * ri / ep;
     if (!ishb)
       vw += A * r6i * r6i - C * r6i;
     else
