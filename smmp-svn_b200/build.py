@@ -58,6 +58,14 @@ def build(force=False, verbose_ptxas=False):
         if force or _stale(obj, [src] + hdrs):
             extra = ["-Xptxas", "-v"] if verbose_ptxas else []
             _run([NVCC] + NVFLAGS + CUDA_EXTRA.get(f, []) + extra + ["-c", src, "-o", obj])
+    # the sweep kernels again with 384 threads per chain (small molecules)
+    src = os.path.join(SRC, "kernels.cu")
+    obj = os.path.join(OBJ, "kernels_t384.cu.o")
+    objs.append(obj)
+    if force or _stale(obj, [src] + hdrs):
+        extra = ["-Xptxas", "-v"] if verbose_ptxas else []
+        _run([NVCC] + NVFLAGS + ["-DSMMP_THREADS=384", "-DSMMP_BLOCK_VARIANT=t384"] + extra +
+             ["-c", src, "-o", obj])
     for f in CXX_SOURCES:
         src = os.path.join(SRC, f)
         obj = os.path.join(OBJ, f + ".o")

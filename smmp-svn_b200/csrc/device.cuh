@@ -7,7 +7,14 @@ namespace smmpb200 {
 
 constexpr int kTypes = 18;
 constexpr int kTP = kTypes * kTypes;
-constexpr int kThreads = 512;            // threads per chain (one CTA per chain)
+// Threads per chain (one CTA per chain).  kernels.cu is built twice: with 512
+// threads, and with 384 for the sweeps of small molecules (its kernels and
+// launchers then sit in namespace smmpb200::t384; SMMP_THREADS and
+// SMMP_BLOCK_VARIANT set by the build).
+#ifndef SMMP_THREADS
+#define SMMP_THREADS 512
+#endif
+constexpr int kThreads = SMMP_THREADS;
 constexpr int kWarps = kThreads / 32;
 constexpr int kMaxNeighbours = 96;       // SASA neighbours per atom (per-warp buffer)
 constexpr int kSasaQueue = 64;           // SASA neighbour candidates queued per warp

@@ -36,6 +36,9 @@
 #include "mt.cuh"
 
 namespace smmpb200 {
+#ifdef SMMP_BLOCK_VARIANT
+namespace SMMP_BLOCK_VARIANT {
+#endif
 
 namespace {
 
@@ -2884,13 +2887,16 @@ __global__ void __launch_bounds__(32) k_exchange(DChains ch, int* temp_chain, co
 
 // ============================================================================ host wrappers
 
-size_t sweep_smem_bytes(const DMolSet& set) {
+// (under another name for the calls below: in the 384-thread build the
+// 512-thread build's sweep_smem_bytes is also visible through the argument)
+static size_t launch_smem_bytes(const DMolSet& set) {
   const bool sasa = set.f.itysol > 0;
   return smem_layout(set.max_atoms, set.max_vars, set.f.npnt, sasa, set.da != 0,
                      sasa ? 0 : set.window, sasa ? 0 : set.cache_pairs,
                      sasa ? 0 : set.cache_cross, nullptr, nullptr) +
          (size_t)set.stage_bytes;
 }
+size_t sweep_smem_bytes(const DMolSet& set) { return launch_smem_bytes(set); }
 
 size_t stage_bytes_of(const DMol& d, bool lists) {
   return stage_size(d.natoms, d.nvar, d.nsib, d.nlevels, d.nfree, d.npairs, d.nheavy,
@@ -3009,7 +3015,7 @@ static int variant(const DMolSet& set, bool fp32) {
 
 cudaError_t launch_energy(const DMolSet& set, const DChains& ch, int first, int count, bool fp32,
                           cudaStream_t st) {
-  const size_t sm = sweep_smem_bytes(set);
+  const size_t sm = launch_smem_bytes(set);
   switch (variant(set, fp32)) {
     case 0: return launch_energy_t<false, false, false>(set, ch, first, count, sm, st);
     case 1: return launch_energy_t<false, false, true>(set, ch, first, count, sm, st);
@@ -3024,7 +3030,7 @@ cudaError_t launch_energy(const DMolSet& set, const DChains& ch, int first, int 
 
 cudaError_t launch_sweep(const DMolSet& set, const DChains& ch, const DWeight& w, int first,
                          int count, int nsweeps, int flags, double check_tol, cudaStream_t st) {
-  const size_t sm = sweep_smem_bytes(set);
+  const size_t sm = launch_smem_bytes(set);
 #define SMMP_SWEEP(a, b, c) \
   launch_sweep_t<a, b, c>(set, ch, w, first, count, nsweeps, flags, check_tol, sm, st)
   switch (variant(set, (flags & kFlagFP32) != 0)) {
@@ -3044,7 +3050,7 @@ cudaError_t launch_sweep_pt(const DMolSet& set, const DChains& ch, const DWeight
                             int nsweeps, int flags, double check_tol, const DPTFused& pt,
                             cudaStream_t st) {
   if (ch.sur.w1 != nullptr || pt.n != count) return cudaErrorNotSupported;
-  const size_t sm = sweep_smem_bytes(set);
+  const size_t sm = launch_smem_bytes(set);
 #define SMMP_SWEEP(a, b, c) \
   launch_sweep_pt_t<a, b, c>(set, ch, w, count, nsweeps, flags, check_tol, pt, sm, st)
   switch (variant(set, (flags & kFlagFP32) != 0)) {
@@ -3062,7 +3068,7 @@ cudaError_t launch_sweep_pt(const DMolSet& set, const DChains& ch, const DWeight
 
 cudaError_t launch_gradient(const DMolSet& set, const DChains& ch, int first, int count,
                             double* grad, cudaStream_t st) {
-  const size_t sm = sweep_smem_bytes(set);
+  const size_t sm = launch_smem_bytes(set);
   cudaError_t e = prep_smem((const void*)k_gradient, sm);
   if (e != cudaSuccess || count <= 0) return e;
   k_gradient<<<count, kThreads, sm, st>>>(set, ch, first, grad);
@@ -3076,4 +3082,7 @@ cudaError_t launch_exchange(const DChains& ch, int* temp_chain, const double* be
   return cudaGetLastError();
 }
 
+#ifdef SMMP_BLOCK_VARIANT
+}  // namespace SMMP_BLOCK_VARIANT
+#endif
 }  // namespace smmpb200

@@ -50,4 +50,15 @@ cudaError_t launch_exchange(const DChains& ch, int* temp_chain, const double* be
                             uint32_t* mt, int* iswitch, int wrap, unsigned long long* stats,
                             cudaStream_t st);
 
+// The sweeps of the 384-thread build of kernels.cu (small molecules: less
+// register spilling per thread, and their pair work needs no more warps).
+namespace t384 {
+size_t sweep_smem_bytes(const DMolSet& set);
+cudaError_t launch_sweep(const DMolSet& set, const DChains& ch, const DWeight& w, int first,
+                         int count, int nsweeps, int flags, double check_tol, cudaStream_t st);
+cudaError_t launch_sweep_pt(const DMolSet& set, const DChains& ch, const DWeight& w, int count,
+                            int nsweeps, int flags, double check_tol, const DPTFused& pt,
+                            cudaStream_t st);
+}  // namespace t384
+
 }  // namespace smmpb200
