@@ -390,12 +390,18 @@ __device__ void load_static(const DForceField& ff, const DMol& m, Smem& s, bool 
 
 // FP32 copy of atom k's position as a hi+lo pair of floats, so that FP32
 // differences of two positions keep FP64-difference accuracy; p4.w holds the
-// charge and l4.w the atom type (as int bits).
+// charge and l4.w the atom type (as int bits).  hi is x with its mantissa cut
+// to the 24 bits a float holds (by masking: exact as a float, and x - hi is
+// exact in FP64), lo the rest rounded to a float, so hi + lo keeps 48 bits of
+// x and only the two independent conversions to float remain.
+__device__ __forceinline__ double float_head(double v) {
+  return __longlong_as_double(__double_as_longlong(v) & (long long)0xFFFFFFFFE0000000ull);
+}
 __device__ __forceinline__ void split_hi_lo(double x, double y, double z, float q, float tbits,
                                             float4& p4, float4& l4) {
-  float xh = (float)x, yh = (float)y, zh = (float)z;
-  p4 = make_float4(xh, yh, zh, q);
-  l4 = make_float4((float)(x - (double)xh), (float)(y - (double)yh), (float)(z - (double)zh), tbits);
+  const double xh = float_head(x), yh = float_head(y), zh = float_head(z);
+  p4 = make_float4((float)xh, (float)yh, (float)zh, q);
+  l4 = make_float4((float)(x - xh), (float)(y - yh), (float)(z - zh), tbits);
 }
 __device__ __forceinline__ void f32_copy(Smem& s, int k) {
   split_hi_lo(s.x[k], s.y[k], s.z[k], (float)s.cq[k], __int_as_float((int)s.type[k]), s.p4[k],
