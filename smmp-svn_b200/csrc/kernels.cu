@@ -1763,7 +1763,7 @@ __device__ bool grid_wait(unsigned* bar, unsigned g, unsigned long long timeout_
 // The master block of a fused parallel-tempering launch (the launch's extra
 // last block, on an SM no chain uses): for each of the nsweeps rounds it
 // waits, bounded, until all `expected` chains have arrived, runs the
-// exchange with its first warp, shuts the count and opens the barrier; then
+// exchange with its first warp and opens the barrier; then
 // it tops up the exchange stream's queue for the next round while the
 // chains sweep.  It alone touches the exchange stream during the launch.  A
 // wait that runs out ends it (the chains' own waits then run out too and
@@ -1775,8 +1775,11 @@ __device__ void pt_master(const DChains& ch, const DPTFused& pt, int nsweeps, un
   for (int r = 0; r < nsweeps; ++r) {
     int ok = 1;
     if (lane == 0) {
+      // the count is never reset within the launch: round r is complete
+      // when (r + 1) * expected chains have arrived
+      const unsigned target = expected * (unsigned)(r + 1);
       const unsigned long long t0 = global_ns();
-      while (*cnt != expected) {
+      while (*cnt < target) {
         if (global_ns() - t0 > pt.timeout_ns) {
           ok = 0;
           break;
@@ -1787,11 +1790,7 @@ __device__ void pt_master(const DChains& ch, const DPTFused& pt, int nsweeps, un
     }
     if (!__shfl_sync(0xffffffffu, ok, 0)) return;
     exchange_core(ch, pt.temp_chain, pt.betas, pt.n, pt.mt, pt.lq, pt.iswitch, pt.wrap, pt.stats);
-    if (lane == 0) {
-      atomicExch(pt.bar, 0u);
-      __threadfence();
-      atomicAdd(pt.bar + 1, 1u);
-    }
+    if (lane == 0) atomicAdd(pt.bar + 1, 1u);   // the exchange's writes are fenced
     __syncwarp();
     // the refill the next exchange would start with, done now (the same
     // values at the same points of the stream)
