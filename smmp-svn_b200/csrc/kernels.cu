@@ -1802,6 +1802,36 @@ __device__ void pt_master(const DChains& ch, const DPTFused& pt, int nsweeps, un
   }
 }
 
+// A chain's arrival at the exchange master's barrier (no generation read).
+__device__ void grid_count_in(unsigned* bar) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(bar, 1u);
+  }
+}
+// Wait, bounded, until the master has opened `round` rounds (spinning: the
+// wait is short and on the chains' critical path).
+__device__ bool grid_wait_round(unsigned* bar, unsigned round, unsigned long long timeout_ns,
+                                int* err, int* flag) {
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    volatile unsigned* gen = bar + 1;
+    const unsigned long long t0 = global_ns();
+    while ((int)(*gen - round) < 0) {
+      if (global_ns() - t0 > timeout_ns) {
+        ok = 0;
+        if (*err == 0) *err = kErrTimeout;
+        break;
+      }
+    }
+    __threadfence();
+    *flag = ok;
+  }
+  __syncthreads();
+  return *flag != 0;
+}
+
 // Atom t of the set a proposal moves: the subtree [lo, lo+span) or, when
 // `flip`, every other atom.
 __device__ __forceinline__ int moved_atom(int t, int lo, int span, bool flip) {
@@ -2480,12 +2510,19 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       // opening energy of its next sweep
       if (threadIdx.x == 0) ch.eol[c] = eol;
       const unsigned nchain = gridDim.x - (pt.master ? 1u : 0u) + pt.extra;
-      const unsigned gen = grid_arrive(pt.bar, nchain, !pt.master, &sc.gen);
+      // (with the master the generation is the number of rounds exchanged,
+      // so a chain need not read it before arriving)
+      const unsigned gen =
+          pt.master ? (grid_count_in(pt.bar), 0u) : grid_arrive(pt.bar, nchain, true, &sc.gen);
       if (sw + 1 < nsweeps) {
         opening(!F32);
         opened = true;
       }
-      if (!grid_wait(pt.bar, gen, pt.timeout_ns, err, &sc.gsync)) break;
+      if (pt.master) {
+        if (!grid_wait_round(pt.bar, (unsigned)(sw + 1), pt.timeout_ns, err, &sc.gsync)) break;
+      } else if (!grid_wait(pt.bar, gen, pt.timeout_ns, err, &sc.gsync)) {
+        break;
+      }
       if (!pt.master) {
         if (blockIdx.x == 0 && warp == 0)
           exchange_core(ch, pt.temp_chain, pt.betas, pt.n, pt.mt, pt.lq, pt.iswitch, pt.wrap,
