@@ -1779,12 +1779,11 @@ __device__ void pt_master(const DChains& ch, const DPTFused& pt, int nsweeps, un
       // when (r + 1) * expected chains have arrived
       const unsigned target = expected * (unsigned)(r + 1);
       const unsigned long long t0 = global_ns();
-      while (*cnt < target) {
+      while (*cnt < target) {   // (spinning: the master's SM has nothing else to do)
         if (global_ns() - t0 > pt.timeout_ns) {
           ok = 0;
           break;
         }
-        __nanosleep(32);
       }
       __threadfence();
     }
@@ -2229,6 +2228,21 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
     }
   };
 
+  // The sweep's first proposal (by the last warp; with the fused exchange it
+  // is made while the chain waits for the exchange: it reads nothing of the
+  // temperature).
+  bool prepared = false;
+  auto first_proposal = [&]() {
+    if (warp == spec_warp) {
+      if (lane < 2) make_proposal(m, s, 0, head, rndord, sc.spec[4], lane);
+      __syncwarp();
+      if (lane == 0) {
+        s.vlvr[sc.spec[4].jv] = sc.spec[4].vnew;
+        sc.refill = 0;
+      }
+    }
+  };
+
   for (int sw = 0; sw < nsweeps; ++sw) {
     if (!opened) opening(!F32 || sw == 0);
     opened = false;
@@ -2246,14 +2260,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
         sweep_windows<F32>(set, m, s, w, beta, err, rndord, eol, etor, ep, head, nacc, nprop,
                            pterms);
     }
-    if (!windowed && m.nfree > 0 && warp == spec_warp) {   // the sweep's first proposal
-      if (lane < 2) make_proposal(m, s, 0, head, rndord, sc.spec[4], lane);
-      __syncwarp();
-      if (lane == 0) {
-        s.vlvr[sc.spec[4].jv] = sc.spec[4].vnew;
-        sc.refill = 0;
-      }
-    }
+    if (!windowed && m.nfree > 0 && !prepared) first_proposal();
+    prepared = false;
     __syncthreads();
 
     int cur_slot = 4;   // sc.spec slot of the current proposal
@@ -2517,6 +2525,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       if (sw + 1 < nsweeps) {
         opening(!F32);
         opened = true;
+        bool win_next = false;   // the next sweep runs in speculative windows
+        if constexpr (ROWS && F32 && !SASA)
+          win_next = m.rows && !set.f.epsd && fabs(enew) < 1e4 && set.window >= 2 && m.nfree > 0;
+        if (!win_next && m.nfree > 0) {
+          first_proposal();
+          prepared = true;
+        }
       }
       if (pt.master) {
         if (!grid_wait_round(pt.bar, (unsigned)(sw + 1), pt.timeout_ns, err, &sc.gsync)) break;
