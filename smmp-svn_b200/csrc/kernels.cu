@@ -2485,6 +2485,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       // the next proposal's slot (every thread reads the same words)
       if (p + 1 < m.nfree) cur_slot = sc.spec[2 * par + drew].jv == cur.jv ? 4 : 2 * par + drew;
     }
+    // with the exchange master, the sweep's energy is published and the chain
+    // counted in at once: the closing setvar and checks need no temperature
+    if (pt.on && pt.master) {
+      if (threadIdx.x == 0) ch.eol[c] = eol;
+      grid_count_in(pt.bar);
+    }
     // ---- closing energy() and consistency check (metropolis.f:172-179)
     if (warp == spec_warp) {
       const bool low = __shfl_sync(0xffffffffu, (s.mt[kQTail] - head) < 24u ? 1 : 0, 0) != 0;
@@ -2516,12 +2522,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       // between two barriers), then every chain takes up its new
       // temperature; between its arrival and its wait, a chain evaluates the
       // opening energy of its next sweep
-      if (threadIdx.x == 0) ch.eol[c] = eol;
+      // (with the master the chain arrived above, and the generation is the
+      // number of rounds exchanged, so it need not be read before arriving)
       const unsigned nchain = gridDim.x - (pt.master ? 1u : 0u) + pt.extra;
-      // (with the master the generation is the number of rounds exchanged,
-      // so a chain need not read it before arriving)
-      const unsigned gen =
-          pt.master ? (grid_count_in(pt.bar), 0u) : grid_arrive(pt.bar, nchain, true, &sc.gen);
+      unsigned gen = 0u;
+      if (!pt.master) {
+        if (threadIdx.x == 0) ch.eol[c] = eol;
+        gen = grid_arrive(pt.bar, nchain, true, &sc.gen);
+      }
       if (sw + 1 < nsweeps) {
         opening(!F32);
         opened = true;
