@@ -297,19 +297,23 @@ namespace {
 // its state in registers (the 512-thread build spills), and the pair work of
 // a small molecule does not need the extra warps (measured: Met-enkephalin
 // 4 % faster; the 256-chain poly-Ala batch and the 60-residue protein 11 %
-// and 17 % slower with 384 threads, so they keep 512).
-bool small_molecules(const DMolSet& set) { return set.max_atoms <= 128; }
+// and 17 % slower with 384 threads, so they keep 512).  Delayed acceptance
+// keeps 512 threads (its surrogate batches were measured at half the speed
+// with 384).
+bool small_molecules(const DMolSet& set, const DChains& ch) {
+  return set.max_atoms <= 128 && ch.sur.w1 == nullptr;
+}
 
 cudaError_t sweep_launch(const DMolSet& set, const DChains& ch, const DWeight& w, int first,
                          int count, int nsweeps, int flags, double check_tol, cudaStream_t st) {
-  return small_molecules(set)
+  return small_molecules(set, ch)
              ? t384::launch_sweep(set, ch, w, first, count, nsweeps, flags, check_tol, st)
              : launch_sweep(set, ch, w, first, count, nsweeps, flags, check_tol, st);
 }
 cudaError_t sweep_launch_pt(const DMolSet& set, const DChains& ch, const DWeight& w, int count,
                             int nsweeps, int flags, double check_tol, const DPTFused& pt,
                             cudaStream_t st) {
-  return small_molecules(set)
+  return small_molecules(set, ch)
              ? t384::launch_sweep_pt(set, ch, w, count, nsweeps, flags, check_tol, pt, st)
              : launch_sweep_pt(set, ch, w, count, nsweeps, flags, check_tol, pt, st);
 }
