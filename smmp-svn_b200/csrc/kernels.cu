@@ -1716,11 +1716,9 @@ __device__ __forceinline__ void pair_warps_sync() {
 // The same barrier in two halves: grid_arrive counts this block in and
 // returns the generation it saw (the barrier opens when the count reaches
 // `expected`); grid_wait waits, bounded as above, for the generation to move
-// on.  The block may work in between.
-// With release false the block whose arrival completes the count leaves the
-// barrier shut: the master block of the fused exchange opens it.
-__device__ unsigned grid_arrive(unsigned* bar, unsigned expected, bool release,
-                                unsigned* gen_seen) {
+// on.  The block may work in between.  (The fused exchange's master block
+// uses grid_count_in / grid_wait_round instead.)
+__device__ unsigned grid_arrive(unsigned* bar, unsigned expected, unsigned* gen_seen) {
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
@@ -1728,7 +1726,7 @@ __device__ unsigned grid_arrive(unsigned* bar, unsigned expected, bool release,
     const unsigned g = *gen;
     __threadfence();
     const unsigned arrived = atomicAdd(bar, 1u) + 1u;
-    if (release && arrived == expected) {
+    if (arrived == expected) {
       atomicExch(bar, 0u);
       __threadfence();
       atomicAdd(bar + 1, 1u);
@@ -2528,7 +2526,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       unsigned gen = 0u;
       if (!pt.master) {
         if (threadIdx.x == 0) ch.eol[c] = eol;
-        gen = grid_arrive(pt.bar, nchain, true, &sc.gen);
+        gen = grid_arrive(pt.bar, nchain, &sc.gen);
       }
       if (sw + 1 < nsweeps) {
         opening(!F32);
