@@ -409,6 +409,11 @@ __device__ __forceinline__ void f32_copy(Smem& s, int k) {
   split_hi_lo(s.x[k], s.y[k], s.z[k], (float)s.cq[k], __int_as_float((int)s.type[k]), s.p4[k],
               s.l4[k]);
 }
+// The same for an atom that moved to (x, y, z): its charge and type words
+// stay as the rebuild wrote them.
+__device__ __forceinline__ void f32_move(Smem& s, int k, double x, double y, double z) {
+  split_hi_lo(x, y, z, s.p4[k].w, s.l4[k].w, s.p4[k], s.l4[k]);
+}
 
 // ---------------------------------------------------------------- setvar
 // setvar.f:30-56 for every variable (one lane per variable; a variable shifts
@@ -2332,11 +2337,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
         for (int t = threadIdx.x; t < nmoved; t += nthr_pairs) {
           const int k = moved_atom(t, lo, span, flip);
           if (flip && (k == cur.a || k == cur.b)) continue;   // on the axis
-          s.bx[k] = s.x[k];
-          s.by[k] = s.y[k];
-          s.bz[k] = s.z[k];
-          rotate_point(ax, s.bx[k], s.by[k], s.bz[k], s.x[k], s.y[k], s.z[k]);
-          if (F32) f32_copy(s, k);
+          const double x0 = s.x[k], y0 = s.y[k], z0 = s.z[k];
+          s.bx[k] = x0;
+          s.by[k] = y0;
+          s.bz[k] = z0;
+          double ox, oy, oz;
+          rotate_point(ax, x0, y0, z0, ox, oy, oz);
+          s.x[k] = ox;
+          s.y[k] = oy;
+          s.z[k] = oz;
+          if (F32) f32_move(s, k, ox, oy, oz);
         }
         pair_warps_sync();
       }
@@ -2453,10 +2463,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
         for (int t = threadIdx.x; t < nmoved; t += blockDim.x) {
           const int k = moved_atom(t, lo, span, flip);
           if (flip && (k == cur.a || k == cur.b)) continue;
-          s.x[k] = s.bx[k];
-          s.y[k] = s.by[k];
-          s.z[k] = s.bz[k];
-          if (F32) f32_copy(s, k);
+          const double x0 = s.bx[k], y0 = s.by[k], z0 = s.bz[k];
+          s.x[k] = x0;
+          s.y[k] = y0;
+          s.z[k] = z0;
+          if (F32) f32_move(s, k, x0, y0, z0);
         }
       }
       head += cur.used + drew;
