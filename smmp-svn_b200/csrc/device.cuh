@@ -73,7 +73,6 @@ struct DMol {
   // variable; cache = 0 when the molecule has none: over 65,535 pairs)
   const int* cross_off;
   const uint16_t* cross_idx;
-  const uint32_t* cross_word;   // flat[cross_idx[q]], so a proposal reads both at once
   int ncross, cross_max;
   int cache;
 };

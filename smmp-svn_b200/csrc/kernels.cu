@@ -291,7 +291,6 @@ __host__ __device__ inline size_t stage_size(int natoms, int nvar, int nsib, int
     if (ncross > 0) {
       a(4, nvar + 1);   // cross_off
       a(2, ncross);     // cross_idx
-      a(4, ncross);     // cross_word
     }
   }
   return b;
@@ -362,7 +361,6 @@ __device__ const DMol& stage_mol(const DMolSet& set, const DChains& ch, int c, S
     if (set.cache_pairs > 0 && g.cache) {
       m.cross_off = stage_array(g.cross_off, g.nvar + 1, pool, end, ok);
       m.cross_idx = stage_array(g.cross_idx, g.ncross, pool, end, ok);
-      m.cross_word = stage_array(g.cross_word, g.ncross, pool, end, ok);
     }
   }
   __syncthreads();
@@ -972,7 +970,7 @@ __device__ double cached_delta(const FFScalars& ff, const DMol& m, Smem& s, int 
     const int t = m.cross_idx[q];
     float term;
     double t64;
-    if (cache_term(ff, s, m.cross_word[q], convf, term, t64)) {
+    if (cache_term(ff, s, m.flat[t], convf, term, t64)) {
       d64 += t64 - (double)s.ecache[t];
       ++nclash;
     } else {

@@ -164,11 +164,6 @@ DeviceSet::DeviceSet(const std::vector<std::shared_ptr<Molecule>>& mols) {
     d.cross_off = upload(t.cross_off);
     d.cross_idx = upload(t.cross_idx.empty() ? std::vector<uint16_t>{0} : t.cross_idx);
     d.ncross = (int)t.cross_idx.size();
-    {
-      std::vector<uint32_t> cw(std::max<size_t>(t.cross_idx.size(), 1), 0u);
-      for (size_t q = 0; q < t.cross_idx.size(); ++q) cw[q] = t.flat[t.cross_idx[q]];
-      d.cross_word = upload(cw);
-    }
     d.cross_max = 0;
     for (int v = 0; v < t.nvar; ++v)
       d.cross_max = std::max(d.cross_max, t.cross_off[v + 1] - t.cross_off[v]);
