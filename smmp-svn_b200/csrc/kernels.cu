@@ -109,6 +109,8 @@ __device__ void rng_refill_warp(uint32_t* slot, double* lq, int cnt = 32) {
 struct Proposal {
   int jv, ivar, used;   // variable, its index in idvr, RNG values its setup consumed
   int b, a;             // base atom of the rotation and its parent (axis a -> b)
+  int lo, hi;           // the atoms the variable moves, [lo, hi]
+  int cb, ce;           // its crossing pairs, cross_idx[cb, ce)
   double vold, vnew, cth, sth;
   double enew, eold;    // torsion energy of jv at its new / current dihedral
 };
@@ -960,9 +962,8 @@ __device__ bool fill_pair_cache(const FFScalars& ff, const DMol& m, Smem& s) {
 // The proposal's change of the pair energy over the crossing pairs of
 // variable v, this thread's share (threads [0, nthr)); its new terms go to
 // s.tnew, and nclash counts its pairs inside their guard distance.
-__device__ double cached_delta(const FFScalars& ff, const DMol& m, Smem& s, int v, int tid,
+__device__ double cached_delta(const FFScalars& ff, const DMol& m, Smem& s, int b, int e, int tid,
                                int nthr, int& nclash) {
-  const int b = m.cross_off[v], e = m.cross_off[v + 1];
   const float convf = (float)ff.conv;
   KSum k;
   double d64 = 0.0;
@@ -1306,6 +1307,10 @@ __device__ void make_proposal(const DMol& m, const Smem& s, int p, uint32_t pos,
       out.used = (int)(k - pos);
       out.b = m.var_base[jv];
       out.a = m.iow[out.b];
+      out.lo = m.var_lo[jv];
+      out.hi = m.var_hi[jv];
+      out.cb = m.cross_off[jv];
+      out.ce = m.cross_off[jv + 1];
       out.vold = vold;
       out.vnew = vnew;
       out.cth = cv;
@@ -1325,6 +1330,10 @@ __device__ void make_proposal(const DMol& m, const Smem& s, int p, uint32_t pos,
     out.used = (int)(k - pos);
     out.b = m.var_base[jv];
     out.a = m.iow[out.b];
+    out.lo = m.var_lo[jv];
+    out.hi = m.var_hi[jv];
+    out.cb = m.cross_off[jv];
+    out.ce = m.cross_off[jv + 1];
     out.vold = vold;
     out.vnew = vnew;
     out.cth = cv;
@@ -1911,6 +1920,10 @@ __device__ void make_proposal_w(const DMol& m, const Smem& s, int p, uint32_t po
   out.used = (int)(k - pos);
   out.b = m.var_base[jv];
   out.a = m.iow[out.b];
+  out.lo = m.var_lo[jv];
+  out.hi = m.var_hi[jv];
+  out.cb = m.cross_off[jv];
+  out.ce = m.cross_off[jv + 1];
   out.vold = vold;
   out.vnew = vnew;
   out.cth = cv;
@@ -2270,7 +2283,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
     int cur_slot = 4;   // sc.spec slot of the current proposal
     for (int p = 0, par = 0; p < (windowed ? 0 : m.nfree); ++p, par ^= 1) {
       const Proposal cur = sc.spec[cur_slot];
-      const int lo = m.var_lo[cur.jv], hi = m.var_hi[cur.jv];
+      const int lo = cur.lo, hi = cur.hi;
       // The rebuild holds the first three backbone atoms in place (setgbl):
       // when the subtree holds i3 (the dihedral about i1-i2), the rest of the
       // molecule turns by -theta instead, so the coordinates keep the
@@ -2306,7 +2319,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
       const bool cached = cmode && cok;
       double xold = 0.0;
       pterms += incr     ? 2ull * (unsigned long long)m.var_cross[cur.jv]
-                : cached ? (unsigned long long)(m.cross_off[cur.jv + 1] - m.cross_off[cur.jv])
+                : cached ? (unsigned long long)(cur.ce - cur.cb)
                          : (unsigned long long)m.npairs;
       if (incr && p > 0 && (p & 15) == 0) {
         pterms += (unsigned long long)m.npairs;
@@ -2356,7 +2369,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
           el = cross_rows<F32>(set.f, m, s, kWarps - 1, lo, hi) - xold;   // the change
         } else if (cached) {   // the change, and in sl the count of guarded pairs
           int nc = 0;
-          el = cached_delta(set.f, m, s, cur.jv, threadIdx.x, nthr_pairs, nc);
+          el = cached_delta(set.f, m, s, cur.cb, cur.ce, threadIdx.x, nthr_pairs, nc);
           sl = (double)nc;
         } else if (ROWS && m.rows) {
           pair_rows<F32, true>(set.f, m, s, kWarps - 1, el, vw, hb);
@@ -2452,7 +2465,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
           if (pclash) {
             cok = false;
           } else {
-            const int cb = m.cross_off[cur.jv], ce = m.cross_off[cur.jv + 1];
+            const int cb = cur.cb, ce = cur.ce;
             for (int q = cb + (int)threadIdx.x; q < ce; q += blockDim.x)
               s.ecache[m.cross_idx[q]] = s.tnew[q - cb];
           }
