@@ -2401,14 +2401,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_sweep(DMolSet set, DChains ch, 
         }
         if (__shfl_sync(0xffffffffu, last, 0)) {
           __threadfence_block();
+          // at most 16 partials: lanes 16-31 hold zeros, and the butterfly's
+          // first step (offset 16) would only add them
+          static_assert(kWarps - 1 <= 16, "pair-warp partials fit in 16 lanes");
           double t = lane < kWarps - 1 ? s.red[lane * 8] : 0.0;
 #pragma unroll
-          for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+          for (int o = 8; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
           double e1 = 0.0;
           if (sasa) {
             e1 = lane < kWarps - 1 ? s.red[lane * 8 + 1] : 0.0;
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) e1 += __shfl_xor_sync(0xffffffffu, e1, o);
+            for (int o = 8; o > 0; o >>= 1) e1 += __shfl_xor_sync(0xffffffffu, e1, o);
           }
           const bool anyc = __any_sync(0xffffffffu, lane < kWarps - 1 && s.red[lane * 8 + 1] > 0.0);
           if (lane == 0) {
